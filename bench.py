@@ -1,0 +1,328 @@
+"""Benchmark: simulated model days per wall second of the QGN time stepper on B200.
+
+Workload (default ``strat1024x8``): 8 geometric layers on a 1024^2 doubly periodic grid,
+L = 2000 km, N^2 = (5e-3)^2 exp(z/1000 m), U = 0.1 exp(z/1000 m), ARK43_QGLeith with the
+PI.3.4 controller and TOL = 1e-6 x max|q_IC|, FP64, from a seeded random PV field (seed 2,
+peak wavenumber 16, rms 1e-6 s^-1).  A step is one accepted TimeStep (6 RHS evaluations
+plus any rejected attempts).  Data are synthetic; the spin-up of the named configuration
+(10 model years) is not run -- timing starts from the seeded state after the warm-up steps.
+
+``value``: device-resident stepping (qgn_advance_resident), CUDA events on the library's
+stream.  ``e2e``: the drop-in path qgn_step (TimeStep) with the host q_hat in pinned memory,
+i.e. every step copies the kept modes host->device and back.  ``--impl reference`` times the
+CPU restatement of the reference (the oracle) on the host cores.
+
+Multi-GPU (torchrun): the path does not shard -- each rank advances an independent replica
+("replicas only"); value = total simulated days of all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "simulated days/s, 1024^2 x 8 layers, ARK43_QGLeith PI.3.4, FP64"
+UNIT = "simulated days/s"
+DAY = 86400.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="strat1024x8")
+    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.gpu = gpu_index
+        self.out = os.path.join("/tmp", f"qgn_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.out, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.out):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.out)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_oracle(w, warmup, steps):
+    """Time the FP64 CPU restatement (oracle) on the host cores."""
+    from oracle import qgn_oracle as O
+
+    nthr = cpu_threads()
+    O.set_fft_workers(nthr)
+    m = O.QGNOracle(O.Params(**w.params), w.H, w.S, w.U)
+    q = m.initialize_spec(w.qp)
+    st = O.SCHEMES[w.scheme](m)
+    t, dt = 0.0, w.dt0
+    for _ in range(warmup):
+        q, t, dt = st.step(q, t, dt)
+    t0 = t
+    c0 = time.perf_counter()
+    for _ in range(steps):
+        q, t, dt = st.step(q, t, dt)
+    sec = time.perf_counter() - c0
+    O.set_fft_workers(None)
+    return (t - t0) / DAY / sec, sec, steps, nthr
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from qgn_fortran_b200.inputs import workload
+    w = workload(args.workload)
+    warm = min(args.warmup, 1)
+    steps = max(1, min(args.steps, 3))
+    val, sec, n, nthr = run_oracle(w, warm, steps)
+    sample = (f"{n} {w.scheme} steps of {args.workload} after {warm} warm-up step(s), FP64 numpy/scipy "
+              f"restatement (oracle), scipy.fft workers={nthr}")
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": n,
+            "warmup": warm, "ms_per_step": 1000.0 * sec / n, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "grid": "1024x1024x8", "scheme": w.scheme},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthr, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ours_arm(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+
+    from qgn_fortran_b200 import QGNModule, _lib
+    from qgn_fortran_b200.inputs import workload
+
+    w = workload(args.workload)
+    g = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme)
+    q = g.initialize(w.qp, 0.0, w.dt0)
+    sptr = _lib.C.c_void_p()
+    g.lib.qgn_stream(g.ctx, _lib.C.byref(sptr))
+    stream = torch.cuda.ExternalStream(sptr.value)
+
+    for _ in range(args.warmup):
+        g.advance_resident(1)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    clocks = ClockSampler(local) if rank == 0 else None
+    g.lib.qgn_profile_enable(g.ctx, 1)
+    t0, _ = g.time()
+    barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    g.advance_resident(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop() if clocks else None
+    t1, dt1 = g.time()
+    days = (t1 - t0) / DAY
+
+    # per-kernel accounting of the timed region
+    fam = []
+    launches = 0
+    for k in range(_lib.QGN_KERNEL_FAMILIES):
+        tot, nb = _lib.C.c_double(), _lib.C.c_double()
+        nt, nl = _lib.C.c_longlong(), _lib.C.c_longlong()
+        g.lib.qgn_profile_read(g.ctx, k, _lib.C.byref(tot), _lib.C.byref(nb), _lib.C.byref(nt), _lib.C.byref(nl))
+        launches += nl.value
+        fam.append((tot.value, nb.value, nt.value, nl.value, g.lib.qgn_kernel_name(k).decode()))
+    g.lib.qgn_profile_enable(g.ctx, 0)
+
+    if ws > 1:
+        tt = torch.tensor([ms, days], dtype=torch.float64, device="cuda")
+        mx = tt.clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        sm = tt.clone()
+        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
+        ms_all, days_all = float(mx[0]), float(sm[1])
+    else:
+        ms_all, days_all = ms, days
+
+    # end-to-end through the drop-in TimeStep (qgn_step) with pinned host q_hat
+    e2e = None
+    if not args.no_e2e:
+        qh = torch.empty(q.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        g.get_state(qh)
+        t, dt = g.time()
+        te0 = t
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            t, dt = g.time_step(qh, t, dt)
+        e1.record(stream)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1)
+        edays = (t - te0) / DAY
+        if ws > 1:
+            tt = torch.tensor([ems, edays], dtype=torch.float64, device="cuda")
+            mx = tt.clone()
+            torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+            sm = tt.clone()
+            torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
+            ems, edays = float(mx[0]), float(sm[1])
+        kept = 16 * (w.params["nx"] // 3) * (w.params["ny"] - w.params["ny"] // 3 - 1) * w.params["nz"]
+        e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
+               "d2h_bytes_per_step": kept, "ms_per_step": ems / args.steps}
+
+    if rank != 0:
+        g.cleanup()
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    peak, peak_kind = measured_peaks()
+    top = max(fam, key=lambda f: f[0])
+    achieved = (top[1] / top[2]) / ((top[0] / top[2]) / 1000.0) / 1e9 if top[2] else None
+    traffic = read_traffic(args.workload, top[4])
+    roofline = {"bound": "hbm", "kernel": top[4], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": top[1] / top[2] if top[2] else None,
+                "ms_per_launch": top[0] / top[2] if top[2] else None,
+                "share_of_timed_region": top[0] / ms if ms else None}
+    kernels = {f[4]: {"ms": round(f[0], 4), "launches": f[3]} for f in fam if f[3]}
+
+    cpu = None
+    if ws == 1 and not args.no_cpu_baseline:
+        val, sec, n, nthr = run_oracle(w, 0, args.cpu_sample_steps)
+        cpu = {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
+               "sample": f"{n} {w.scheme} step(s) of {args.workload} from the seeded IC, FP64 numpy/scipy "
+                         f"restatement (oracle), scipy.fft workers={nthr}, {sec:.1f} s"}
+
+    line = {"metric": METRIC, "value": days_all / (ms_all / 1000.0), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "grid": f"{w.params['nx']}x{w.params['ny']}x{w.params['nz']}",
+                       "scheme": w.scheme, "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
+                       "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects()},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "kernels": kernels}
+    print(json.dumps(line), flush=True)
+    g.cleanup()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def read_traffic(workload, kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{workload}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+/*
+ * qgn_gpu.h -- C-ABI of the B200 (sm_100a) QGN spectral right-hand side and time steppers.
+ *
+ * This is the drop-in boundary for the reference's TimeStep path
+ * (iangrooms/QGN_Fortran).  A Fortran host binds these entry points through
+ * iso_c_binding from an include file selected exactly like the reference's
+ * schemes (QGN_Module.f90:306).  Every entry point returns an int status
+ * (QGN_OK == 0); qgn_last_error() gives the message of the last failure.
+ *
+ * Array conventions (identical to the reference's Fortran storage):
+ *   spectral  complex(dp) q_hat(nx/2+1, ny, nz)  -> interleaved (re,im) doubles,
+ *             element (i,j,k) (1-based) at offset 2*((i-1) + (nx/2+1)*((j-1) + ny*(k-1))).
+ *   physical  real(dp) q(nx, ny, nz), column-major.
+ *   Modes     real(dp) Modes(nz, nz), column-major: Modes(kk,k) = layer kk of mode k.
+ *
+ * Threading: one host thread per context; a context is not re-entrant (as the
+ * reference's module state is not).  Distinct contexts are independent.
+ */
+#ifndef QGN_GPU_H
+#define QGN_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define QGN_OK                0
+#define QGN_ERR_CONFIG        1   /* bad or unsupported parameters / inputs          */
+#define QGN_ERR_CUDA          2   /* a CUDA runtime call failed                       */
+#define QGN_ERR_NONFINITE     3   /* NaN/Inf found in the error norm or the state     */
+#define QGN_ERR_REJECT_LIMIT  4   /* adaptive step rejected max_rejects times in a row*/
+#define QGN_ERR_ARG           5   /* null pointer / invalid argument                  */
+#define QGN_ERR_NO_DEVICE     6   /* no CUDA device, or not an sm_100 device          */
+
+/* ---- time integrators: the include files of QGN_Module.f90:306 ---------- */
+#define QGN_SCHEME_ARK43_QGLEITH 0  /* ARK43_QGLeith.f90 (reference default) */
+#define QGN_SCHEME_ARK43         1  /* ARK43.f90  (fixed A8)                 */
+#define QGN_SCHEME_BSRK3         2  /* BSRK3.f90  (Bogacki-Shampine 3(2))    */
+#define QGN_SCHEME_RK4           3  /* RK4.f90                               */
+#define QGN_SCHEME_AB3           4  /* AB3.f90                               */
+
+/* ---- arithmetic of the spectral path ------------------------------------ */
+#define QGN_PREC_FP64   0   /* everything in FP64 (parity mode)                       */
+#define QGN_PREC_MIXED  1   /* FP32 transforms/products/stages, FP64 modes/norm/control */
+
+/* Runtime copy of the compile-time constants of parameters.f90:1-31. */
+typedef struct qgn_params {
+    int    nx, ny, nz;       /* grid; nx, ny powers of two in [16, 2048]; 2 <= nz <= 32 */
+    int    is_explicit;      /* parameters.f90:28 (0 = .FALSE.)                          */
+    double Lx, Ly, Htot;
+    double f0, beta;
+    double A2, A8, r0, C_d;
+    double TOL;              /* absolute error tolerance of the adaptive schemes         */
+    double dt_max;           /* parameters.f90:31                                        */
+    int    max_rejects;      /* consecutive rejected attempts before QGN_ERR_REJECT_LIMIT; 0 -> 64 */
+    int    reserved;
+} qgn_params;
+
+typedef struct qgn_ctx qgn_ctx;
+
+/*
+ * Create a device context.  Replaces the device-relevant half of Initialize
+ * (QGN_Module.f90:53-188): the host keeps reading H/S/UBar, building L and running
+ * DGEEV; it passes the results here.
+ *   H      nz layer thicknesses AFTER the rescale H=Htot*H/sum(H) (QGN_Module.f90:87)
+ *   S      nz+1 stratification values S(0:nz) (validated, not otherwise used); may be NULL
+ *   uBar   nz mean zonal velocities (QGN_Module.f90:145-147)
+ *   qyBar  nz mean PV gradients L*(-uBar) (QGN_Module.f90:148)
+ *   Modes  nz*nz normalised right eigenvectors, column-major (QGN_Module.f90:121-127)
+ *   EVals  nz eigenvalues (QGN_Module.f90:121)
+ * scheme: QGN_SCHEME_*; precision: QGN_PREC_*.
+ */
+int qgn_create(const qgn_params* p, const double* H, const double* S,
+               const double* uBar, const double* qyBar,
+               const double* Modes, const double* EVals,
+               int scheme, int precision, qgn_ctx** out);
+
+/*
+ * One call of TimeStep(q_hat,t,dt) (QGN_Module.f90:302-309) with the scheme chosen
+ * at qgn_create.  q_hat is the host spectral array (interleaved complex, Fortran
+ * order).  Only the modes that DeAlias keeps are read and written: the entries
+ * DeAlias zeroes (QGN_Module.f90:194-204) are treated as zero on input and left
+ * untouched on output (the reference's TimeStep zeroes them with its trailing
+ * DeAlias call).  t and dt are updated exactly as by the reference scheme.
+ * Stepper memory (FSAL stage, AB history, err0) persists in the context like the
+ * reference's `save` variables.
+ */
+int qgn_step(qgn_ctx* ctx, double* q_hat, double* t, double* dt);
+
+/* nsteps consecutive TimeStep calls with one host<->device transfer of q_hat. */
+int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps);
+
+/* Device-resident variants: the state lives on the GPU between calls. */
+int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt);
+int qgn_get_state(qgn_ctx* ctx, double* q_hat, double* t, double* dt);  /* writes all of q_hat */
+int qgn_advance_resident(qgn_ctx* ctx, int nsteps);
+int qgn_get_time(qgn_ctx* ctx, double* t, double* dt);
+
+/*
+ * One GetRHS(q_hat, RHS) evaluation (QGN_Module.f90:258-296), the parity hook.
+ * q_hat is dealiased on input (GetRHS assumes dealiased input, QGN_Module.f90:211);
+ * rhs receives the full dealiased right-hand side (zeros included).
+ */
+int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs);
+
+/* psi_hat of GetPsi (QGN_Module.f90:315-341) for a host q_hat; writes all of psi_hat. */
+int qgn_psi(qgn_ctx* ctx, const double* q_hat, double* psi_hat);
+
+/* QG-Leith coefficients A8L(1:nz) of ARK43_QGLeith.f90:62-73 for the resident state. */
+int qgn_leith(qgn_ctx* ctx, double* A8L);
+
+/*
+ * FP64 diagnostics of the resident state (the reference has none, QGN_Driver.f90:52-55):
+ *   ke_layer[nz]       0.5*mean(u^2+v^2)*H_k/Htot per layer
+ *   spectrum[nbins*nz] isotropic KE spectrum per layer in integer shells
+ *                      round(sqrt((i)^2+(jj)^2)) (wavenumber index units), may be NULL
+ */
+int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins);
+
+/*
+ * WriteQP's fields (QGN_Module.f90:348-377) in physical space: q_phys = c2r(q_hat)/(nx*ny)
+ * and psi_phys = c2r(psi_hat)/(nx*ny) as real(dp)(nx,ny,nz) column-major.  q_hat is a host
+ * spectral array, or NULL for the resident state.  Either output pointer may be NULL.
+ */
+int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_phys);
+
+/*
+ * Set the resident state from a physical PV field real(dp) q(nx,ny,nz): the forward
+ * transform and DeAlias of Initialize (QGN_Module.f90:179-183), as used for the IC and
+ * for restarts from q.%09d.dat (QGN_Driver.f90:21-30).
+ */
+int qgn_set_state_physical(qgn_ctx* ctx, const double* q_phys, double t, double dt);
+
+/* Number of rejected attempts since creation (the reference prints 'Rejected step'). */
+int qgn_rejects(qgn_ctx* ctx, long long* count);
+
+/*
+ * Kernel accounting (no counterpart in the reference, which prints only t and dt).
+ * Every kernel launch is counted per kernel family; with profiling enabled each launch is
+ * also bracketed by CUDA events on the context's stream.  qgn_profile_enable resets the
+ * counters.  qgn_profile_read returns, for one family id in [0, QGN_KERNEL_FAMILIES),
+ * the summed device time (ms), the summed algorithmic bytes of the timed launches, the
+ * number of timed launches and the number of launches.
+ */
+#define QGN_KERNEL_FAMILIES 14
+int qgn_profile_enable(qgn_ctx* ctx, int enable);
+int qgn_profile_read(qgn_ctx* ctx, int kernel, double* total_ms, double* bytes,
+                     long long* timed_launches, long long* launches);
+const char* qgn_kernel_name(int kernel);
+
+/* The cudaStream_t (as void*) all of this context's work is issued on. */
+int qgn_stream(qgn_ctx* ctx, void** stream);
+
+/* Message of the last failing call on this context (never NULL). */
+const char* qgn_last_error(const qgn_ctx* ctx);
+
+/* Release all device memory (replaces the DFTI frees of Cleanup, QGN_Module.f90:448-458). */
+int qgn_destroy(qgn_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QGN_GPU_H */

@@ -1,0 +1,102 @@
+"""ctypes binding of include/qgn_gpu.h.
+
+This is the same binding a Python host (or the ctypes stub in INTEGRATION.md) makes.
+Loading fails loudly when the CUDA library has not been built: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqgn_b200.so")
+
+QGN_OK = 0
+QGN_ERR_CONFIG = 1
+QGN_ERR_CUDA = 2
+QGN_ERR_NONFINITE = 3
+QGN_ERR_REJECT_LIMIT = 4
+QGN_ERR_ARG = 5
+QGN_ERR_NO_DEVICE = 6
+QGN_KERNEL_FAMILIES = 14
+
+SCHEMES = {"ark43_qgleith": 0, "ark43": 1, "bsrk3": 2, "rk4": 3, "ab3": 4}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+ERROR_NAMES = {
+    QGN_ERR_CONFIG: "QGN_ERR_CONFIG",
+    QGN_ERR_CUDA: "QGN_ERR_CUDA",
+    QGN_ERR_NONFINITE: "QGN_ERR_NONFINITE",
+    QGN_ERR_REJECT_LIMIT: "QGN_ERR_REJECT_LIMIT",
+    QGN_ERR_ARG: "QGN_ERR_ARG",
+    QGN_ERR_NO_DEVICE: "QGN_ERR_NO_DEVICE",
+}
+
+
+class qgn_params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("is_explicit", C.c_int),
+        ("Lx", C.c_double), ("Ly", C.c_double), ("Htot", C.c_double),
+        ("f0", C.c_double), ("beta", C.c_double),
+        ("A2", C.c_double), ("A8", C.c_double), ("r0", C.c_double), ("C_d", C.c_double),
+        ("TOL", C.c_double), ("dt_max", C.c_double),
+        ("max_rejects", C.c_int), ("reserved", C.c_int),
+    ]
+
+
+# every symbol include/qgn_gpu.h declares, with its ctypes signature
+_dp = C.POINTER(C.c_double)
+_ctxp = C.c_void_p
+SIGNATURES = {
+    "qgn_create": (C.c_int, [C.POINTER(qgn_params), _dp, _dp, _dp, _dp, _dp, _dp, C.c_int, C.c_int,
+                             C.POINTER(C.c_void_p)]),
+    "qgn_step": (C.c_int, [_ctxp, _dp, _dp, _dp]),
+    "qgn_advance": (C.c_int, [_ctxp, _dp, _dp, _dp, C.c_int]),
+    "qgn_set_state": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
+    "qgn_get_state": (C.c_int, [_ctxp, _dp, _dp, _dp]),
+    "qgn_advance_resident": (C.c_int, [_ctxp, C.c_int]),
+    "qgn_get_time": (C.c_int, [_ctxp, _dp, _dp]),
+    "qgn_rhs": (C.c_int, [_ctxp, _dp, _dp]),
+    "qgn_psi": (C.c_int, [_ctxp, _dp, _dp]),
+    "qgn_leith": (C.c_int, [_ctxp, _dp]),
+    "qgn_diagnostics": (C.c_int, [_ctxp, _dp, _dp, C.c_int]),
+    "qgn_physical": (C.c_int, [_ctxp, _dp, _dp, _dp]),
+    "qgn_set_state_physical": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
+    "qgn_rejects": (C.c_int, [_ctxp, C.POINTER(C.c_longlong)]),
+    "qgn_profile_enable": (C.c_int, [_ctxp, C.c_int]),
+    "qgn_profile_read": (C.c_int, [_ctxp, C.c_int, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "qgn_kernel_name": (C.c_char_p, [C.c_int]),
+    "qgn_stream": (C.c_int, [_ctxp, C.POINTER(C.c_void_p)]),
+    "qgn_last_error": (C.c_char_p, [_ctxp]),
+    "qgn_destroy": (C.c_int, [_ctxp]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libqgn_b200.so; raises if it is missing (build it with qgn_fortran_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build the CUDA library first (python -m qgn_fortran_b200.build)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class QGNError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def dptr(a):
+    """double* of a contiguous numpy array (complex arrays as interleaved doubles)."""
+    return a.ctypes.data_as(_dp)

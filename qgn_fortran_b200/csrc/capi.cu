@@ -1,0 +1,715 @@
+// capi.cu -- extern "C" boundary (include/qgn_gpu.h) and the host-side scheme drivers.
+//
+// The scheme drivers issue, per TimeStep, the same sequence of RHS evaluations, stage
+// combinations, error norms and controller updates as the reference include files
+// (ARK43_QGLeith.f90, ARK43.f90, BSRK3.f90, RK4.f90, AB3.f90).  Adaptive schemes read one
+// small scalar block back per attempt to decide accept/reject; the reject loop is bounded
+// by qgn_params.max_rejects (the reference loops forever and silently accepts NaN errors).
+#include "qgn_internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <utility>
+
+using namespace qgn;
+
+namespace qgn {
+Prof*& current_prof() {
+    thread_local Prof* p = nullptr;
+    return p;
+}
+}  // namespace qgn
+
+namespace {
+
+// Makes the context's profiler the current one for the duration of an API call.
+struct ProfScope {
+    Prof* prev;
+    explicit ProfScope(qgn_ctx* ctx) : prev(current_prof()) { current_prof() = ctx ? &ctx->prof : nullptr; }
+    ~ProfScope() { current_prof() = prev; }
+};
+
+int set_err(qgn_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+int cuda_err(qgn_ctx* ctx, const char* what, cudaError_t e) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    return set_err(ctx, QGN_ERR_CUDA, buf);
+}
+
+#define CK(call)                                                    \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return cuda_err(ctx, #call, _e);     \
+    } while (0)
+
+#define RET(call)                        \
+    do {                                 \
+        int _r = (call);                 \
+        if (_r != QGN_OK) return _r;     \
+    } while (0)
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// twiddles exp(-2 pi i m/n), m in [0,n), in long double with octant reduction
+void make_twiddles(int n, std::vector<double2>& tw) {
+    tw.resize(n);
+    const long double PI = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < n; ++m) {
+        long double a = 2.0L * PI * (long double)m / (long double)n;
+        tw[m] = make_double2((double)cosl(a), (double)(-sinl(a)));
+    }
+    // exact values at the quadrant points
+    for (int m = 0; m < n; m += (n >= 4 ? n / 4 : n)) {
+        const int qd = (n >= 4) ? (4 * m / n) : 0;
+        const double c[4] = {1.0, 0.0, -1.0, 0.0}, s[4] = {0.0, -1.0, 0.0, 1.0};
+        tw[m] = make_double2(c[qd], s[qd]);
+    }
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+int copy_kept(qgn_ctx* ctx, double* host, bool h2d) {
+    const Geom& g = ctx->g;
+    for (int part = 0; part < 2; ++part) {
+        const int j0 = part == 0 ? 0 : g.kylo + g.kyshift;
+        const int m0 = part == 0 ? 0 : g.kylo;
+        const int rows = part == 0 ? g.kylo : g.nky - g.kylo;
+        if (rows <= 0) continue;
+        cudaMemcpy3DParms prm;
+        std::memset(&prm, 0, sizeof(prm));
+        cudaPitchedPtr hp = make_cudaPitchedPtr(host, (size_t)g.nxh * 16, (size_t)g.nxh * 16, (size_t)g.ny);
+        cudaPitchedPtr dp = make_cudaPitchedPtr(ctx->b.xfer, (size_t)g.nkx * 16, (size_t)g.nkx * 16, (size_t)g.nky);
+        cudaPos hpos = make_cudaPos(0, (size_t)j0, 0), dpos = make_cudaPos(0, (size_t)m0, 0);
+        prm.extent = make_cudaExtent((size_t)g.nkx * 16, (size_t)rows, (size_t)g.nz);
+        if (h2d) {
+            prm.srcPtr = hp; prm.srcPos = hpos; prm.dstPtr = dp; prm.dstPos = dpos;
+            prm.kind = cudaMemcpyHostToDevice;
+        } else {
+            prm.srcPtr = dp; prm.srcPos = dpos; prm.dstPtr = hp; prm.dstPos = hpos;
+            prm.kind = cudaMemcpyDeviceToHost;
+        }
+        CK(cudaMemcpy3DAsync(&prm, ctx->stream));
+    }
+    return QGN_OK;
+}
+
+// host q_hat (kept modes) -> compact device field
+int upload_kept(qgn_ctx* ctx, const double* host, double2* dst) {
+    RET(copy_kept(ctx, const_cast<double*>(host), true));
+    CK(launch_xfer_to_compact(ctx->g, ctx->b.xfer, dst, ctx->stream));
+    return QGN_OK;
+}
+
+// compact device field -> host q_hat (kept modes only)
+int download_kept(qgn_ctx* ctx, const double2* src, double* host) {
+    CK(launch_compact_to_xfer(ctx->g, src, ctx->b.xfer, ctx->stream));
+    RET(copy_kept(ctx, host, false));
+    return QGN_OK;
+}
+
+int ensure_full(qgn_ctx* ctx) {
+    if (!ctx->b.full) CK(dalloc(&ctx->b.full, (size_t)ctx->g.nz * ctx->g.ny * ctx->g.nxh));
+    return QGN_OK;
+}
+
+// compact device field -> whole host q_hat (zeros in the dealiased band)
+int download_full(qgn_ctx* ctx, const double2* src, double* host) {
+    RET(ensure_full(ctx));
+    const Geom& g = ctx->g;
+    CK(launch_compact_to_xfer(g, src, ctx->b.xfer, ctx->stream));
+    CK(launch_xfer_to_full(g, ctx->b.xfer, ctx->b.full, ctx->stream));
+    CK(cudaMemcpyAsync(host, ctx->b.full, sizeof(double2) * (size_t)g.nz * g.ny * g.nxh, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    return QGN_OK;
+}
+
+int read_scalars(qgn_ctx* ctx, DevScalars* out) {
+    CK(cudaMemcpyAsync(ctx->host_pin, ctx->b.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.harvest();
+    std::memcpy(out, ctx->host_pin, sizeof(DevScalars));
+    return QGN_OK;
+}
+
+int write_time(qgn_ctx* ctx, double t, double dt) {
+    // t and dt are the first two members of DevScalars
+    double* pin = ctx->host_pin;
+    CK(cudaStreamSynchronize(ctx->stream));
+    pin[0] = t;
+    pin[1] = dt;
+    CK(cudaMemcpyAsync(ctx->b.sc, pin, 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+bool drag_on(const qgn_ctx* ctx) { return ctx->p.C_d != 0.0; }
+
+double leith_c12(const qgn_params& p) {
+    const double pi = 4.0 * std::atan(1.0);
+    const double x = (double)1.3f * p.Lx / ((double)p.nx * pi);   // default-REAL 1.3 (ARK43_QGLeith.f90:72)
+    const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
+    return x4 * x8;
+}
+
+int rhs_of(qgn_ctx* ctx, const double2* q, const double2* psi, double2* out) {
+    CK(launch_rhs(ctx->g, ctx->b, q, psi, out, drag_on(ctx), ctx->stream));
+    return QGN_OK;
+}
+
+int max_rejects(const qgn_ctx* ctx) { return ctx->p.max_rejects > 0 ? ctx->p.max_rejects : 64; }
+
+// ---- ARK4(3)6L[2]SA, ARK43_QGLeith.f90 / ARK43.f90 ------------------------------------------
+int step_ark(qgn_ctx* ctx, bool leith) {
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    if (leith) CK(launch_leith(g, b, b.q, leith_c12(ctx->p), st));
+    b.Qs[0] = b.q;
+    CK(launch_modal(g, b.mc, b.q, b.psi, st));
+    RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
+    int nrej = 0;
+    for (;;) {
+        for (int s = 1; s < 6; ++s) {
+            CK(launch_ark_stage(g, b, s, st));
+            RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
+        }
+        CK(launch_ark_update(g, b, st));
+        CK(launch_zero_scalar_max(b.sc, st));
+        CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
+        CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, st));
+        DevScalars s;
+        RET(read_scalars(ctx, &s));
+        if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite embedded error estimate");
+        if (s.accept) {
+            std::swap(b.q, b.qnew);
+            b.Qs[0] = b.q;
+            return QGN_OK;
+        }
+        ++ctx->rejects;
+        if (++nrej >= max_rejects(ctx))
+            return set_err(ctx, QGN_ERR_REJECT_LIMIT, "adaptive step rejected max_rejects times in a row");
+    }
+}
+
+// ---- Bogacki-Shampine 3(2), BSRK3.f90 -----------------------------------------------------
+int step_bsrk3(qgn_ctx* ctx) {
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    if (ctx->first_call) {
+        CK(launch_modal(g, b.mc, b.q, b.psi, st));
+        RET(rhs_of(ctx, b.q, b.psi, b.N[0]));     // RHS0 (kept between calls, FSAL)
+        ctx->first_call = false;
+    }
+    int nrej = 0;
+    for (;;) {
+        Combo c1{{b.N[0]}, {0.5}, 1};
+        CK(launch_combo(g, b, c1, b.q, b.Qs[1], b.psi, true, st));
+        RET(rhs_of(ctx, b.Qs[1], b.psi, b.N[1]));
+        Combo c2{{b.N[1]}, {0.75}, 1};
+        CK(launch_combo(g, b, c2, b.q, b.Qs[2], b.psi, true, st));
+        RET(rhs_of(ctx, b.Qs[2], b.psi, b.N[2]));
+        Combo c3{{b.N[0], b.N[1], b.N[2]}, {2.0 / 9.0, 1.0 / 3.0, 4.0 / 9.0}, 3};
+        CK(launch_combo(g, b, c3, b.q, b.Qs[3], b.psi, true, st));
+        RET(rhs_of(ctx, b.Qs[3], b.psi, b.N[3]));
+        Combo ce{{b.N[0], b.N[1], b.N[2], b.N[3]}, {5.0 / 72.0, -1.0 / 12.0, -1.0 / 9.0, 1.0 / 8.0}, 4};
+        CK(launch_lincomb(g, ce, b.err, st));
+        CK(launch_zero_scalar_max(b.sc, st));
+        CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
+        CK(launch_controller(g, b, 2, ctx->p.TOL, ctx->p.dt_max, st));
+        DevScalars s;
+        RET(read_scalars(ctx, &s));
+        if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite embedded error estimate");
+        if (s.accept) {
+            std::swap(b.q, b.Qs[3]);      // q_hat = q_tmp
+            std::swap(b.N[0], b.N[3]);    // RHS0 = RHS3
+            return QGN_OK;
+        }
+        ++ctx->rejects;
+        if (++nrej >= max_rejects(ctx))
+            return set_err(ctx, QGN_ERR_REJECT_LIMIT, "adaptive step rejected max_rejects times in a row");
+    }
+}
+
+// ---- classic RK4, RK4.f90 -------------------------------------------------------------------
+int step_rk4(qgn_ctx* ctx) {
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    CK(launch_modal(g, b.mc, b.q, b.psi, st));
+    RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
+    Combo c1{{b.N[0]}, {0.5}, 1};
+    CK(launch_combo(g, b, c1, b.q, b.Qs[1], b.psi, true, st));
+    RET(rhs_of(ctx, b.Qs[1], b.psi, b.N[1]));
+    Combo c2{{b.N[1]}, {0.5}, 1};
+    CK(launch_combo(g, b, c2, b.q, b.Qs[2], b.psi, true, st));
+    RET(rhs_of(ctx, b.Qs[2], b.psi, b.N[2]));
+    Combo c3{{b.N[2]}, {1.0}, 1};
+    CK(launch_combo(g, b, c3, b.q, b.Qs[3], b.psi, true, st));
+    RET(rhs_of(ctx, b.Qs[3], b.psi, b.N[3]));
+    Combo cu{{b.N[0], b.N[1], b.N[2], b.N[3]}, {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0}, 4};
+    CK(launch_combo(g, b, cu, b.q, b.qnew, nullptr, false, st));
+    std::swap(b.q, b.qnew);
+    CK(launch_advance_time(b.sc, st));
+    return QGN_OK;
+}
+
+// ---- AB3 with Euler / AB2 start-up, AB3.f90 -------------------------------------------------
+int step_ab3(qgn_ctx* ctx) {
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    CK(launch_modal(g, b.mc, b.q, b.psi, st));
+    if (ctx->ab_calls == 0) {
+        RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
+        Combo c{{b.N[0]}, {1.0}, 1};
+        CK(launch_combo(g, b, c, b.q, b.qnew, nullptr, false, st));
+    } else if (ctx->ab_calls == 1) {
+        RET(rhs_of(ctx, b.q, b.psi, b.N[1]));
+        Combo c{{b.N[1], b.N[0]}, {1.5, -0.5}, 2};
+        CK(launch_combo(g, b, c, b.q, b.qnew, nullptr, false, st));
+    } else {
+        RET(rhs_of(ctx, b.q, b.psi, b.N[2]));
+        Combo c{{b.N[2], b.N[1], b.N[0]}, {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}, 3};
+        CK(launch_combo(g, b, c, b.q, b.qnew, nullptr, false, st));
+        double2* old0 = b.N[0];
+        b.N[0] = b.N[1];
+        b.N[1] = b.N[2];
+        b.N[2] = old0;
+    }
+    ++ctx->ab_calls;
+    std::swap(b.q, b.qnew);
+    CK(launch_advance_time(b.sc, st));
+    return QGN_OK;
+}
+
+int step_once(qgn_ctx* ctx) {
+    switch (ctx->scheme) {
+        case QGN_SCHEME_ARK43_QGLEITH: return step_ark(ctx, true);
+        case QGN_SCHEME_ARK43: return step_ark(ctx, false);
+        case QGN_SCHEME_BSRK3: return step_bsrk3(ctx);
+        case QGN_SCHEME_RK4: return step_rk4(ctx);
+        case QGN_SCHEME_AB3: return step_ab3(ctx);
+        default: return set_err(ctx, QGN_ERR_CONFIG, "unknown scheme");
+    }
+}
+
+int check_state(qgn_ctx* ctx) {
+    DevScalars s;
+    CK(launch_nonfinite_check(ctx->g, ctx->b.q, ctx->b.sc, ctx->stream));
+    RET(read_scalars(ctx, &s));
+    if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite values in the state q_hat");
+    return QGN_OK;
+}
+
+int advance_n(qgn_ctx* ctx, int nsteps) {
+    for (int i = 0; i < nsteps; ++i) RET(step_once(ctx));
+    return QGN_OK;
+}
+
+bool finite_all(const double* a, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+void free_all(qgn_ctx* ctx) {
+    ctx->prof.release();
+    // stage buffers are swapped between roles while stepping, so memory is released
+    // through the ownership list recorded at creation, never through the role pointers
+    for (void* p : ctx->owned) cudaFree(p);
+    ctx->owned.clear();
+    Buffers& b = ctx->b;
+    if (b.full) cudaFree(b.full);
+    if (b.phys) cudaFree(b.phys);
+    if (b.diag) cudaFree(b.diag);
+    b = Buffers{};
+    if (ctx->host_pin) cudaFreeHost(ctx->host_pin);
+    ctx->host_pin = nullptr;
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = nullptr;
+}
+
+}  // namespace
+
+// ============================================================================================
+extern "C" {
+
+int qgn_create(const qgn_params* p, const double* H, const double* S, const double* uBar, const double* qyBar,
+               const double* Modes, const double* EVals, int scheme, int precision, qgn_ctx** out) {
+    if (!out) return QGN_ERR_ARG;
+    *out = nullptr;
+    if (!p || !H || !uBar || !qyBar || !Modes || !EVals) return QGN_ERR_ARG;
+    if (!is_pow2(p->nx) || !is_pow2(p->ny) || p->nx < 16 || p->ny < 16 || p->nx > 2048 || p->ny > 2048)
+        return QGN_ERR_CONFIG;
+    if (p->nz < 2 || p->nz > kMaxNZ) return QGN_ERR_CONFIG;
+    if (scheme < 0 || scheme > 4) return QGN_ERR_CONFIG;
+    if (precision != QGN_PREC_FP64) return QGN_ERR_CONFIG;
+    if (!(p->Lx > 0) || !(p->Ly > 0) || !(p->Htot > 0)) return QGN_ERR_CONFIG;
+    const int nz = p->nz;
+    if (!finite_all(H, nz) || !finite_all(uBar, nz) || !finite_all(qyBar, nz) || !finite_all(Modes, (size_t)nz * nz) ||
+        !finite_all(EVals, nz) || (S && !finite_all(S, nz + 1)))
+        return QGN_ERR_CONFIG;
+    for (int k = 0; k < nz; ++k)
+        if (!(H[k] > 0)) return QGN_ERR_CONFIG;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return QGN_ERR_NO_DEVICE;
+    }
+    qgn_ctx* ctx = new (std::nothrow) qgn_ctx();
+    if (!ctx) return QGN_ERR_CUDA;
+    ctx->p = *p;
+    ctx->scheme = scheme;
+    ctx->precision = precision;
+    cudaGetDevice(&ctx->device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || prop.major != 10) {
+        delete ctx;
+        return QGN_ERR_NO_DEVICE;
+    }
+    ctx->H.assign(H, H + nz);
+    ctx->uBar.assign(uBar, uBar + nz);
+    ctx->qyBar.assign(qyBar, qyBar + nz);
+    ctx->Modes.assign(Modes, Modes + (size_t)nz * nz);
+    ctx->EVals.assign(EVals, EVals + nz);
+
+    Geom& g = ctx->g;
+    g.nx = p->nx; g.ny = p->ny; g.nz = nz; g.nxh = p->nx / 2 + 1;
+    g.nkx = p->nx / 3;
+    g.kylo = p->ny / 3;
+    g.kyshift = p->ny / 3 + 1;
+    g.nky = p->ny - p->ny / 3 - 1;
+    g.nkxp = (g.nkx + 3) / 4 * 4;
+    const double pi = 4.0 * std::atan(1.0);
+    g.dkx = 2.0 * pi / p->Lx;
+    g.dky = 2.0 * pi / p->Ly;
+    g.inv_nxny = 1.0 / ((double)p->nx * (double)p->ny);
+
+    Buffers& b = ctx->b;
+    int rc = QGN_OK;
+    auto fail = [&](const char* what, cudaError_t e) {
+        rc = cuda_err(ctx, what, e);
+    };
+#define AL(ptr, n)                                   \
+    if (rc == QGN_OK) {                              \
+        cudaError_t _e = dalloc(&(ptr), (n));        \
+        if (_e != cudaSuccess) fail(#ptr, _e);       \
+        else ctx->owned.push_back((void*)(ptr));     \
+    }
+    const size_t C = g.csize(), Hh = g.hsize();
+    AL(b.q, C); AL(b.qnew, C); AL(b.psi, C); AL(b.err, C);
+    for (int j = 0; j < 6; ++j) AL(b.N[j], C);
+    for (int j = 1; j < 6; ++j) AL(b.Qs[j], C);
+    AL(b.hq, Hh); AL(b.hp, Hh); AL(b.hu, Hh); AL(b.huq, Hh); AL(b.hvq, Hh);
+    AL(b.hdu, (size_t)g.ny * g.nkxp); AL(b.hdv, (size_t)g.ny * g.nkxp);
+    AL(b.xfer, C);
+    AL(b.twx, (size_t)g.nx); AL(b.twy, (size_t)g.ny);
+    AL(b.red, (size_t)512 * kMaxNZ);
+    AL(b.Hw, (size_t)kMaxNZ);
+    AL(b.lc, 1); AL(b.mc, 1); AL(b.sc, 1);
+#undef AL
+    if (rc == QGN_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) fail("cudaStreamCreate", e);
+    }
+    if (rc == QGN_OK) {
+        cudaError_t e = cudaMallocHost((void**)&ctx->host_pin, sizeof(DevScalars) + 64);
+        if (e != cudaSuccess) fail("cudaMallocHost", e);
+    }
+    if (rc == QGN_OK) {
+        // zero everything once: padding columns of the half fields stay zero forever
+        double2* zs[] = {b.q, b.qnew, b.psi, b.err, b.hq, b.hp, b.hu, b.huq, b.hvq};
+        for (double2* z : zs) {
+            cudaError_t e = cudaMemset(z, 0, sizeof(double2) * ((z == b.hq || z == b.hp || z == b.hu || z == b.huq ||
+                                                                   z == b.hvq) ? Hh : C));
+            if (e != cudaSuccess) { fail("cudaMemset", e); break; }
+        }
+        for (int j = 0; j < 6 && rc == QGN_OK; ++j) {
+            cudaError_t e = cudaMemset(b.N[j], 0, sizeof(double2) * C);
+            if (e == cudaSuccess && j > 0) e = cudaMemset(b.Qs[j], 0, sizeof(double2) * C);
+            if (e != cudaSuccess) fail("cudaMemset", e);
+        }
+        if (rc == QGN_OK) {
+            cudaError_t e = cudaMemset(b.hdu, 0, sizeof(double2) * g.ny * g.nkxp);
+            if (e == cudaSuccess) e = cudaMemset(b.hdv, 0, sizeof(double2) * g.ny * g.nkxp);
+            if (e != cudaSuccess) fail("cudaMemset", e);
+        }
+    }
+    if (rc == QGN_OK) {
+        std::vector<double2> tw;
+        make_twiddles(g.nx, tw);
+        cudaError_t e = cudaMemcpy(b.twx, tw.data(), sizeof(double2) * g.nx, cudaMemcpyHostToDevice);
+        make_twiddles(g.ny, tw);
+        if (e == cudaSuccess) e = cudaMemcpy(b.twy, tw.data(), sizeof(double2) * g.ny, cudaMemcpyHostToDevice);
+        LayerConst lc;
+        std::memset(&lc, 0, sizeof(lc));
+        for (int k = 0; k < nz; ++k) {
+            lc.uBar[k] = uBar[k];
+            lc.betaq[k] = p->beta + qyBar[k];
+        }
+        lc.ekman = p->r0 * p->Htot / H[nz - 1];
+        lc.dragc = p->C_d * p->Htot / H[nz - 1];
+        lc.A2 = p->A2;
+        lc.A8 = p->A8;
+        lc.explicit_diss = p->is_explicit ? 1 : 0;
+        ModalConst mc;
+        std::memset(&mc, 0, sizeof(mc));
+        for (int k = 0; k < nz; ++k) {
+            for (int kk = 0; kk < nz; ++kk) {
+                mc.proj[k * nz + kk] = H[kk] * Modes[kk + (size_t)k * nz];   // H(kk)*Modes(kk,k)
+                mc.back[k * nz + kk] = Modes[k + (size_t)kk * nz];          // Modes(k,kk)
+            }
+            mc.evals[k] = EVals[k];
+        }
+        mc.Htot = p->Htot;
+        DevScalars sc;
+        std::memset(&sc, 0, sizeof(sc));
+        sc.err0 = p->TOL;   // FirstCall: err0 = TOL (ARK43*.f90:17), r0 = TOL (BSRK3.f90:15)
+        for (int k = 0; k < nz; ++k) sc.A8L[k] = p->A8;
+        double Hw[kMaxNZ] = {0};
+        for (int k = 0; k < nz; ++k) Hw[k] = H[k] / p->Htot;
+        if (e == cudaSuccess) e = cudaMemcpy(b.lc, &lc, sizeof(lc), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b.mc, &mc, sizeof(mc), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b.Hw, Hw, sizeof(Hw), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) fail("constant upload", e);
+    }
+    if (rc != QGN_OK) {
+        free_all(ctx);
+        delete ctx;
+        return rc;
+    }
+    b.Qs[0] = b.q;
+    *out = ctx;
+    return QGN_OK;
+}
+
+int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_hat) return set_err(ctx, QGN_ERR_ARG, "q_hat is NULL");
+    CK(cudaSetDevice(ctx->device));
+    RET(upload_kept(ctx, q_hat, ctx->b.q));
+    ctx->b.Qs[0] = ctx->b.q;
+    RET(write_time(ctx, t, dt));
+    return QGN_OK;
+}
+
+int qgn_get_time(qgn_ctx* ctx, double* t, double* dt) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    DevScalars s;
+    RET(read_scalars(ctx, &s));
+    if (t) *t = s.t;
+    if (dt) *dt = s.dt;
+    return QGN_OK;
+}
+
+int qgn_get_state(qgn_ctx* ctx, double* q_hat, double* t, double* dt) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    CK(cudaSetDevice(ctx->device));
+    if (q_hat) RET(download_full(ctx, ctx->b.q, q_hat));
+    return qgn_get_time(ctx, t, dt);
+}
+
+int qgn_advance_resident(qgn_ctx* ctx, int nsteps) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
+    CK(cudaSetDevice(ctx->device));
+    RET(advance_n(ctx, nsteps));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.harvest();
+    return QGN_OK;
+}
+
+int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_hat || !t || !dt) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
+    if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
+    RET(qgn_set_state(ctx, q_hat, *t, *dt));
+    RET(advance_n(ctx, nsteps));
+    RET(check_state(ctx));
+    RET(download_kept(ctx, ctx->b.q, q_hat));
+    DevScalars s;
+    RET(read_scalars(ctx, &s));
+    *t = s.t;
+    *dt = s.dt;
+    return QGN_OK;
+}
+
+int qgn_step(qgn_ctx* ctx, double* q_hat, double* t, double* dt) { return qgn_advance(ctx, q_hat, t, dt, 1); }
+
+int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_hat || !rhs) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(ctx->device));
+    Buffers& b = ctx->b;
+    RET(upload_kept(ctx, q_hat, b.err));
+    CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
+    RET(rhs_of(ctx, b.err, b.psi, b.qnew));
+    RET(download_full(ctx, b.qnew, rhs));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+int qgn_psi(qgn_ctx* ctx, const double* q_hat, double* psi_hat) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_hat || !psi_hat) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(ctx->device));
+    Buffers& b = ctx->b;
+    RET(upload_kept(ctx, q_hat, b.err));
+    CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
+    RET(download_full(ctx, b.psi, psi_hat));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+int qgn_leith(qgn_ctx* ctx, double* A8L) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!A8L) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(ctx->device));
+    CK(launch_leith(ctx->g, ctx->b, ctx->b.q, leith_c12(ctx->p), ctx->stream));
+    DevScalars s;
+    RET(read_scalars(ctx, &s));
+    std::memcpy(A8L, s.A8L, sizeof(double) * ctx->g.nz);
+    return QGN_OK;
+}
+
+int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!ke_layer) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
+    if (spectrum && nbins <= 0) return set_err(ctx, QGN_ERR_ARG, "nbins <= 0");
+    CK(cudaSetDevice(ctx->device));
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    const size_t need = (size_t)g.nz * (1 + (spectrum ? nbins : 0));
+    if (b.diag) { cudaFree(b.diag); b.diag = nullptr; }
+    CK(dalloc(&b.diag, need));
+    CK(launch_modal(g, b.mc, b.q, b.psi, ctx->stream));
+    CK(launch_ke(g, b, b.psi, b.Hw, b.diag, ctx->stream));
+    if (spectrum) CK(launch_ke_spectrum(g, b.psi, b.Hw, nbins, b.diag + g.nz, ctx->stream));
+    CK(cudaMemcpyAsync(ke_layer, b.diag, sizeof(double) * g.nz, cudaMemcpyDeviceToHost, ctx->stream));
+    if (spectrum)
+        CK(cudaMemcpyAsync(spectrum, b.diag + g.nz, sizeof(double) * (size_t)g.nz * nbins, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_phys) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    CK(cudaSetDevice(ctx->device));
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    const size_t np = (size_t)g.nz * g.ny * g.nx;
+    if (!b.phys) CK(dalloc(&b.phys, np));
+    const double2* src = b.q;
+    if (q_hat) {
+        RET(upload_kept(ctx, q_hat, b.err));
+        src = b.err;
+    }
+    if (q_phys) {
+        CK(launch_to_phys(g, b, src, b.phys, ctx->stream));
+        CK(cudaMemcpyAsync(q_phys, b.phys, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (psi_phys) {
+        CK(launch_modal(g, b.mc, src, b.psi, ctx->stream));
+        CK(launch_to_phys(g, b, b.psi, b.phys, ctx->stream));
+        CK(cudaMemcpyAsync(psi_phys, b.phys, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+int qgn_set_state_physical(qgn_ctx* ctx, const double* q_phys, double t, double dt) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_phys) return set_err(ctx, QGN_ERR_ARG, "q_phys is NULL");
+    CK(cudaSetDevice(ctx->device));
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    const size_t np = (size_t)g.nz * g.ny * g.nx;
+    if (!b.phys) CK(dalloc(&b.phys, np));
+    CK(cudaMemcpyAsync(b.phys, q_phys, sizeof(double) * np, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_from_phys(g, b, b.phys, b.q, ctx->stream));
+    b.Qs[0] = b.q;
+    RET(write_time(ctx, t, dt));
+    return QGN_OK;
+}
+
+int qgn_profile_enable(qgn_ctx* ctx, int enable) {
+    if (!ctx) return QGN_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.reset();
+    ctx->prof.timing = enable != 0;
+    return QGN_OK;
+}
+
+int qgn_profile_read(qgn_ctx* ctx, int kernel, double* total_ms, double* bytes, long long* timed,
+                     long long* launches) {
+    if (!ctx) return QGN_ERR_ARG;
+    if (kernel < 0 || kernel >= KID_COUNT) return set_err(ctx, QGN_ERR_ARG, "kernel id out of range");
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.harvest();
+    if (total_ms) *total_ms = ctx->prof.total_ms[kernel];
+    if (bytes) *bytes = ctx->prof.bytes[kernel];
+    if (timed) *timed = ctx->prof.timed[kernel];
+    if (launches) *launches = ctx->prof.launches[kernel];
+    return QGN_OK;
+}
+
+const char* qgn_kernel_name(int kernel) {
+    static const char* names[KID_COUNT] = {"modal", "yinv", "xpass", "yfwd", "xinv1", "xfwd1", "yfwd1",
+                                           "ark_stage", "ark_update", "combo", "lincomb", "parseval",
+                                           "scalar", "layout"};
+    if (kernel < 0 || kernel >= KID_COUNT) return "";
+    return names[kernel];
+}
+
+int qgn_stream(qgn_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return QGN_ERR_ARG;
+    *stream = (void*)ctx->stream;
+    return QGN_OK;
+}
+
+int qgn_rejects(qgn_ctx* ctx, long long* count) {
+    if (!ctx || !count) return QGN_ERR_ARG;
+    *count = ctx->rejects;
+    return QGN_OK;
+}
+
+const char* qgn_last_error(const qgn_ctx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->last_error.c_str();
+}
+
+int qgn_destroy(qgn_ctx* ctx) {
+    if (!ctx) return QGN_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+    return QGN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// qgn_internal.cuh -- device data layout, context and launch wrappers of the QGN path.
+//
+// HBM layout (all FP64 complex = double2):
+//   compact spectral field  [nz][nkx][nky]   -- only the modes DeAlias keeps
+//       (QGN_Module.f90:194-204): kx index i in [0, nx/3), ky index j in
+//       [0, ny/3) U [2(ny/3)+1, ny); compact m < ny/3 -> j = m, else j = m + ny/3 + 1.
+//       ky is the contiguous axis so the y transforms stream whole columns.
+//   half-transformed field  [nz][ny][nkxp]   -- x still spectral (kept kx only), y physical;
+//       the row layout the x pass streams.  nkxp = nkx rounded up to a multiple of 4.
+//   Mode (0,0) of every compact field is held at zero, as DeAlias does.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include "../../include/qgn_gpu.h"
+#include "prof.cuh"
+
+namespace qgn {
+
+constexpr int kMaxNZ = 32;
+constexpr int kTKX = 4;   // kx columns per CTA in the y-pass kernels
+
+struct Geom {
+    int nx, ny, nz, nxh;
+    int nkx, nky, kylo, kyshift, nkxp;
+    double dkx, dky, inv_nxny;
+    __host__ __device__ size_t csize() const { return (size_t)nz * nkx * nky; }
+    __host__ __device__ size_t hsize() const { return (size_t)nz * ny * nkxp; }
+    __host__ __device__ int jfull(int m) const { return m < kylo ? m : m + kyshift; }
+    __host__ __device__ double kyval(int j) const { return dky * (double)(j <= ny / 2 ? j : j - ny); }
+};
+
+// Per-layer physical constants of the RHS (QGN_Module.f90:268-292).
+struct LayerConst {
+    double uBar[kMaxNZ];
+    double betaq[kMaxNZ];   // beta + qyBar(k)
+    double ekman;           // r0*Htot/H(nz)
+    double dragc;           // C_d*Htot/H(nz)
+    double A2, A8;
+    int explicit_diss;
+};
+
+// Modal-inversion coefficients (GetPsi, QGN_Module.f90:315-341).
+struct ModalConst {
+    double proj[kMaxNZ * kMaxNZ];   // proj[k*nz+kk] = H(kk)*Modes(kk,k)
+    double back[kMaxNZ * kMaxNZ];   // back[k*nz+kk] = Modes(k,kk)
+    double evals[kMaxNZ];
+    double Htot;
+};
+
+// Device scalars of the adaptive controllers.
+struct DevScalars {
+    double t, dt, err0, err1;
+    unsigned long long maxbits;   // bit pattern of max|err_phys| (non-negative doubles)
+    int accept;                   // 1 accepted, 0 rejected
+    int nonfinite;
+    double A8L[kMaxNZ];
+};
+
+struct Buffers {
+    double2* q = nullptr;        // state q_hat (compact)
+    double2* qnew = nullptr;     // candidate update
+    double2* N[6] = {};          // stage right-hand sides
+    double2* Qs[6] = {};         // stage states (Qs[0] aliases q for the ARK schemes)
+    double2* psi = nullptr;      // psi of the field being evaluated
+    double2* err = nullptr;      // error combination (compact)
+    double2* hq = nullptr;       // half-transformed q, psi, u   [nz][ny][nkxp]
+    double2* hp = nullptr;
+    double2* hu = nullptr;
+    double2* huq = nullptr;      // half-transformed u*q, v*q
+    double2* hvq = nullptr;
+    double2* hdu = nullptr;      // half-transformed |u|u, |u|v of the bottom layer [ny][nkxp]
+    double2* hdv = nullptr;
+    double2* xfer = nullptr;     // host-order kept modes [nz][nky][nkx]
+    double2* full = nullptr;     // full CCE field [nz][ny][nxh] (lazy)
+    double* phys = nullptr;      // physical field [nz][ny][nx] (lazy)
+    double2* twx = nullptr;      // twiddles exp(-2 pi i m/nx)
+    double2* twy = nullptr;      // twiddles exp(-2 pi i m/ny)
+    double* red = nullptr;       // reduction partials
+    double* Hw = nullptr;        // H(k)/Htot per layer
+    double* diag = nullptr;      // diagnostics output (lazy)
+    LayerConst* lc = nullptr;
+    ModalConst* mc = nullptr;
+    DevScalars* sc = nullptr;
+};
+
+}  // namespace qgn
+
+struct qgn_ctx {
+    qgn_params p{};
+    int scheme = 0, precision = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    qgn::Geom g{};
+    qgn::Buffers b{};
+    std::vector<double> H, uBar, qyBar, Modes, EVals;
+    // stepper memory (the reference's `save` variables); BSRK3's RHS0 and AB3's history
+    // live in b.N[0..1], err0 / r0 in the device scalars
+    bool first_call = true;
+    int ab_calls = 0;
+    long long rejects = 0;
+    double* host_pin = nullptr;    // pinned scalar readback
+    std::vector<void*> owned;      // every device allocation made at creation
+    std::string last_error;
+    qgn::Prof prof;                // launch counts and per-kernel event timing
+};
+
+namespace qgn {
+
+// ---- launch wrappers (rhs_kernels.cu) -------------------------------------------------
+cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, double2* psi, cudaStream_t s);
+cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
+                       bool do_drag, cudaStream_t s);
+// y-inverse + x-pass of one compact field with a max|.| reduction into sc->maxbits
+cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s);
+// physical field (c2r/(nx*ny)) of a compact field into b.phys ([nz][ny][nx])
+cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, double* out, cudaStream_t s);
+// forward transform + dealias of a physical field [nz][ny][nx] into a compact field
+cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys, double2* out, cudaStream_t s);
+
+// ---- layout kernels (layout.cu) -------------------------------------------------------
+cudaError_t launch_xfer_to_compact(const Geom& g, const double2* xfer, double2* c, cudaStream_t s);
+cudaError_t launch_compact_to_xfer(const Geom& g, const double2* c, double2* xfer, cudaStream_t s);
+cudaError_t launch_xfer_to_full(const Geom& g, const double2* xfer, double2* full, cudaStream_t s);
+cudaError_t launch_nonfinite_check(const Geom& g, const double2* c, DevScalars* sc, cudaStream_t s);
+
+// ---- stepper kernels (stepper.cu) -----------------------------------------------------
+struct Combo {
+    const double2* R[4];
+    double a[4];
+    int n;
+};
+cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t s);
+cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
+cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t s);
+cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const double2* q, double2* out,
+                         double2* psi, bool want_psi, cudaStream_t s);
+cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStream_t s);
+cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, cudaStream_t s);
+cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t s);
+cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t s);
+cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t s);
+cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* Hw, int nbins, double* spec,
+                               cudaStream_t s);
+
+}  // namespace qgn

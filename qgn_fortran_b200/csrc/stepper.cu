@@ -1,0 +1,465 @@
+// stepper.cu -- stage combinations, implicit solve, QG-Leith, error norm and PI controllers.
+//
+// The ARK4(3)6L[2]SA stage kernel fuses, per kept mode and for all layers at once:
+//   L_j = -(A2 k^2 + A8L_k k^8) q_j                        (ARK43_QGLeith.f90:77-118)
+//   q_s = Mq (q + dt (sum_j ae_sj N_j + sum_j ai_sj L_j)),  Mq = 1/(1 + dt/4 (A2 k^2 + A8L_k k^8))
+//   psi_s = GetPsi(q_s)                                     (QGN_Module.f90:315-341)
+// so the next RHS starts from q_s and psi_s without another pass.  L_j is recomputed from
+// the stored stage state q_j instead of being stored.  dt, t and the controller memory live
+// in device scalars so a whole step can be replayed without host round trips.
+#include "qgn_internal.cuh"
+#include "prof.cuh"
+
+namespace qgn {
+
+// ARK4(3)6L[2]SA tableau, ARK43_QGLeith.f90:18-58 (exact rationals rounded once).
+__constant__ double c_ae[36] = {
+    0, 0, 0, 0, 0, 0,
+    0.5, 0, 0, 0, 0, 0,
+    13861.0 / 62500.0, 6889.0 / 62500.0, 0, 0, 0, 0,
+    -116923316275.0 / 2393684061468.0, -2731218467317.0 / 15368042101831.0, 9408046702089.0 / 11113171139209.0, 0, 0, 0,
+    -451086348788.0 / 2902428689909.0, -2682348792572.0 / 7519795681897.0, 12662868775082.0 / 11960479115383.0,
+    3355817975965.0 / 11060851509271.0, 0, 0,
+    647845179188.0 / 3216320057751.0, 73281519250.0 / 8382639484533.0, 552539513391.0 / 3454668386233.0,
+    3354512671639.0 / 8306763924573.0, 4040.0 / 17871.0, 0};
+__constant__ double c_ai[36] = {
+    0, 0, 0, 0, 0, 0,
+    0.25, 0.25, 0, 0, 0, 0,
+    8611.0 / 62500.0, -1743.0 / 31250.0, 0, 0, 0, 0,
+    5012029.0 / 34652500.0, -654441.0 / 2922500.0, 174375.0 / 388108.0, 0, 0, 0,
+    15267082809.0 / 155376265600.0, -71443401.0 / 120774400.0, 730878875.0 / 902184768.0, 2285395.0 / 8070912.0, 0, 0,
+    82889.0 / 524892.0, 0.0, 15625.0 / 83664.0, 69875.0 / 102672.0, -2260.0 / 8211.0, 0.25};
+__constant__ double c_b[6] = {82889.0 / 524892.0, 0.0, 15625.0 / 83664.0, 69875.0 / 102672.0, -2260.0 / 8211.0, 0.25};
+__constant__ double c_be[6] = {31666707.0 / 9881966720.0, 0.0, -256875.0 / 105007616.0, -2768025.0 / 128864768.0,
+                               169839.0 / 3864644.0, -5247.0 / 225920.0};
+
+template <int NZ>
+__device__ __forceinline__ void modal_invert_s(const double* proj, const double* back, const double* ev, double Htot,
+                                               int nz, double k2, bool mean_mode, const double2* qv, double2* pv) {
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    const int n = NZ > 0 ? NZ : nz;
+    double2 pm[NZC];
+#pragma unroll
+    for (int k = 0; k < NZC; ++k) {
+        if (k < n) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int kk = 0; kk < NZC; ++kk)
+                if (kk < n) {
+                    const double c = proj[k * n + kk];
+                    acc.x += c * qv[kk].x;
+                    acc.y += c * qv[kk].y;
+                }
+            const double den = -k2 + ev[k];
+            pm[k] = mean_mode ? make_double2(0.0, 0.0) : make_double2((acc.x / Htot) / den, (acc.y / Htot) / den);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NZC; ++k) {
+        if (k < n) {
+            double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int kk = 0; kk < NZC; ++kk)
+                if (kk < n) {
+                    const double c = back[k * n + kk];
+                    acc.x += pm[kk].x * c;
+                    acc.y += pm[kk].y * c;
+                }
+            pv[k] = acc;
+        }
+    }
+}
+
+struct StagePtrs {
+    const double2* N[6];
+    const double2* Qs[6];
+};
+
+__device__ __forceinline__ void point_k(const Geom& g, size_t p, int& kx, int& m, double& k2) {
+    kx = (int)(p / g.nky);
+    m = (int)(p % g.nky);
+    const double kxv = g.dkx * kx, kyv = g.kyval(g.jfull(m));
+    k2 = kxv * kxv + kyv * kyv;
+}
+
+// ---- ARK stage s (1..5): q_s and psi_s -----------------------------------------------------
+template <int NZ>
+__global__ void __launch_bounds__(256) k_ark_stage(Geom g, int s, StagePtrs sp, const double2* __restrict__ q,
+                                                   double2* __restrict__ qout, double2* __restrict__ psi,
+                                                   const ModalConst* __restrict__ mc,
+                                                   const LayerConst* __restrict__ lc,
+                                                   const DevScalars* __restrict__ sc) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ], s_a8[kMaxNZ];
+    const int nz = g.nz;
+    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) { s_ev[i] = mc->evals[i]; s_a8[i] = sc->A8L[i]; }
+    __syncthreads();
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double dt = sc->dt;
+    const double A2 = lc->A2;
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    double2 qv[NZC], pv[NZC];
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            const size_t idx = (size_t)l * P + p;
+            const double D = A2 * k2 + s_a8[l] * k8;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int j = 0; j < s; ++j) {
+                const double a = c_ae[s * 6 + j];
+                const double2 n = sp.N[j][idx];
+                acc.x += a * n.x;
+                acc.y += a * n.y;
+            }
+            for (int j = 0; j < s; ++j) {
+                const double a = c_ai[s * 6 + j];
+                const double2 qj = sp.Qs[j][idx];
+                acc.x += a * (-D * qj.x);
+                acc.y += a * (-D * qj.y);
+            }
+            const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
+            const double2 q0 = q[idx];
+            qv[l] = make_double2(Mq * (q0.x + dt * acc.x), Mq * (q0.y + dt * acc.y));
+        }
+    }
+    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            qout[(size_t)l * P + p] = qv[l];
+            psi[(size_t)l * P + p] = pv[l];
+        }
+    }
+}
+
+// ---- ARK update + embedded error combination (ARK43_QGLeith.f90:120-134) ---------------------
+__global__ void __launch_bounds__(256) k_ark_update(Geom g, StagePtrs sp, const double2* __restrict__ q,
+                                                    double2* __restrict__ qnew, double2* __restrict__ err,
+                                                    const LayerConst* __restrict__ lc,
+                                                    const DevScalars* __restrict__ sc) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t total = P * g.nz;
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int l = (int)(e / P);
+    const size_t p = e % P;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double D = lc->A2 * k2 + sc->A8L[l] * k8;
+    const double dt = sc->dt;
+    double2 ec = make_double2(0.0, 0.0), uc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        if (i == 1) continue;   // b(2) = be(2) = 0
+        const double2 n = sp.N[i][e];
+        const double2 qi = sp.Qs[i][e];
+        const double2 nl = make_double2(n.x + (-D * qi.x), n.y + (-D * qi.y));
+        ec.x += c_be[i] * nl.x;
+        ec.y += c_be[i] * nl.y;
+        uc.x += c_b[i] * nl.x;
+        uc.y += c_b[i] * nl.y;
+    }
+    err[e] = ec;
+    const double2 q0 = q[e];
+    qnew[e] = (p == 0) ? make_double2(0.0, 0.0) : make_double2(q0.x + dt * uc.x, q0.y + dt * uc.y);
+}
+
+// ---- explicit combinations: out = q + sum_j (a_j dt) R_j, then optionally psi = GetPsi(out) ---
+template <int NZ>
+__global__ void __launch_bounds__(256) k_combo(Geom g, Combo cb, const double2* __restrict__ q,
+                                               double2* __restrict__ out, double2* __restrict__ psi,
+                                               const ModalConst* __restrict__ mc,
+                                               const DevScalars* __restrict__ sc, int want_psi) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    const int nz = g.nz;
+    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
+    __syncthreads();
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double dt = sc->dt;
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    double2 qv[NZC], pv[NZC];
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            const size_t idx = (size_t)l * P + p;
+            double2 v = q[idx];
+            for (int j = 0; j < cb.n; ++j) {
+                const double c = cb.a[j] * dt;
+                const double2 r = cb.R[j][idx];
+                v.x += c * r.x;
+                v.y += c * r.y;
+            }
+            qv[l] = v;
+        }
+    }
+    if (want_psi) modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            out[(size_t)l * P + p] = qv[l];
+            if (want_psi) psi[(size_t)l * P + p] = pv[l];
+        }
+    }
+}
+
+// ---- linear combination without q: out = sum_j a_j R_j (error spectra) --------------------
+__global__ void k_lincomb(size_t n, Combo cb, double2* __restrict__ out) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    double2 v = make_double2(0.0, 0.0);
+    for (int j = 0; j < cb.n; ++j) {
+        const double2 r = cb.R[j][e];
+        v.x += cb.a[j] * r.x;
+        v.y += cb.a[j] * r.y;
+    }
+    out[e] = v;
+}
+
+// ---- weighted Parseval sums over the full plane, per layer ------------------------------------
+// sum_k w(k) |F_k|^2 with the Hermitian extension of the kept half plane; the kx=0 column
+// uses the Hermitian projection (f(ky) + conj f(-ky))/2 that the reference's c2r applies.
+// POW selects the weight (k^2)^POW.
+template <int POW>
+__device__ __forceinline__ double kpow(double k2) {
+    if (POW == 1) return k2;
+    const double k4 = k2 * k2;
+    return k4 * k4;
+}
+
+template <int POW>
+__global__ void __launch_bounds__(256) k_parseval(Geom g, const double2* __restrict__ f, double* __restrict__ partial) {
+    __shared__ double red[8];
+    const size_t P = (size_t)g.nkx * g.nky;
+    for (int l = 0; l < g.nz; ++l) {
+        double acc = 0.0;
+        for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+            int kx, m;
+            double k2;
+            point_k(g, p, kx, m, k2);
+            const double w = kpow<POW>(k2);
+            const double2 v = f[(size_t)l * P + p];
+            if (kx > 0) {
+                acc += 2.0 * w * (v.x * v.x + v.y * v.y);
+            } else {
+                const int j = g.jfull(m);
+                const int jp = (g.ny - j) % g.ny;
+                const bool pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
+                double2 fp = make_double2(0.0, 0.0);
+                if (pk) fp = f[(size_t)l * P + (jp < g.kylo ? jp : jp - g.kyshift)];
+                const double hx = 0.5 * (v.x + fp.x), hy = 0.5 * (v.y - fp.y);
+                acc += (pk ? 1.0 : 2.0) * w * (hx * hx + hy * hy);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+            partial[(size_t)blockIdx.x * g.nz + l] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// A8L(k) = (1.3*Lx/(nx*pi))**12 * sqrt(mean(q*d))  with mean(q*d) = S/(nx ny)^2  (ARK43_QGLeith.f90:71-73)
+__global__ void k_leith_final(Geom g, const double* __restrict__ partial, int nblocks, double c12, DevScalars* sc) {
+    const int l = threadIdx.x;
+    if (l >= g.nz) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * g.nz + l];
+    const double N = (double)g.nx * (double)g.ny;
+    sc->A8L[l] = c12 * sqrt((s / N) / N);
+}
+
+// layer KE = 0.5 * S/(nx ny)^2 * H_k/Htot with S the k^2-weighted Parseval sum of psi
+__global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nblocks, const double* __restrict__ Hw,
+                           double* __restrict__ ke) {
+    const int l = threadIdx.x;
+    if (l >= g.nz) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * g.nz + l];
+    const double N = (double)g.nx * (double)g.ny;
+    ke[l] = 0.5 * ((s / N) / N) * Hw[l];
+}
+
+// isotropic KE spectrum per layer in integer shells round(sqrt(i^2 + jj^2))
+__global__ void k_ke_spectrum(Geom g, const double2* __restrict__ psi, const double* __restrict__ Hw, int nbins,
+                              double* __restrict__ spec) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t total = P * g.nz;
+    const double N = (double)g.nx * (double)g.ny;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int l = (int)(e / P);
+        const size_t p = e % P;
+        int kx, m;
+        double k2;
+        point_k(g, p, kx, m, k2);
+        const int j = g.jfull(m);
+        const int jj = j <= g.ny / 2 ? j : j - g.ny;
+        const int bin = (int)floor(sqrt((double)kx * kx + (double)jj * jj) + 0.5);
+        if (bin >= nbins) continue;
+        const double2 v = psi[e];
+        double c;
+        if (kx > 0) {
+            c = 2.0 * k2 * (v.x * v.x + v.y * v.y);
+        } else {
+            const int jp = (g.ny - j) % g.ny;
+            const bool pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
+            double2 fp = make_double2(0.0, 0.0);
+            if (pk) fp = psi[(size_t)l * P + (jp < g.kylo ? jp : jp - g.kyshift)];
+            const double hx = 0.5 * (v.x + fp.x), hy = 0.5 * (v.y - fp.y);
+            c = (pk ? 1.0 : 2.0) * k2 * (hx * hx + hy * hy);
+        }
+        atomicAdd(&spec[(size_t)l * nbins + bin], 0.5 * c / N / N * Hw[l]);
+    }
+}
+
+// ---- PI controllers (ARK43_QGLeith.f90:124-138, ARK43.f90:108-124, BSRK3.f90:35-48) ----------
+// kind 0: ARK43_QGLeith (reject x0.5, safety 0.2); 1: ARK43 (x0.75, 0.75); 2: BSRK3.
+__global__ void k_controller(int kind, double inv_n, double TOL, double dt_max, DevScalars* sc) {
+    const double M = __longlong_as_double((long long)sc->maxbits);
+    const double dt = sc->dt;
+    double err1;
+    if (kind == 2) err1 = dt * (M * inv_n);
+    else err1 = dt * M * inv_n;
+    sc->err1 = err1;
+    if (!(err1 == err1) || isinf(err1)) {
+        sc->nonfinite = 1;
+        sc->accept = 0;
+        return;
+    }
+    if (err1 > TOL) {
+        sc->dt = (kind == 0 ? 0.5 : 0.75) * dt;
+        sc->accept = 0;
+        return;
+    }
+    sc->accept = 1;
+    sc->t = sc->t + dt;
+    const double err0 = sc->err0;
+    double nd;
+    if (kind == 0) nd = dt * pow(0.2 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
+    else if (kind == 1) nd = dt * pow(0.75 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
+    else nd = dt * pow(0.75 * TOL / err1, 0.1) * pow(err0 / err1, 0.4 / 3.0);
+    sc->dt = nd < dt_max ? nd : dt_max;
+    sc->err0 = err1;
+}
+
+__global__ void k_zero_max(DevScalars* sc) {
+    sc->maxbits = 0ULL;
+    sc->accept = 0;
+}
+
+__global__ void k_advance_time(DevScalars* sc) { sc->t = sc->t + sc->dt; }
+
+// ------------------------------------------------------------------------------------------
+// launch wrappers
+// ------------------------------------------------------------------------------------------
+static inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    StagePtrs sp{};
+    for (int j = 0; j < 6; ++j) { sp.N[j] = b.N[j]; sp.Qs[j] = b.Qs[j]; }
+    const size_t P = (size_t)g.nkx * g.nky;
+    dim3 grid(blocks_for(P, 256));
+    const double nb = 16.0 * (double)g.csize() * (2.0 * s + 2.0);
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<2><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<4><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<8><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<16><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<0><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t st) {
+    StagePtrs sp{};
+    for (int j = 0; j < 6; ++j) { sp.N[j] = b.N[j]; sp.Qs[j] = b.Qs[j]; }
+    QGN_LAUNCH(KID_UPDATE, 12.0 * 16.0 * (double)g.csize(), st,
+               k_ark_update<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const double2* q, double2* out,
+                         double2* psi, bool want_psi, cudaStream_t st) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    dim3 grid(blocks_for(P, 256));
+    const int wp = want_psi ? 1 : 0;
+    const double nb = 16.0 * (double)g.csize() * (1.0 + cb.n + 1.0 + wp);
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<2><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 4: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<4><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 8: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<8><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 16: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<16><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        default: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<0><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStream_t st) {
+    QGN_LAUNCH(KID_LINCOMB, 16.0 * (double)g.csize() * (cb.n + 1.0), st,
+               k_lincomb<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g.csize(), cb, out));
+    return cudaGetLastError();
+}
+
+static int parseval_blocks(const Geom& g) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    size_t nb = (P + 255) / 256;
+    return (int)(nb < 296 ? nb : 296);
+}
+
+cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t st) {
+    const int nb = parseval_blocks(g);
+    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st, k_parseval<4><<<nb, 256, 0, st>>>(g, q, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_leith_final<<<1, 32, 0, st>>>(g, b.red, nb, c12, b.sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t st) {
+    const int nb = parseval_blocks(g);
+    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st, k_parseval<1><<<nb, 256, 0, st>>>(g, psi, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_ke_final<<<1, 32, 0, st>>>(g, b.red, nb, Hw, ke));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* Hw, int nbins, double* spec,
+                               cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(spec, 0, sizeof(double) * (size_t)nbins * g.nz, st);
+    if (e != cudaSuccess) return e;
+    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
+               k_ke_spectrum<<<148 * 8, 256, 0, st>>>(g, psi, Hw, nbins, spec));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_controller<<<1, 1, 0, st>>>(kind, g.inv_nxny, TOL, dt_max, b.sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_zero_max<<<1, 1, 0, st>>>(sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_advance_time<<<1, 1, 0, st>>>(sc));
+    return cudaGetLastError();
+}
+
+}  // namespace qgn

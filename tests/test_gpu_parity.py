@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the FP64 oracle.
+
+Tolerance: per-layer relative L2 <= 1e-12 for one RHS, GetPsi, the transforms and the
+first steps; trajectories over 100 fixed-dt steps <= 1e-11.  t and dt sequences of the
+adaptive schemes agree to 1e-12 relative (the controller's pow() may differ by an ulp).
+"""
+import glob
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.qgn_oracle import Params, QGNOracle, SCHEMES
+from qgn_fortran_b200 import QGNModule
+from qgn_fortran_b200._lib import QGNError, QGN_ERR_NONFINITE, QGN_ERR_REJECT_LIMIT
+from qgn_fortran_b200.inputs import exponential_stratification, phillips_two_layer, seeded_random_pv, workload
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+RHS_TOL = 1e-12
+
+
+def layer_rel(a, b):
+    num = np.sqrt(np.sum(np.abs(a - b) ** 2, axis=(1, 2)))
+    den = np.sqrt(np.sum(np.abs(b) ** 2, axis=(1, 2)))
+    return num / np.where(den > 0, den, 1.0)
+
+
+def pair(params: dict, H, S, U, scheme="ark43_qgleith", **kw):
+    m = QGNOracle(Params(**params), H, S, U)
+    g = QGNModule(params, H, S, U, scheme=scheme, **kw)
+    return m, g
+
+
+def strat_params(nx, ny, nz, **kw):
+    p = dict(nx=nx, ny=ny, nz=nz, Lx=2.0e6, Ly=2.0e6 * ny / nx, Htot=4000.0, f0=1.0e-4, beta=2.0e-11,
+             A2=0.0, A8=1.0e20, r0=1.0e-7, C_d=0.0, TOL=1.0e-12, is_explicit=False,
+             dt_max=math.pi / (2.0e-11 * 2.0e6))
+    p.update(kw)
+    return p
+
+
+def golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_case(path):
+    d = np.load(path)
+    meta = json.loads(str(d["meta"]))
+    return d, meta
+
+
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_rhs_psi_leith_golden(cuda_ok, path):
+    d, meta = load_case(path)
+    g = QGNModule(meta["params"], d["H"], d["S"], d["U"], scheme=meta["scheme"])
+    assert np.all(layer_rel(g.get_rhs(d["q0"]), d["rhs"]) <= RHS_TOL)
+    assert np.all(layer_rel(g.get_psi(d["q0"]), d["psi"]) <= RHS_TOL)
+    q0 = g.initialize(d["qp"])
+    assert np.all(layer_rel(q0, d["q0"]) <= RHS_TOL)
+    assert np.allclose(g.leith(), d["a8l"], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_trajectory_golden(cuda_ok, path):
+    d, meta = load_case(path)
+    g = QGNModule(meta["params"], d["H"], d["S"], d["U"], scheme=meta["scheme"])
+    q = np.ascontiguousarray(d["q0"]).copy()
+    t, dt = 0.0, meta["dt0"]
+    for k in range(meta["nsteps"]):
+        t, dt = g.time_step(q, t, dt)
+        assert t == pytest.approx(d["t"][k], rel=1e-12)
+        assert dt == pytest.approx(d["dt"][k], rel=1e-12)
+    assert np.all(layer_rel(q, d["qfinal"]) <= 1e-11)
+    assert g.rejects() == meta["rejects"]
+
+
+@pytest.mark.parametrize("nx,ny,nz,drag,expl", [
+    (16, 16, 2, False, False), (32, 64, 3, True, False), (64, 32, 2, True, True),
+    (128, 128, 4, False, True), (256, 128, 5, True, False), (512, 512, 2, True, False),
+    (64, 2048, 2, False, False), (2048, 64, 2, True, False), (128, 128, 16, False, False),
+    (64, 64, 32, True, False), (64, 64, 7, False, False)])
+def test_rhs_sizes(cuda_ok, nx, ny, nz, drag, expl):
+    H, S, U = exponential_stratification(nz)
+    params = strat_params(nx, ny, nz, C_d=1.0e-5 if drag else 0.0, is_explicit=expl, A2=3.0 if expl else 0.0)
+    m, g = pair(params, H, S, U)
+    q = m.initialize_spec(seeded_random_pv(nx, ny, nz, 6.0, 1.0e-6, seed=nx + 7 * ny + nz))
+    assert np.all(layer_rel(g.get_rhs(q), m.get_rhs(q)) <= RHS_TOL)
+    assert np.all(layer_rel(g.get_psi(q), m.get_psi(q)) <= RHS_TOL)
+
+
+def test_rhs_strat1024x8(cuda_ok):
+    """One RHS of the 1024^2 x 8 stratified workload against the oracle, per-layer L2 <= 1e-12."""
+    w = workload("strat1024x8")
+    m, g = pair(w.params, w.H, w.S, w.U)
+    q = m.initialize_spec(w.qp)
+    q_gpu = g.initialize(w.qp)
+    assert np.all(layer_rel(q_gpu, q) <= RHS_TOL)
+    assert np.all(layer_rel(g.get_rhs(q), m.get_rhs(q)) <= RHS_TOL)
+    a8 = g.leith()
+    assert np.allclose(a8, m.leith_A8L(q), rtol=1e-12, atol=0)
+
+
+def test_physical_fields(cuda_ok):
+    H, S, U = exponential_stratification(3)
+    params = strat_params(64, 128, 3)
+    m, g = pair(params, H, S, U)
+    q = m.initialize_spec(seeded_random_pv(64, 128, 3, 6.0, 1.0e-6, seed=5))
+    qp, pp = g.physical(q)
+    assert np.allclose(qp, m.s2g_scaled(q), rtol=0, atol=1e-13 * np.abs(qp).max())
+    assert np.allclose(pp, m.s2g_scaled(m.get_psi(q)), rtol=0, atol=1e-13 * np.abs(pp).max())
+    g.set_state(q, 0.0, 100.0)
+    ke, _ = g.diagnostics()
+    assert np.allclose(ke, m.layer_ke(q), rtol=1e-11)
+
+
+@pytest.mark.parametrize("scheme", ["ark43_qgleith", "ark43", "bsrk3", "rk4", "ab3"])
+def test_schemes_short_run(cuda_ok, scheme):
+    H, S, U = exponential_stratification(4)
+    params = strat_params(128, 128, 4, C_d=1.0e-5, TOL=2.0e-12, is_explicit=scheme in ("bsrk3", "rk4", "ab3"))
+    m, g = pair(params, H, S, U, scheme=scheme)
+    q = m.initialize_spec(seeded_random_pv(128, 128, 4, 10.0, 1.0e-6, seed=21))
+    qg = q.copy()
+    st = SCHEMES[scheme](m)
+    t = tg = 0.0
+    dt = dtg = 900.0
+    for _ in range(8):
+        q, t, dt = st.step(q, t, dt)
+        tg, dtg = g.time_step(qg, tg, dtg)
+    assert tg == pytest.approx(t, rel=1e-12)
+    assert dtg == pytest.approx(dt, rel=1e-12)
+    assert np.all(layer_rel(qg, q) <= 1e-11)
+
+
+def test_hundred_fixed_steps(cuda_ok):
+    """100 fixed-dt ARK43 steps (dt_max clip, huge TOL) of the 2-layer Phillips problem."""
+    H, S, U = phillips_two_layer()
+    n = 128
+    A8 = 1.0 / (86400.0 * (math.pi * n / 1.0e6) ** 8)
+    params = dict(nx=n, ny=n, nz=2, Lx=1.0e6, Ly=1.0e6, Htot=4000.0, f0=1.0e-4, beta=1.6e-11, A2=0.0, A8=A8,
+                  r0=1.0e-7, C_d=0.0, TOL=1.0e30, is_explicit=False, dt_max=900.0)
+    m, g = pair(params, H, S, U, scheme="ark43")
+    q = m.initialize_spec(seeded_random_pv(n, n, 2, 10.0, 1.0e-6, seed=1))
+    g.set_state(q, 0.0, 900.0)
+    g.advance_resident(100)
+    qg = g.get_state()
+    st = SCHEMES["ark43"](m)
+    t, dt = 0.0, 900.0
+    for _ in range(100):
+        q, t, dt = st.step(q, t, dt)
+    assert g.t == pytest.approx(t, rel=1e-14)
+    assert np.all(layer_rel(qg, q) <= 1e-11)
+
+
+def test_resident_equals_step_api(cuda_ok):
+    w = workload("strat1024x8", nx=128, nz=4)
+    g1 = QGNModule(w.params, w.H, w.S, w.U, scheme="ark43_qgleith")
+    g2 = QGNModule(w.params, w.H, w.S, w.U, scheme="ark43_qgleith")
+    q = g1.initialize(w.qp, 0.0, 750.0)
+    q1 = q.copy()
+    t, dt = 0.0, 750.0
+    for _ in range(4):
+        t, dt = g1.time_step(q1, t, dt)
+    g2.set_state(q, 0.0, 750.0)
+    g2.advance_resident(4)
+    q2 = g2.get_state()
+    assert np.array_equal(q1, q2)
+    assert (g2.t, g2.dt) == (t, dt)
+
+
+def test_reject_limit_is_reported(cuda_ok):
+    H, S, U = exponential_stratification(2)
+    params = strat_params(32, 32, 2, TOL=0.0)
+    g = QGNModule(params, H, S, U, scheme="ark43_qgleith", max_rejects=3)
+    q = g.initialize(seeded_random_pv(32, 32, 2, 4.0, 1.0e-6, seed=3), 0.0, 500.0)
+    with pytest.raises(QGNError) as ei:
+        g.time_step(q, 0.0, 500.0)
+    assert ei.value.code == QGN_ERR_REJECT_LIMIT
+    assert g.rejects() == 3
+    # the context stays usable after the failure
+    g.p["TOL"] = 1.0
+    assert np.isfinite(g.get_rhs(q)).all()
+
+
+def test_nonfinite_input_is_reported(cuda_ok):
+    H, S, U = exponential_stratification(2)
+    params = strat_params(32, 32, 2)
+    for scheme in ("ark43_qgleith", "rk4"):
+        g = QGNModule(params, H, S, U, scheme=scheme)
+        q = g.initialize(seeded_random_pv(32, 32, 2, 4.0, 1.0e-6, seed=3), 0.0, 500.0)
+        q[1, 3, 2] = np.nan
+        with pytest.raises(QGNError) as ei:
+            g.time_step(q, 0.0, 500.0)
+        assert ei.value.code == QGN_ERR_NONFINITE
