@@ -148,6 +148,14 @@ int qgn_profile_read(qgn_ctx* ctx, int kernel, double* total_ms, double* bytes,
                      long long* timed_launches, long long* launches);
 const char* qgn_kernel_name(int kernel);
 
+/*
+ * Debugging hook: copy one device work buffer to the host as interleaved doubles
+ * (count = capacity in doubles).  which: 0 state q (compact [nz][nx/3][nky]), 1 psi of
+ * the last evaluation (compact), 2..6 the half-transformed fields [nz][ny][nkxp] of the
+ * last RHS: q, psi, u, u*q, v*q.  nkxp = nx/3 rounded up to a multiple of 4.
+ */
+int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
+
 /* The cudaStream_t (as void*) all of this context's work is issued on. */
 int qgn_stream(qgn_ctx* ctx, void** stream);
 

@@ -67,6 +67,7 @@ SIGNATURES = {
     "qgn_profile_read": (C.c_int, [_ctxp, C.c_int, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "qgn_kernel_name": (C.c_char_p, [C.c_int]),
     "qgn_stream": (C.c_int, [_ctxp, C.POINTER(C.c_void_p)]),
+    "qgn_debug_read": (C.c_int, [_ctxp, C.c_int, _dp, C.c_longlong]),
     "qgn_last_error": (C.c_char_p, [_ctxp]),
     "qgn_destroy": (C.c_int, [_ctxp]),
 }

@@ -686,6 +686,28 @@ const char* qgn_kernel_name(int kernel) {
     return names[kernel];
 }
 
+int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count) {
+    if (!ctx || !out) return QGN_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const Buffers& b = ctx->b;
+    const double2* src = nullptr;
+    size_t n = 0;
+    switch (which) {
+        case 0: src = b.q; n = ctx->g.csize(); break;
+        case 1: src = b.psi; n = ctx->g.csize(); break;
+        case 2: src = b.hq; n = ctx->g.hsize(); break;
+        case 3: src = b.hp; n = ctx->g.hsize(); break;
+        case 4: src = b.hu; n = ctx->g.hsize(); break;
+        case 5: src = b.huq; n = ctx->g.hsize(); break;
+        case 6: src = b.hvq; n = ctx->g.hsize(); break;
+        default: return set_err(ctx, QGN_ERR_ARG, "unknown buffer");
+    }
+    if ((size_t)count < 2 * n) return set_err(ctx, QGN_ERR_ARG, "output too small");
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(out, src, sizeof(double2) * n, cudaMemcpyDeviceToHost));
+    return QGN_OK;
+}
+
 int qgn_stream(qgn_ctx* ctx, void** stream) {
     if (!ctx || !stream) return QGN_ERR_ARG;
     *stream = (void*)ctx->stream;

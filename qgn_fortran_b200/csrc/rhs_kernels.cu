@@ -6,7 +6,7 @@
 //
 //   yinv  (per layer, per tile of kx columns)  compact q, psi -> y-inverse of q, psi, u=-i ky psi
 //         written as half-transformed rows [nz][ny][nkxp]                     (3 inverse y FFTs)
-//   xpass (per layer, per pair of rows y)       c2r of q+iu (x2 rows) and v1+iv2 (v = i kx psi),
+//   xpass (per layer, per pair of rows y)       c2r of q1+iq2, u1+iu2, v1+iv2 (v = i kx psi),
 //         products uq, vq (and |u|u, |u|v in the bottom layer), r2c of uq+ivq; keeps kx < nx/3
 //   yfwd  (per layer, per tile of kx columns)  forward y FFT of uq, vq (and drag fields), then
 //         J = i kx (uq)^ + i ky (vq)^ and RHS = -J - U i kx q - (beta+Qy) v + Ekman + drag,
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(YInvCfg<NY>::THREADS) k_yinv(Geom g, const dou
 }
 
 // ------------------------------------------------------------------------------------
-// xpass: x transforms of row pairs.  c2r of a = q + i u and b = v1 + i v2 (Hermitian
+// xpass: x transforms of row pairs.  c2r of q1 + i q2, u1 + i u2 and v1 + i v2 (Hermitian
 // extension of the kept kx, Re of kx=0 as the c2r Hermitian projection), physical products,
 // r2c of p = uq + i vq, split and truncated to kx < nx/3.
 // ------------------------------------------------------------------------------------
@@ -217,17 +217,20 @@ __global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS) k_xpass(Geom g, int l
             const double kxv = g.dkx * kk;
             const double2 V1 = make_double2(-kxv * P1.y, kxv * P1.x);   // v_hat = i kx psi_hat
             const double2 V2 = make_double2(-kxv * P2.y, kxv * P2.x);
+            // pack two rows of the same field per complex transform: q1+iq2, u1+iu2, v1+iv2
+            // (pairing fields of very different magnitude, e.g. q+iu, would leak the roundoff
+            // of the larger one into the smaller one)
             if (k == 0) {
-                a1 = make_double2(Q1.x, U1.x);
-                a2 = make_double2(Q2.x, U2.x);
+                a1 = make_double2(Q1.x, Q2.x);
+                a2 = make_double2(U1.x, U2.x);
                 b = make_double2(V1.x, V2.x);
             } else if (lo) {
-                a1 = make_double2(Q1.x - U1.y, Q1.y + U1.x);
-                a2 = make_double2(Q2.x - U2.y, Q2.y + U2.x);
+                a1 = make_double2(Q1.x - Q2.y, Q1.y + Q2.x);
+                a2 = make_double2(U1.x - U2.y, U1.y + U2.x);
                 b = make_double2(V1.x - V2.y, V1.y + V2.x);
             } else {
-                a1 = make_double2(Q1.x + U1.y, U1.x - Q1.y);
-                a2 = make_double2(Q2.x + U2.y, U2.x - Q2.y);
+                a1 = make_double2(Q1.x + Q2.y, Q2.x - Q1.y);
+                a2 = make_double2(U1.x + U2.y, U2.x - U1.y);
                 b = make_double2(V1.x + V2.y, V2.x - V1.y);
             }
         }
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS) k_xpass(Geom g, int l
         if (rp0 + r >= npairs) continue;
         double2* base = sm + (r * C::SP) * C::TS;
         const double2 a1 = base[fpad(x)], a2 = base[C::TS + fpad(x)], b = base[2 * C::TS + fpad(x)];
-        const double q1 = a1.x * s, u1 = a1.y * s, q2 = a2.x * s, u2 = a2.y * s;
+        const double q1 = a1.x * s, q2 = a1.y * s, u1 = a2.x * s, u2 = a2.y * s;
         const double v1 = b.x * s, v2 = b.y * s;
         base[fpad(x)] = make_double2(u1 * q1, v1 * q1);
         base[C::TS + fpad(x)] = make_double2(u2 * q2, v2 * q2);
