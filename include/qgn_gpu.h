@@ -31,6 +31,7 @@ extern "C" {
 #define QGN_ERR_REJECT_LIMIT  4   /* adaptive step rejected max_rejects times in a row*/
 #define QGN_ERR_ARG           5   /* null pointer / invalid argument                  */
 #define QGN_ERR_NO_DEVICE     6   /* no CUDA device, or not an sm_100 device          */
+#define QGN_ERR_TOO_LARGE     7   /* grid does not fit QGN_STATIC_SCRATCH_BYTES (qgn_rhs_static) */
 
 /* ---- time integrators: the include files of QGN_Module.f90:306 ---------- */
 #define QGN_SCHEME_ARK43_QGLEITH 0  /* ARK43_QGLeith.f90 (reference default) */
@@ -158,6 +159,34 @@ int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
 
 /* The cudaStream_t (as void*) all of this context's work is issued on. */
 int qgn_stream(qgn_ctx* ctx, void** stream);
+
+/*
+ * One GetRHS (QGN_Module.f90:258-296) that allocates no device memory.  No counterpart in
+ * the reference: it exists for hosts that cannot call cudaMalloc where the model is
+ * evaluated -- a component coupled into a larger application that owns all device memory
+ * (an OpenACC or OpenMP-offload data region, or a pool carved up at start-up), or a time
+ * loop that must not take cudaMalloc's implicit device synchronisation.
+ *
+ * q_hat_dev and rhs_dev are DEVICE arrays in the reference's layout
+ * complex(dp)(nx/2+1,ny,nz) (interleaved doubles, Fortran order); rhs_dev receives the
+ * dealiased right-hand side with zeros in the dealiased band.  The other arguments are the
+ * host arrays of qgn_create.  Work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and is not waited for.
+ *
+ * Intermediates live in one file-scope device array of QGN_STATIC_SCRATCH_BYTES that the
+ * library's module reserves on every GPU where it is used, until process exit.  A grid
+ * needs 16*(5*nz*ny*nkxp + 2*ny*nkxp + 3*nz*nkx*nky + nx + ny) bytes plus about 18 KB of
+ * constants (nkx = nx/3, nkxp = nkx rounded up to 4, nky = ny - ny/3 - 1); larger grids
+ * return QGN_ERR_TOO_LARGE (256^2 x 8 and 512^2 x 2 fit).  All calls share the array and
+ * it keeps the last call's contents, so calls whose GPU work overlaps (other streams,
+ * other host threads on the same device) race.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and loads the module if it is not loaded
+ * yet; make that first call before any stream capture on that device.
+ */
+#define QGN_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int qgn_rhs_static(const qgn_params* p, const double* H, const double* uBar, const double* qyBar,
+                   const double* Modes, const double* EVals, const double* q_hat_dev, double* rhs_dev,
+                   void* stream);
 
 /* Message of the last failing call on this context (never NULL). */
 const char* qgn_last_error(const qgn_ctx* ctx);

@@ -18,6 +18,8 @@ QGN_ERR_NONFINITE = 3
 QGN_ERR_REJECT_LIMIT = 4
 QGN_ERR_ARG = 5
 QGN_ERR_NO_DEVICE = 6
+QGN_ERR_TOO_LARGE = 7
+QGN_STATIC_SCRATCH_BYTES = 32 * 1024 * 1024
 QGN_KERNEL_FAMILIES = 14
 
 SCHEMES = {"ark43_qgleith": 0, "ark43": 1, "bsrk3": 2, "rk4": 3, "ab3": 4}
@@ -30,6 +32,7 @@ ERROR_NAMES = {
     QGN_ERR_REJECT_LIMIT: "QGN_ERR_REJECT_LIMIT",
     QGN_ERR_ARG: "QGN_ERR_ARG",
     QGN_ERR_NO_DEVICE: "QGN_ERR_NO_DEVICE",
+    QGN_ERR_TOO_LARGE: "QGN_ERR_TOO_LARGE",
 }
 
 
@@ -68,6 +71,8 @@ SIGNATURES = {
     "qgn_kernel_name": (C.c_char_p, [C.c_int]),
     "qgn_stream": (C.c_int, [_ctxp, C.POINTER(C.c_void_p)]),
     "qgn_debug_read": (C.c_int, [_ctxp, C.c_int, _dp, C.c_longlong]),
+    "qgn_rhs_static": (C.c_int, [C.POINTER(qgn_params), _dp, _dp, _dp, _dp, _dp, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
     "qgn_last_error": (C.c_char_p, [_ctxp]),
     "qgn_destroy": (C.c_int, [_ctxp]),
 }
