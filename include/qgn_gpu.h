@@ -153,7 +153,9 @@ const char* qgn_kernel_name(int kernel);
  * Debugging hook: copy one device work buffer to the host as interleaved doubles
  * (count = capacity in doubles).  which: 0 state q (compact [nz][nx/3][nky]), 1 psi of
  * the last evaluation (compact), 2..6 the half-transformed fields [nz][ny][nkxp] of the
- * last RHS: q, psi, u, u*q, v*q.  nkxp = nx/3 rounded up to a multiple of 4.
+ * last RHS as packed row pairs [nz][ny/2][2][nkxp]: 2 q, 3 v = i kx psi, 4 u = -i ky psi;
+ * 5 the forward x transforms of u*q + i v*q, [nz][ny][2][nkxp] (P[k], P[nx-k] for k < nkx).
+ * nkxp = nx/3 rounded up to a multiple of 4.
  */
 int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
 

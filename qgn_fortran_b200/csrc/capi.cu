@@ -411,8 +411,8 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     AL(b.q, C); AL(b.qnew, C); AL(b.psi, C); AL(b.err, C);
     for (int j = 0; j < 6; ++j) AL(b.N[j], C);
     for (int j = 1; j < 6; ++j) AL(b.Qs[j], C);
-    AL(b.hq, Hh); AL(b.hp, Hh); AL(b.hu, Hh); AL(b.huq, Hh); AL(b.hvq, Hh);
-    AL(b.hdu, (size_t)g.ny * g.nkxp); AL(b.hdv, (size_t)g.ny * g.nkxp);
+    AL(b.hq, Hh); AL(b.hp, Hh); AL(b.hu, Hh); AL(b.hpp, 2 * Hh);
+    AL(b.hpd, (size_t)2 * g.ny * g.nkxp);
     AL(b.xfer, C);
     AL(b.twx, (size_t)g.nx); AL(b.twy, (size_t)g.ny);
     AL(b.red, (size_t)512 * kMaxNZ);
@@ -429,10 +429,10 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     }
     if (rc == QGN_OK) {
         // zero everything once: padding columns of the half fields stay zero forever
-        double2* zs[] = {b.q, b.qnew, b.psi, b.err, b.hq, b.hp, b.hu, b.huq, b.hvq};
+        double2* zs[] = {b.q, b.qnew, b.psi, b.err, b.hq, b.hp, b.hu, b.hpp};
         for (double2* z : zs) {
-            cudaError_t e = cudaMemset(z, 0, sizeof(double2) * ((z == b.hq || z == b.hp || z == b.hu || z == b.huq ||
-                                                                   z == b.hvq) ? Hh : C));
+            const size_t n = (z == b.hpp) ? 2 * Hh : ((z == b.hq || z == b.hp || z == b.hu) ? Hh : C);
+            cudaError_t e = cudaMemset(z, 0, sizeof(double2) * n);
             if (e != cudaSuccess) { fail("cudaMemset", e); break; }
         }
         for (int j = 0; j < 6 && rc == QGN_OK; ++j) {
@@ -441,8 +441,7 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
             if (e != cudaSuccess) fail("cudaMemset", e);
         }
         if (rc == QGN_OK) {
-            cudaError_t e = cudaMemset(b.hdu, 0, sizeof(double2) * g.ny * g.nkxp);
-            if (e == cudaSuccess) e = cudaMemset(b.hdv, 0, sizeof(double2) * g.ny * g.nkxp);
+            cudaError_t e = cudaMemset(b.hpd, 0, sizeof(double2) * 2 * g.ny * g.nkxp);
             if (e != cudaSuccess) fail("cudaMemset", e);
         }
     }
@@ -698,8 +697,7 @@ int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count) {
         case 2: src = b.hq; n = ctx->g.hsize(); break;
         case 3: src = b.hp; n = ctx->g.hsize(); break;
         case 4: src = b.hu; n = ctx->g.hsize(); break;
-        case 5: src = b.huq; n = ctx->g.hsize(); break;
-        case 6: src = b.hvq; n = ctx->g.hsize(); break;
+        case 5: src = b.hpp; n = 2 * ctx->g.hsize(); break;
         default: return set_err(ctx, QGN_ERR_ARG, "unknown buffer");
     }
     if ((size_t)count < 2 * n) return set_err(ctx, QGN_ERR_ARG, "output too small");

@@ -103,82 +103,131 @@ struct FFTShape {
     static constexpr int G = N / T;             // threads per transform
 };
 
-// twiddle w^r for r = 1..R-1 with w = table[k*S] (conjugated for DIR=+1);
-// powers of two are read from the table, the rest formed by at most 3 products.
-template <int R, int DIR>
-__device__ __forceinline__ void load_twiddles(double2* w, const double2* __restrict__ tw, int kS) {
-    w[0] = make_double2(1.0, 0.0);
-#pragma unroll
-    for (int r = 1; r < R; ++r) {
-        if ((r & (r - 1)) == 0) {
-            double2 t = __ldg(&tw[r * kS]);
-            w[r] = DIR > 0 ? cconj(t) : t;
-        }
-    }
-#pragma unroll
-    for (int r = 3; r < R; ++r) {
-        if ((r & (r - 1)) != 0) {
-            const int hi = r >= 8 ? 8 : (r >= 4 ? 4 : 2);
-            w[r] = cmul(w[hi], w[r - hi]);
+// Inter-pass twiddles of one radix-R butterfly: v[r] *= w^r, w = exp(DIR 2 pi i k/(NS R)).
+// w^(2^q) come from the table tw[m] = exp(-2 pi i m/N) (conjugated for DIR=+1); the other
+// powers are products of at most three table values, formed just before use.
+template <int N, int NS, int R, int DIR>
+__device__ __forceinline__ void apply_twiddles(double2* v, int k, const double2* __restrict__ tw) {
+    if constexpr (NS > 1) {
+        constexpr int S = N / (NS * R);
+        const int kS = k * S;
+        auto ldw = [&](int r) {
+            const double2 t = __ldg(&tw[r * kS]);
+            return DIR > 0 ? cconj(t) : t;
+        };
+        const double2 w1 = ldw(1);
+        v[1] = cmul(v[1], w1);
+        if constexpr (R > 2) {
+            const double2 w2 = ldw(2);
+            const double2 w3 = cmul(w2, w1);
+            v[2] = cmul(v[2], w2);
+            v[3] = cmul(v[3], w3);
+            if constexpr (R > 4) {
+                const double2 w4 = ldw(4);
+                const double2 w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+                v[4] = cmul(v[4], w4);
+                v[5] = cmul(v[5], w5);
+                v[6] = cmul(v[6], w6);
+                v[7] = cmul(v[7], w7);
+                if constexpr (R > 8) {
+                    const double2 w8 = ldw(8);
+                    v[8] = cmul(v[8], w8);
+                    v[9] = cmul(v[9], cmul(w8, w1));
+                    v[10] = cmul(v[10], cmul(w8, w2));
+                    v[11] = cmul(v[11], cmul(w8, w3));
+                    v[12] = cmul(v[12], cmul(w8, w4));
+                    v[13] = cmul(v[13], cmul(w8, w5));
+                    v[14] = cmul(v[14], cmul(w8, w6));
+                    v[15] = cmul(v[15], cmul(w8, w7));
+                }
+            }
         }
     }
 }
 
-// One Stockham DIT pass (current sub-transform length NS, radix R) of an N-point
-// transform stored padded at x.  lane in [0,G).
-template <int N, int NS, int DIR>
-__device__ __forceinline__ void fft_pass(double2* x, int lane, bool active, const double2* __restrict__ tw) {
+// Where a pass takes its input from / puts its output to.
+enum FftSrc { SRC_SMEM = 0, SRC_FN = 1, SRC_FN_SMEM = 2 };   // SRC_FN_SMEM: a functor that reads this smem
+enum FftDst { DST_SMEM = 0, DST_FN = 1 };
+
+// One Stockham DIT pass (sub-length NS, radix R) of an N-point transform whose
+// intermediate lives padded at x.  Pass 0 may read through ld(idx), the last pass may
+// write through st(idx, value); every other access goes to x.  Barriers: a pass that reads
+// the shared buffer it overwrites syncs between its reads and writes, and a pass that
+// writes the shared buffer syncs after its writes.  With SRC_FN the caller guarantees
+// that no thread still reads x when the pass starts writing it.
+template <int N, int NS, int DIR, int SRC, int DST, class Ld, class St>
+__device__ __forceinline__ void fft_pass_io(double2* x, int lane, bool active, const double2* __restrict__ tw,
+                                            Ld& ld, St& st) {
     constexpr int T = FFTShape<N>::T;
     constexpr int G = FFTShape<N>::G;
     constexpr int R = (N / NS >= 16) ? 16 : N / NS;
-    constexpr int BPT = T / R;           // butterflies per thread
+    constexpr int BPT = T / R;
     constexpr int STRIDE = N / R;
     double2 v[T];
     if (active) {
 #pragma unroll
         for (int b = 0; b < BPT; ++b) {
-            int j = lane + b * G;
+            const int j = lane + b * G;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[b * R + r] = x[fpad(j + r * STRIDE)];
+            for (int r = 0; r < R; ++r) {
+                const int idx = j + r * STRIDE;
+                if constexpr (SRC == SRC_SMEM) v[b * R + r] = x[fpad(idx)];
+                else v[b * R + r] = ld(idx);
+            }
         }
     }
-    __syncthreads();
+    if constexpr (DST == DST_SMEM && SRC != SRC_FN) __syncthreads();
     if (active) {
 #pragma unroll
         for (int b = 0; b < BPT; ++b) {
-            int j = lane + b * G;
-            int k = j & (NS - 1);
-            if (NS > 1) {
-                double2 w[R];
-                load_twiddles<R, DIR>(w, tw, k * (N / (NS * R)));
-#pragma unroll
-                for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], w[r]);
-            }
+            const int j = lane + b * G;
+            const int k = j & (NS - 1);
+            apply_twiddles<N, NS, R, DIR>(&v[b * R], k, tw);
             RegDFT<R, DIR>::run(&v[b * R]);
-            int base = (j - k) * R + k;
+            const int base = (j - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) x[fpad(base + r * NS)] = v[b * R + r];
+            for (int r = 0; r < R; ++r) {
+                const int idx = base + r * NS;
+                if constexpr (DST == DST_SMEM) x[fpad(idx)] = v[b * R + r];
+                else st(idx, v[b * R + r]);
+            }
         }
     }
-    __syncthreads();
+    if constexpr (DST == DST_SMEM) __syncthreads();
 }
 
-template <int N, int NS, int DIR>
-__device__ __forceinline__ void fft_passes(double2* x, int lane, bool active, const double2* __restrict__ tw) {
-    if constexpr (NS < N) {
-        constexpr int R = (N / NS >= 16) ? 16 : N / NS;
-        fft_pass<N, NS, DIR>(x, lane, active, tw);
-        fft_passes<N, NS * R, DIR>(x, lane, active, tw);
-    }
+template <int N, int NS, int DIR, int SRC0, int DSTL, class Ld, class St>
+__device__ __forceinline__ void fft_rec(double2* x, int lane, bool active, const double2* __restrict__ tw, Ld& ld,
+                                        St& st) {
+    constexpr int R = (N / NS >= 16) ? 16 : N / NS;
+    constexpr bool FIRST = (NS == 1);
+    constexpr bool LAST = (NS * R == N);
+    constexpr int SRC = FIRST ? SRC0 : SRC_SMEM;
+    constexpr int DST = LAST ? DSTL : DST_SMEM;
+    fft_pass_io<N, NS, DIR, SRC, DST>(x, lane, active, tw, ld, st);
+    if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
 }
 
-// In-place N-point transform of the padded array x by the G threads with lane in [0,G).
-// Every thread of the block must call this (it contains __syncthreads); threads that
-// own no transform pass active=false and only take part in the barriers.  The caller
-// syncs before (data ready); the function ends with a barrier.
+struct NoIO {
+    __device__ double2 operator()(int) const { return make_double2(0.0, 0.0); }
+    __device__ void operator()(int, double2) const {}
+};
+
+// N-point transform of one slot by the G threads with lane in [0,G), reading its input
+// through ld (SRC0 = SRC_FN / SRC_FN_SMEM) or from x (SRC_SMEM, written and synced by the
+// caller) and delivering its output through st (DSTL = DST_FN) or into x (DST_SMEM, synced
+// on return).  Every thread of the block calls this (it may contain __syncthreads).
+template <int N, int DIR, int SRC0, int DSTL, class Ld, class St>
+__device__ __forceinline__ void fft_fused(double2* x, int lane, bool active, const double2* __restrict__ tw, Ld ld,
+                                          St st) {
+    fft_rec<N, 1, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
+}
+
+// In-place N-point transform of the padded array x (caller syncs before; ends with a barrier).
 template <int N, int DIR>
 __device__ __forceinline__ void fft_block(double2* x, int lane, bool active, const double2* __restrict__ tw) {
-    fft_passes<N, 1, DIR>(x, lane, active, tw);
+    NoIO io;
+    fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM>(x, lane, active, tw, io, io);
 }
 
 }  // namespace qgn

@@ -6,7 +6,8 @@
 //       [0, ny/3) U [2(ny/3)+1, ny); compact m < ny/3 -> j = m, else j = m + ny/3 + 1.
 //       ky is the contiguous axis so the y transforms stream whole columns.
 //   half-transformed field  [nz][ny][nkxp]   -- x still spectral (kept kx only), y physical;
-//       the row layout the x pass streams.  nkxp = nkx rounded up to a multiple of 4.
+//       the row layout the x pass streams, stored as packed row pairs (see rhs_kernels.cu).
+//       nkxp = nkx rounded up to a multiple of 4.
 //   Mode (0,0) of every compact field is held at zero, as DeAlias does.
 #pragma once
 #include <cuda_runtime.h>
@@ -65,13 +66,11 @@ struct Buffers {
     double2* Qs[6] = {};         // stage states (Qs[0] aliases q for the ARK schemes)
     double2* psi = nullptr;      // psi of the field being evaluated
     double2* err = nullptr;      // error combination (compact)
-    double2* hq = nullptr;       // half-transformed q, psi, u   [nz][ny][nkxp]
-    double2* hp = nullptr;
-    double2* hu = nullptr;
-    double2* huq = nullptr;      // half-transformed u*q, v*q
-    double2* hvq = nullptr;
-    double2* hdu = nullptr;      // half-transformed |u|u, |u|v of the bottom layer [ny][nkxp]
-    double2* hdv = nullptr;
+    double2* hq = nullptr;       // packed row pairs of q (and of single fields) [nz][ny/2][2][nkxp]
+    double2* hp = nullptr;       // packed row pairs of v = i kx psi
+    double2* hu = nullptr;       // packed row pairs of u = -i ky psi
+    double2* hpp = nullptr;      // forward x transforms P[k], P[nx-k] of u*q + i v*q [nz][ny][2][nkxp]
+    double2* hpd = nullptr;      // same for |u|u + i |u|v of the bottom layer [ny][2][nkxp]
     double2* xfer = nullptr;     // host-order kept modes [nz][nky][nkx]
     double2* full = nullptr;     // full CCE field [nz][ny][nxh] (lazy)
     double* phys = nullptr;      // physical field [nz][ny][nx] (lazy)

@@ -4,10 +4,10 @@
 // DeAlias is evaluated as three streaming passes over HBM plus the modal inversion
 // that the stage kernels fuse into their epilogue:
 //
-//   yinv  (per layer, per tile of kx columns)  compact q, psi -> y-inverse of q, psi, u=-i ky psi
-//         written as half-transformed rows [nz][ny][nkxp]                     (3 inverse y FFTs)
-//   xpass (per layer, per pair of rows y)       c2r of q1+iq2, u1+iu2, v1+iv2 (v = i kx psi),
-//         products uq, vq (and |u|u, |u|v in the bottom layer), r2c of uq+ivq; keeps kx < nx/3
+//   yinv  (per layer, per tile of kx columns)  compact q, psi -> y-inverse of q, u = -i ky psi,
+//         v = i kx psi, written as packed row pairs [nz][ny/2][2][nkxp]     (3 inverse y FFTs)
+//   xpass (per layer, per pair of rows y)       c2r of q1+iq2, u1+iu2, v1+iv2, products uq, vq
+//         (and |u|u, |u|v in the bottom layer), r2c of uq+ivq per row; keeps kx < nx/3
 //   yfwd  (per layer, per tile of kx columns)  forward y FFT of uq, vq (and drag fields), then
 //         J = i kx (uq)^ + i ky (vq)^ and RHS = -J - U i kx q - (beta+Qy) v + Ekman + drag,
 //         written for the kept modes only (DeAlias is the storage format).
@@ -33,10 +33,19 @@ __host__ __device__ constexpr int slot_stride(int N, int target_mod8) {
     return fpadlen(N) + ((target_mod8 - (fpadlen(N) % 8)) + 8) % 8;
 }
 
+// minimum resident CTAs for __launch_bounds__ such that a thread keeps up to maxregs registers
+__host__ __device__ constexpr int minb(int threads, int maxregs = 128) {
+    return cmax(1, cmin(8, 65536 / (threads * maxregs)));
+}
+
+// y-pass tiles: TKX kx columns per CTA, lane-interleaved (slot = tid % TKX) so that one
+// warp touches 8 consecutive y rows of TKX adjacent columns: 16*TKX-byte segments in the
+// half-transformed row layout, 128-byte segments in the compact column layout.
 template <int NY>
 struct YInvCfg {
     static constexpr int G = FFTShape<NY>::G;
-    static constexpr int TKX = cmin(cmax(4, 128 / G), 64);
+    // <= 16 so that the row partner of a lane (thread tid ^ TKX) is in the same warp
+    static constexpr int TKX = cmin(cmax(4, 128 / G), 16);
     static constexpr int THREADS = TKX * G;
     static constexpr int TS = slot_stride(NY, TKX >= 8 ? 1 : 8 / TKX);
     static constexpr int SMEM = TKX * TS * (int)sizeof(double2);
@@ -55,10 +64,10 @@ struct XCfg {
 template <int NY, bool DRAG>
 struct YFwdCfg {
     static constexpr int G = FFTShape<NY>::G;
-    static constexpr int TKX = cmin(cmax(2, 64 / G), 32);
+    static constexpr int TKX = cmin(cmax(2, 64 / G), 16);   // tid ^ TKX stays in the warp
     static constexpr int SLOTS = 2 * TKX;
     static constexpr int THREADS = SLOTS * G;
-    static constexpr int TS = slot_stride(NY, TKX >= 8 ? 1 : 8 / TKX);
+    static constexpr int TS = slot_stride(NY, SLOTS >= 8 ? 1 : 8 / SLOTS);
     static constexpr int SMEM = SLOTS * TS * (int)sizeof(double2);
 };
 
@@ -84,9 +93,8 @@ __device__ __forceinline__ void modal_invert(const double* __restrict__ proj, co
                     acc.y += c * qv[kk].y;
                 }
             }
-            double2 qm = make_double2(acc.x / Htot, acc.y / Htot);
-            double den = -k2 + ev[k];
-            pm[k] = mean_mode ? make_double2(0.0, 0.0) : make_double2(qm.x / den, qm.y / den);
+            const double rden = 1.0 / ((-k2 + ev[k]) * Htot);
+            pm[k] = mean_mode ? make_double2(0.0, 0.0) : make_double2(acc.x * rden, acc.y * rden);
         }
     }
 #pragma unroll
@@ -132,204 +140,195 @@ __global__ void __launch_bounds__(256) k_modal(Geom g, const ModalConst* __restr
 }
 
 // ------------------------------------------------------------------------------------
-// yinv: inverse y transforms of kept columns into half-transformed rows.
-// NF = 3: (q -> hq, psi -> hp, -i ky psi -> hu);  NF = 1: (f -> hq).
+// Packed row pairs.  The x pass transforms rows y1 = 2p and y2 = 2p+1 of one field as one
+// complex signal f1 + i f2 whose Hermitian extension is
+//     A[k]      = F1[k] + i F2[k]               (0 <= k < nkx; Re parts only at k = 0)
+//     A[nx - k] = conj(F1[k]) + i conj(F2[k])   (1 <= k < nkx)
+// The y passes store exactly these two arrays per row pair: [nz][ny/2][2][nkxp] with slot
+// 0 = A[k] and slot 1 = A[nx-k] (same bytes as two plain rows).  The x pass reads one value
+// per element, and its forward transform writes P[k] and P[nx-k] of every row the same
+// way, which the forward y pass splits into (uq)^ = (P[k] + conj P[nx-k])/2 and
+// (vq)^ = (P[k] - conj P[nx-k])/(2i).
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double2 pack_lo(double2 f1, double2 f2, bool k0) {
+    return k0 ? make_double2(f1.x, f2.x) : make_double2(f1.x - f2.y, f1.y + f2.x);
+}
+__device__ __forceinline__ double2 pack_hi(double2 f1, double2 f2) {
+    return make_double2(f1.x + f2.y, f2.x - f1.y);
+}
+
+// ------------------------------------------------------------------------------------
+// yinv: inverse y transforms of kept columns into packed row pairs.
+// NF = 3: (q -> pq, -i ky psi -> pu, i kx psi -> pv);  NF = 1: (f -> pq).
+// The first radix pass reads the compact column straight from HBM (zeros in the dealiased
+// band); the transformed column stays in shared memory, where a packing loop pairs rows
+// y and y+1 and writes the two packed arrays with TKX-wide coalesced stores.
 // ------------------------------------------------------------------------------------
 template <int NY, int NF>
-__global__ void __launch_bounds__(YInvCfg<NY>::THREADS) k_yinv(Geom g, const double2* __restrict__ q,
-                                                               const double2* __restrict__ psi,
-                                                               double2* __restrict__ hq, double2* __restrict__ hp,
-                                                               double2* __restrict__ hu,
-                                                               const double2* __restrict__ twy) {
+__global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREADS))
+    k_yinv(Geom g, const double2* __restrict__ q, const double2* __restrict__ psi, double2* __restrict__ pq,
+           double2* __restrict__ pv, double2* __restrict__ pu, const double2* __restrict__ twy) {
     using C = YInvCfg<NY>;
     extern __shared__ double2 sm[];
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
     const int kx0 = blockIdx.x * C::TKX;
-    const int slot = tid / C::G, lane = tid % C::G;
-    const size_t colbase = (size_t)l * g.nkx;
-#pragma unroll 1
+    const int slot = tid % C::TKX, lane = tid / C::TKX;
+    const int kx = kx0 + slot;
+    const bool colok = kx < g.nkx;
+    const size_t colbase = ((size_t)l * g.nkx + kx) * g.nky;
+    const double kxv = g.dkx * kx;
+    double2* xs = sm + slot * C::TS;
+    NoIO none;
+#pragma unroll
     for (int f = 0; f < NF; ++f) {
         const double2* src = (f == 0) ? q : psi;
-        double2* dst = (f == 0) ? hq : (f == 1 ? hp : hu);
-        for (int e = tid; e < C::TKX * NY; e += C::THREADS) {
-            const int c = e / NY, j = e % NY;
-            const int kx = kx0 + c;
-            double2 v = make_double2(0.0, 0.0);
+        double2* dst = (f == 0) ? pq : (f == 1 ? pu : pv);
+        auto ld = [&](int j) -> double2 {
             const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
-            if (kx < g.nkx && kept) {
-                const int m = j < g.kylo ? j : j - g.kyshift;
-                v = src[(colbase + kx) * g.nky + m];
-                if (f == 2) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
-                    const double kyv = g.kyval(j);
-                    v = make_double2(kyv * v.y, -kyv * v.x);
-                }
+            if (!colok || !kept) return make_double2(0.0, 0.0);
+            double2 v = src[colbase + (j < g.kylo ? j : j - g.kyshift)];
+            if (f == 1) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
+                const double kyv = g.kyval(j);
+                v = make_double2(kyv * v.y, -kyv * v.x);
+            } else if (f == 2) {   // v_hat = i kx psi_hat  (QGN_Module.f90:224)
+                v = make_double2(-kxv * v.y, kxv * v.x);
             }
-            sm[c * C::TS + fpad(j)] = v;
+            return v;
+        };
+        fft_fused<NY, +1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
+        // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
+        double2* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
+        for (int e = tid; e < (NY / 2) * C::TKX; e += C::THREADS) {
+            const int p = e / C::TKX, c = e % C::TKX;
+            const int k = kx0 + c;
+            if (k >= g.nkxp) continue;
+            const double2 f1 = sm[c * C::TS + fpad(2 * p)], f2 = sm[c * C::TS + fpad(2 * p + 1)];
+            const bool ok = k < g.nkx;
+            double2* row = dl + (size_t)p * 2 * g.nkxp;
+            row[k] = ok ? pack_lo(f1, f2, k == 0) : make_double2(0.0, 0.0);
+            row[g.nkxp + k] = (ok && k > 0) ? pack_hi(f1, f2) : make_double2(0.0, 0.0);
         }
-        __syncthreads();
-        fft_block<NY, +1>(sm + slot * C::TS, lane, true, twy);
-        for (int e = tid; e < C::TKX * NY; e += C::THREADS) {
-            const int y = e / C::TKX, c = e % C::TKX;
-            const int kx = kx0 + c;
-            if (kx < g.nkxp) dst[((size_t)l * NY + y) * g.nkxp + kx] = sm[c * C::TS + fpad(y)];
-        }
-        __syncthreads();
+        if (f + 1 < NF) __syncthreads();   // the next field's first pass reuses the slots
     }
 }
 
 // ------------------------------------------------------------------------------------
-// xpass: x transforms of row pairs.  c2r of q1 + i q2, u1 + i u2 and v1 + i v2 (Hermitian
-// extension of the kept kx, Re of kx=0 as the c2r Hermitian projection), physical products,
-// r2c of p = uq + i vq, split and truncated to kx < nx/3.
+// xpass: x transforms of row pairs.  c2r of the packed q1 + i q2, u1 + i u2, v1 + i v2
+// (pairing two rows of one field keeps roundoff relative to that field; q and u differ by
+// ~1e4 in these units), physical products formed inside the first pass of the forward
+// transforms, r2c of p = uq + i vq per row, whose last pass writes P[k] and P[nx-k] for the
+// kept kx straight to HBM.
 // ------------------------------------------------------------------------------------
 template <int NX, bool DRAG>
-__global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS) k_xpass(Geom g, int layer0,
-                                                                   const double2* __restrict__ hq,
-                                                                   const double2* __restrict__ hp,
-                                                                   const double2* __restrict__ hu,
-                                                                   double2* __restrict__ huq,
-                                                                   double2* __restrict__ hvq,
-                                                                   double2* __restrict__ hdu,
-                                                                   double2* __restrict__ hdv,
-                                                                   const double2* __restrict__ twx) {
+__global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS, minb(XCfg<NX, DRAG>::THREADS))
+    k_xpass(Geom g, int layer0, const double2* __restrict__ pq, const double2* __restrict__ pv,
+            const double2* __restrict__ pu, double2* __restrict__ pp, double2* __restrict__ pd,
+            const double2* __restrict__ twx) {
     using C = XCfg<NX, DRAG>;
     extern __shared__ double2 sm[];
     const int tid = threadIdx.x;
     const int l = layer0 + blockIdx.y;
-    const int rp0 = blockIdx.x * C::RP;
     const int npairs = g.ny / 2;
     const int nkx = g.nkx;
-    // ---- load: Hermitian-extended spectra of the three complex signals per row pair
-    for (int e = tid; e < C::RP * NX; e += C::THREADS) {
-        const int r = e / NX, k = e % NX;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
-        double2* base = sm + (r * C::SP) * C::TS;
-        double2 a1 = make_double2(0.0, 0.0), a2 = a1, b = a1;
-        const bool lo = k < nkx, hi = k > NX - nkx;
-        if (lo || hi) {
-            const int kk = lo ? k : NX - k;
-            const size_t r1 = ((size_t)l * g.ny + 2 * rp) * g.nkxp + kk;
-            const size_t r2 = r1 + g.nkxp;
-            const double2 Q1 = hq[r1], Q2 = hq[r2], U1 = hu[r1], U2 = hu[r2];
-            const double2 P1 = hp[r1], P2 = hp[r2];
-            const double kxv = g.dkx * kk;
-            const double2 V1 = make_double2(-kxv * P1.y, kxv * P1.x);   // v_hat = i kx psi_hat
-            const double2 V2 = make_double2(-kxv * P2.y, kxv * P2.x);
-            // pack two rows of the same field per complex transform: q1+iq2, u1+iu2, v1+iv2
-            // (pairing fields of very different magnitude, e.g. q+iu, would leak the roundoff
-            // of the larger one into the smaller one)
-            if (k == 0) {
-                a1 = make_double2(Q1.x, Q2.x);
-                a2 = make_double2(U1.x, U2.x);
-                b = make_double2(V1.x, V2.x);
-            } else if (lo) {
-                a1 = make_double2(Q1.x - Q2.y, Q1.y + Q2.x);
-                a2 = make_double2(U1.x - U2.y, U1.y + U2.x);
-                b = make_double2(V1.x - V2.y, V1.y + V2.x);
-            } else {
-                a1 = make_double2(Q1.x + Q2.y, Q2.x - Q1.y);
-                a2 = make_double2(U1.x + U2.y, U2.x - U1.y);
-                b = make_double2(V1.x + V2.y, V2.x - V1.y);
-            }
-        }
-        base[fpad(k)] = a1;
-        base[C::TS + fpad(k)] = a2;
-        base[2 * C::TS + fpad(k)] = b;
-    }
-    __syncthreads();
     const int slot = tid / C::G, lane = tid % C::G;
     const int r_of = slot / C::SP, s_of = slot % C::SP;
-    const bool pair_ok = (rp0 + r_of) < npairs;
-    fft_block<NX, +1>(sm + slot * C::TS, lane, pair_ok && s_of < 3, twx);
-    // ---- physical products (grid/(nx*ny) as in QGN_Module.f90:229-235)
-    const double s = g.inv_nxny;
-    for (int e = tid; e < C::RP * NX; e += C::THREADS) {
-        const int r = e / NX, x = e % NX;
-        if (rp0 + r >= npairs) continue;
-        double2* base = sm + (r * C::SP) * C::TS;
-        const double2 a1 = base[fpad(x)], a2 = base[C::TS + fpad(x)], b = base[2 * C::TS + fpad(x)];
-        const double q1 = a1.x * s, q2 = a1.y * s, u1 = a2.x * s, u2 = a2.y * s;
-        const double v1 = b.x * s, v2 = b.y * s;
-        base[fpad(x)] = make_double2(u1 * q1, v1 * q1);
-        base[C::TS + fpad(x)] = make_double2(u2 * q2, v2 * q2);
-        if (DRAG) {   // URMS = sqrt(u^2+v^2), QGN_Module.f90:285
-            const double m1 = sqrt(u1 * u1 + v1 * v1), m2 = sqrt(u2 * u2 + v2 * v2);
-            base[2 * C::TS + fpad(x)] = make_double2(m1 * u1, m1 * v1);
-            base[3 * C::TS + fpad(x)] = make_double2(m2 * u2, m2 * v2);
-        }
-    }
-    __syncthreads();
-    fft_block<NX, -1>(sm + slot * C::TS, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx);
-    // ---- split the packed real transforms and keep kx < nx/3
-    for (int e = tid; e < C::RP * nkx; e += C::THREADS) {
-        const int r = e / nkx, k = e % nkx;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
-        const double2* base = sm + (r * C::SP) * C::TS;
-        const int km = (NX - k) & (NX - 1);
-#pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            const size_t row = ((size_t)l * g.ny + 2 * rp + w) * g.nkxp + k;
-            const double2 X = base[w * C::TS + fpad(k)];
-            const double2 Y = cconj(base[w * C::TS + fpad(km)]);
-            huq[row] = make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y));
-            hvq[row] = make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
-            if (DRAG) {
-                const size_t drow = (size_t)(2 * rp + w) * g.nkxp + k;
-                const double2 Xd = base[(2 + w) * C::TS + fpad(k)];
-                const double2 Yd = cconj(base[(2 + w) * C::TS + fpad(km)]);
-                hdu[drow] = make_double2(0.5 * (Xd.x + Yd.x), 0.5 * (Xd.y + Yd.y));
-                hdv[drow] = make_double2(0.5 * (Xd.y - Yd.y), -0.5 * (Xd.x - Yd.x));
-            }
-        }
-    }
+    const int rp = blockIdx.x * C::RP + r_of;
+    const bool pair_ok = rp < npairs;
+    double2* base = sm + (r_of * C::SP) * C::TS;
+    double2* xs = sm + slot * C::TS;
+
+    // ---- inverse: slot 0 = q1+iq2, 1 = u1+iu2, 2 = v1+iv2
+    const double2* F = (s_of == 0 ? pq : (s_of == 1 ? pu : pv)) + ((size_t)l * npairs + rp) * 2 * g.nkxp;
+    auto ld_inv = [&](int k) -> double2 {
+        if (k < nkx) return F[k];
+        if (k > NX - nkx) return F[g.nkxp + (NX - k)];
+        return make_double2(0.0, 0.0);
+    };
+    NoIO none;
+    fft_fused<NX, +1, SRC_FN, DST_SMEM>(xs, lane, pair_ok && s_of < 3, twx, ld_inv, none);
+
+    // ---- forward: slot 0 = u1 q1 + i v1 q1, 1 = u2 q2 + i v2 q2 (grid/(nx*ny) scaling as in
+    //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
+    const double sc = g.inv_nxny;
+    auto ld_fwd = [&](int x) -> double2 {
+        const double2 a = base[fpad(x)], bu = base[C::TS + fpad(x)], cv = base[2 * C::TS + fpad(x)];
+        const bool second = (s_of & 1) != 0;
+        const double qv = (second ? a.y : a.x) * sc;
+        const double uv = (second ? bu.y : bu.x) * sc;
+        const double vv = (second ? cv.y : cv.x) * sc;
+        if (s_of < 2) return make_double2(uv * qv, vv * qv);
+        const double m = sqrt(uv * uv + vv * vv);   // URMS, QGN_Module.f90:285
+        return make_double2(m * uv, m * vv);
+    };
+    const int y = 2 * rp + (s_of & 1);
+    double2* out = (s_of < 2) ? pp + ((size_t)l * g.ny + y) * 2 * g.nkxp : pd + (size_t)y * 2 * g.nkxp;
+    auto st_fwd = [&](int k, double2 v) {
+        if (k < nkx) out[k] = v;
+        else if (k > NX - nkx) out[g.nkxp + (NX - k)] = v;
+    };
+    fft_fused<NX, -1, SRC_FN_SMEM, DST_FN>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd, st_fwd);
 }
 
 // ------------------------------------------------------------------------------------
 // yfwd: forward y transforms of uq, vq columns and assembly of the right-hand side.
+// Slots are lane-interleaved: slot = tid % (2 TKX), slot = field*TKX + column.  The first
+// radix pass reads the half-transformed rows straight from HBM.
 // ------------------------------------------------------------------------------------
+// split of the packed forward x transform of row y at kx: fld 0 -> (uq)^, fld 1 -> (vq)^
+__device__ __forceinline__ double2 unpack_p(const double2* __restrict__ row, int nkxp, int kx, int fld) {
+    const double2 X = row[kx];
+    const double2 Y = kx == 0 ? cconj(X) : cconj(row[nkxp + kx]);
+    return fld == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
+                    : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
+}
+
+__device__ __forceinline__ double2 unpack_pair(const double2* __restrict__ row, int nkxp, int kx, int fld, bool ok,
+                                               int partner) {
+    double2 mine = make_double2(0.0, 0.0);
+    if (ok && (fld == 0 || kx > 0)) mine = row[fld == 0 ? kx : nkxp + kx];
+    double2 other;
+    other.x = __shfl_xor_sync(0xffffffffu, mine.x, partner);
+    other.y = __shfl_xor_sync(0xffffffffu, mine.y, partner);
+    const double2 X = fld == 0 ? mine : other;
+    const double2 Y = kx == 0 ? cconj(X) : cconj(fld == 0 ? other : mine);
+    return fld == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
+                    : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
+}
+
 template <int NY, bool DRAG>
-__global__ void __launch_bounds__(YFwdCfg<NY, DRAG>::THREADS) k_yfwd(Geom g, int layer0,
-                                                                     const LayerConst* __restrict__ lc,
-                                                                     const double2* __restrict__ q,
-                                                                     const double2* __restrict__ psi,
-                                                                     const double2* __restrict__ huq,
-                                                                     const double2* __restrict__ hvq,
-                                                                     const double2* __restrict__ hdu,
-                                                                     const double2* __restrict__ hdv,
-                                                                     double2* __restrict__ out,
-                                                                     const double2* __restrict__ twy) {
+__global__ void __launch_bounds__(YFwdCfg<NY, DRAG>::THREADS, minb(YFwdCfg<NY, DRAG>::THREADS))
+    k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const double2* __restrict__ q,
+           const double2* __restrict__ psi, const double2* __restrict__ pp, const double2* __restrict__ pd,
+           double2* __restrict__ out, const double2* __restrict__ twy) {
     using C = YFwdCfg<NY, DRAG>;
     extern __shared__ double2 sm[];
     const int tid = threadIdx.x;
     const int l = layer0 + blockIdx.y;
     const int kx0 = blockIdx.x * C::TKX;
-    const int slot = tid / C::G, lane = tid % C::G;
+    const int slot = tid % C::SLOTS, lane = tid / C::SLOTS;
+    const int fld = slot / C::TKX, c = slot % C::TKX;
+    const bool colok = kx0 + c < g.nkx;
     const int nky = g.nky;
     const size_t colbase = (size_t)l * g.nkx;
     const bool bottom = (l == g.nz - 1);
+    double2* xs = sm + slot * C::TS;
+    NoIO none;
 
     if (DRAG) {
         // drag_hat = i ky (|u|u)^ - i kx (|u|v)^ on the bottom layer (QGN_Module.f90:284-292)
-        for (int e = tid; e < C::TKX * NY; e += C::THREADS) {
-            const int y = e / C::TKX, c = e % C::TKX;
-            const size_t src = (size_t)y * g.nkxp + kx0 + c;
-            const bool ok = kx0 + c < g.nkx;
-            sm[c * C::TS + fpad(y)] = ok ? hdu[src] : make_double2(0.0, 0.0);
-            sm[(C::TKX + c) * C::TS + fpad(y)] = ok ? hdv[src] : make_double2(0.0, 0.0);
-        }
-        __syncthreads();
-        fft_block<NY, -1>(sm + slot * C::TS, lane, true, twy);
+        auto ldd = [&](int y) -> double2 {
+            return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, colok, C::TKX);
+        };
+        fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ldd, none);
         const double dc = lc->dragc;
         for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
-            const int c = e / nky, m = e % nky;
-            const int kx = kx0 + c;
+            const int cc = e / nky, m = e % nky;
+            const int kx = kx0 + cc;
             if (kx >= g.nkx) continue;
             const int j = g.jfull(m);
             const double kxv = g.dkx * kx, kyv = g.kyval(j);
-            const double2 fu = sm[c * C::TS + fpad(j)], fv = sm[(C::TKX + c) * C::TS + fpad(j)];
+            const double2 fu = sm[cc * C::TS + fpad(j)], fv = sm[(C::TKX + cc) * C::TS + fpad(j)];
             double2 d = make_double2(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
             d = make_double2(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
             out[(colbase + kx) * nky + m] = make_double2(dc * d.x, dc * d.y);
@@ -337,27 +336,23 @@ __global__ void __launch_bounds__(YFwdCfg<NY, DRAG>::THREADS) k_yfwd(Geom g, int
         __syncthreads();
     }
 
-    for (int e = tid; e < C::TKX * NY; e += C::THREADS) {
-        const int y = e / C::TKX, c = e % C::TKX;
-        const size_t src = ((size_t)l * NY + y) * g.nkxp + kx0 + c;
-        const bool ok = kx0 + c < g.nkx;
-        sm[c * C::TS + fpad(y)] = ok ? huq[src] : make_double2(0.0, 0.0);
-        sm[(C::TKX + c) * C::TS + fpad(y)] = ok ? hvq[src] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    fft_block<NY, -1>(sm + slot * C::TS, lane, true, twy);
+    // the (uq)^ and (vq)^ slots of one column load P[k] and P[nx-k] respectively and swap
+    // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
+    auto ld = [&](int y) -> double2 { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
+                                                         fld, colok, C::TKX); };
+    fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
 
     const double ub = lc->uBar[l], bq = lc->betaq[l];
     const double ek = lc->ekman;
     const bool expl = lc->explicit_diss != 0;
     for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
-        const int c = e / nky, m = e % nky;
-        const int kx = kx0 + c;
+        const int cc = e / nky, m = e % nky;
+        const int kx = kx0 + cc;
         if (kx >= g.nkx) continue;
         const int j = g.jfull(m);
         const double kxv = g.dkx * kx, kyv = g.kyval(j);
         const size_t idx = (colbase + kx) * nky + m;
-        const double2 fuq = sm[c * C::TS + fpad(j)], fvq = sm[(C::TKX + c) * C::TS + fpad(j)];
+        const double2 fuq = sm[cc * C::TS + fpad(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad(j)];
         const double2 qv = q[idx], pv = psi[idx];
         // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)
         const double2 jac = make_double2(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);
@@ -401,53 +396,39 @@ struct X1Cfg {
 };
 
 template <int NX, int EPI>
-__global__ void __launch_bounds__(X1Cfg<NX>::THREADS) k_xinv1(Geom g, const double2* __restrict__ hq,
-                                                              DevScalars* __restrict__ sc, double* __restrict__ outp,
-                                                              const double2* __restrict__ twx) {
+__global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
+    k_xinv1(Geom g, const double2* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
+            const double2* __restrict__ twx) {
     using C = X1Cfg<NX>;
     extern __shared__ double2 sm[];
     __shared__ double smax[32];
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
-    const int rp0 = blockIdx.x * C::RP;
     const int npairs = g.ny / 2;
     const int nkx = g.nkx;
-    for (int e = tid; e < C::RP * NX; e += C::THREADS) {
-        const int r = e / NX, k = e % NX;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
-        double2 a = make_double2(0.0, 0.0);
-        const bool lo = k < nkx, hi = k > NX - nkx;
-        if (lo || hi) {
-            const int kk = lo ? k : NX - k;
-            const size_t r1 = ((size_t)l * g.ny + 2 * rp) * g.nkxp + kk;
-            const double2 F1 = hq[r1], F2 = hq[r1 + g.nkxp];
-            if (k == 0) a = make_double2(F1.x, F2.x);
-            else if (lo) a = make_double2(F1.x - F2.y, F1.y + F2.x);
-            else a = make_double2(F1.x + F2.y, F2.x - F1.y);
-        }
-        sm[r * C::TS + fpad(k)] = a;
-    }
-    __syncthreads();
     const int slot = tid / C::G, lane = tid % C::G;
-    fft_block<NX, +1>(sm + slot * C::TS, lane, (rp0 + slot) < npairs, twx);
+    const int rp = blockIdx.x * C::RP + slot;
+    const bool ok = rp < npairs;
+    const double2* F = hq + ((size_t)l * npairs + rp) * 2 * g.nkxp;   // packed row pair
+    auto ld = [&](int k) -> double2 {
+        if (k < nkx) return F[k];
+        if (k > NX - nkx) return F[g.nkxp + (NX - k)];
+        return make_double2(0.0, 0.0);
+    };
     double mx = 0.0;
-    for (int e = tid; e < C::RP * NX; e += C::THREADS) {
-        const int r = e / NX, x = e % NX;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
-        const double2 a = sm[r * C::TS + fpad(x)];
+    const size_t prow = ((size_t)l * g.ny + 2 * rp) * NX;
+    auto st = [&](int x, double2 a) {
         if (EPI == 0) {
-            // NaN propagates through fmax only if both are NaN; flag it explicitly
+            // NaN is kept as the largest value
             const double m1 = fabs(a.x), m2 = fabs(a.y);
-            if (!(m1 == m1) || !(m2 == m2)) mx = __longlong_as_double(0x7ff8000000000000ULL);
+            if (!(m1 == m1) || !(m2 == m2)) mx = __longlong_as_double(0x7ff8000000000000LL);
             else if (mx == mx) mx = fmax(mx, fmax(m1, m2));
         } else {
-            const size_t row = ((size_t)l * g.ny + 2 * rp) * NX + x;
-            outp[row] = a.x * g.inv_nxny;
-            outp[row + NX] = a.y * g.inv_nxny;
+            outp[prow + x] = a.x * g.inv_nxny;
+            outp[prow + NX + x] = a.y * g.inv_nxny;
         }
-    }
+    };
+    fft_fused<NX, +1, SRC_FN, DST_FN>(sm + slot * C::TS, lane, ok, twx, ld, st);
     if (EPI == 0) {
         // block max of non-negative doubles (NaN as the largest bit pattern)
         unsigned long long bits = (unsigned long long)__double_as_longlong(mx);
@@ -477,64 +458,54 @@ __global__ void __launch_bounds__(X1Cfg<NX>::THREADS) k_xinv1(Geom g, const doub
 // keeping the dealiased modes only.
 // ------------------------------------------------------------------------------------
 template <int NX>
-__global__ void __launch_bounds__(X1Cfg<NX>::THREADS) k_xfwd1(Geom g, const double* __restrict__ phys,
-                                                              double2* __restrict__ hq,
-                                                              const double2* __restrict__ twx) {
+__global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
+    k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx) {
     using C = X1Cfg<NX>;
     extern __shared__ double2 sm[];
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
-    const int rp0 = blockIdx.x * C::RP;
     const int npairs = g.ny / 2;
-    for (int e = tid; e < C::RP * NX; e += C::THREADS) {
-        const int r = e / NX, x = e % NX;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
-        const size_t row = ((size_t)l * g.ny + 2 * rp) * NX + x;
-        sm[r * C::TS + fpad(x)] = make_double2(phys[row], phys[row + NX]);
-    }
-    __syncthreads();
     const int slot = tid / C::G, lane = tid % C::G;
-    fft_block<NX, -1>(sm + slot * C::TS, lane, (rp0 + slot) < npairs, twx);
+    const int rp = blockIdx.x * C::RP + slot;
+    const size_t prow = ((size_t)l * g.ny + 2 * rp) * NX;
+    auto ld = [&](int x) -> double2 { return make_double2(phys[prow + x], phys[prow + NX + x]); };
+    NoIO none;
+    fft_fused<NX, -1, SRC_FN, DST_SMEM>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
     const int nkx = g.nkx;
     for (int e = tid; e < C::RP * nkx; e += C::THREADS) {
         const int r = e / nkx, k = e % nkx;
-        const int rp = rp0 + r;
-        if (rp >= npairs) continue;
+        const int rq = blockIdx.x * C::RP + r;
+        if (rq >= npairs) continue;
         const double2 X = sm[r * C::TS + fpad(k)];
         const double2 Y = cconj(sm[r * C::TS + fpad((NX - k) & (NX - 1))]);
-        const size_t row = ((size_t)l * g.ny + 2 * rp) * g.nkxp + k;
+        const size_t row = ((size_t)l * g.ny + 2 * rq) * g.nkxp + k;
         hq[row] = make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y));
         hq[row + g.nkxp] = make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
     }
 }
 
 template <int NY>
-__global__ void __launch_bounds__(YInvCfg<NY>::THREADS) k_yfwd1(Geom g, const double2* __restrict__ hq,
-                                                                double2* __restrict__ out,
-                                                                const double2* __restrict__ twy) {
+__global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREADS))
+    k_yfwd1(Geom g, const double2* __restrict__ hq, double2* __restrict__ out, const double2* __restrict__ twy) {
     using C = YInvCfg<NY>;
     extern __shared__ double2 sm[];
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
-    const int kx0 = blockIdx.x * C::TKX;
-    const int slot = tid / C::G, lane = tid % C::G;
-    for (int e = tid; e < C::TKX * NY; e += C::THREADS) {
-        const int y = e / C::TKX, c = e % C::TKX;
-        const bool ok = kx0 + c < g.nkx;
-        sm[c * C::TS + fpad(y)] = ok ? hq[((size_t)l * NY + y) * g.nkxp + kx0 + c] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    fft_block<NY, -1>(sm + slot * C::TS, lane, true, twy);
-    const int nky = g.nky;
-    for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
-        const int c = e / nky, m = e % nky;
-        const int kx = kx0 + c;
-        if (kx >= g.nkx) continue;
-        double2 v = sm[c * C::TS + fpad(g.jfull(m))];
+    const int slot = tid % C::TKX, lane = tid / C::TKX;
+    const int kx = blockIdx.x * C::TKX + slot;
+    const bool colok = kx < g.nkx;
+    const size_t colbase = ((size_t)l * g.nkx + kx) * g.nky;
+    auto ld = [&](int y) -> double2 {
+        return colok ? hq[((size_t)l * NY + y) * g.nkxp + kx] : make_double2(0.0, 0.0);
+    };
+    auto st = [&](int j, double2 v) {
+        const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
+        if (!colok || !kept) return;
+        const int m = j < g.kylo ? j : j - g.kyshift;
         if (kx == 0 && m == 0) v = make_double2(0.0, 0.0);
-        out[((size_t)l * g.nkx + kx) * nky + m] = v;
-    }
+        out[colbase + m] = v;
+    };
+    fft_fused<NY, -1, SRC_FN, DST_FN>(sm + slot * C::TS, lane, true, twy, ld, st);
 }
 
 // ------------------------------------------------------------------------------------
@@ -606,8 +577,8 @@ static cudaError_t launch_xpass(const Geom& g, const Buffers& b, bool drag, cuda
             if ((e = set_smem(k_xpass<NX, false>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, nplain);
             QGN_LAUNCH(KID_XPASS, 5.0 * 16.0 * (double)nplain * g.ny * g.nkx, s,
-                       k_xpass<NX, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.hq, b.hp, b.hu, b.huq, b.hvq,
-                                                                             b.hdu, b.hdv, b.twx));
+                       k_xpass<NX, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.hq, b.hp, b.hu, b.hpp, b.hpd,
+                                                                             b.twx));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (drag) {
@@ -615,8 +586,8 @@ static cudaError_t launch_xpass(const Geom& g, const Buffers& b, bool drag, cuda
             if ((e = set_smem(k_xpass<NX, true>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 1);
             QGN_LAUNCH(KID_XPASS, 7.0 * 16.0 * (double)g.ny * g.nkx, s,
-                       k_xpass<NX, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.hq, b.hp, b.hu, b.huq,
-                                                                            b.hvq, b.hdu, b.hdv, b.twx));
+                       k_xpass<NX, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.hq, b.hp, b.hu, b.hpp,
+                                                                            b.hpd, b.twx));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -635,8 +606,8 @@ static cudaError_t launch_yfwd(const Geom& g, const Buffers& b, const double2* q
             dim3 grid((g.nkx + C::TKX - 1) / C::TKX, nplain);
             const double lb = 16.0 * (double)nplain * g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (2.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.lc, q, psi, b.huq, b.hvq, b.hdu,
-                                                                            b.hdv, out, b.twy));
+                       k_yfwd<NY, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.lc, q, psi, b.hpp, b.hpd, out,
+                                                                            b.twy));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (drag) {
@@ -645,8 +616,8 @@ static cudaError_t launch_yfwd(const Geom& g, const Buffers& b, const double2* q
             dim3 grid((g.nkx + C::TKX - 1) / C::TKX, 1);
             const double lb = 16.0 * (double)g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (4.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.lc, q, psi, b.huq, b.hvq,
-                                                                           b.hdu, b.hdv, out, b.twy));
+                       k_yfwd<NY, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.lc, q, psi, b.hpp,
+                                                                           b.hpd, out, b.twy));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         return cudaSuccess;

@@ -122,7 +122,7 @@ extern "C" int qgn_rhs_static(const qgn_params* p, const double* H, const double
     const size_t cb = sizeof(double2) * g.csize();
     size_t off[16];
     size_t total = 0;
-    const size_t sizes[13] = {hb, hb, hb, hb, hb, db, db, cb, cb, cb, sizeof(double2) * (size_t)g.nx,
+    const size_t sizes[13] = {hb, hb, hb, 2 * hb, 0, 2 * db, 0, cb, cb, cb, sizeof(double2) * (size_t)g.nx,
                               sizeof(double2) * (size_t)g.ny, sizeof(LayerConst) + sizeof(ModalConst) + 256};
     for (int i = 0; i < 13; ++i) {
         off[i] = total;
@@ -138,10 +138,8 @@ extern "C" int qgn_rhs_static(const qgn_params* p, const double* H, const double
     b.hq = reinterpret_cast<double2*>(base + off[0]);
     b.hp = reinterpret_cast<double2*>(base + off[1]);
     b.hu = reinterpret_cast<double2*>(base + off[2]);
-    b.huq = reinterpret_cast<double2*>(base + off[3]);
-    b.hvq = reinterpret_cast<double2*>(base + off[4]);
-    b.hdu = reinterpret_cast<double2*>(base + off[5]);
-    b.hdv = reinterpret_cast<double2*>(base + off[6]);
+    b.hpp = reinterpret_cast<double2*>(base + off[3]);
+    b.hpd = reinterpret_cast<double2*>(base + off[5]);
     double2* qc = reinterpret_cast<double2*>(base + off[7]);
     double2* pc = reinterpret_cast<double2*>(base + off[8]);
     double2* oc = reinterpret_cast<double2*>(base + off[9]);

@@ -50,8 +50,8 @@ __device__ __forceinline__ void modal_invert_s(const double* proj, const double*
                     acc.x += c * qv[kk].x;
                     acc.y += c * qv[kk].y;
                 }
-            const double den = -k2 + ev[k];
-            pm[k] = mean_mode ? make_double2(0.0, 0.0) : make_double2((acc.x / Htot) / den, (acc.y / Htot) / den);
+            const double rden = 1.0 / ((-k2 + ev[k]) * Htot);
+            pm[k] = mean_mode ? make_double2(0.0, 0.0) : make_double2(acc.x * rden, acc.y * rden);
         }
     }
 #pragma unroll
@@ -83,8 +83,9 @@ __device__ __forceinline__ void point_k(const Geom& g, size_t p, int& kx, int& m
 }
 
 // ---- ARK stage s (1..5): q_s and psi_s -----------------------------------------------------
-template <int NZ>
-__global__ void __launch_bounds__(256) k_ark_stage(Geom g, int s, StagePtrs sp, const double2* __restrict__ q,
+// S and NZ are template parameters so that every load of the stage is unrolled and in flight.
+template <int S, int NZ>
+__global__ void __launch_bounds__(256) k_ark_stage(Geom g, StagePtrs sp, const double2* __restrict__ q,
                                                    double2* __restrict__ qout, double2* __restrict__ psi,
                                                    const ModalConst* __restrict__ mc,
                                                    const LayerConst* __restrict__ lc,
@@ -109,23 +110,28 @@ __global__ void __launch_bounds__(256) k_ark_stage(Geom g, int s, StagePtrs sp, 
     for (int l = 0; l < NZC; ++l) {
         if (l < nz) {
             const size_t idx = (size_t)l * P + p;
+            double2 nn[S], qq[S];
+#pragma unroll
+            for (int j = 0; j < S; ++j) nn[j] = sp.N[j][idx];
+            qq[0] = q[idx];
+#pragma unroll
+            for (int j = 1; j < S; ++j) qq[j] = sp.Qs[j][idx];
             const double D = A2 * k2 + s_a8[l] * k8;
             double2 acc = make_double2(0.0, 0.0);
-            for (int j = 0; j < s; ++j) {
-                const double a = c_ae[s * 6 + j];
-                const double2 n = sp.N[j][idx];
-                acc.x += a * n.x;
-                acc.y += a * n.y;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const double a = c_ae[S * 6 + j];
+                acc.x += a * nn[j].x;
+                acc.y += a * nn[j].y;
             }
-            for (int j = 0; j < s; ++j) {
-                const double a = c_ai[s * 6 + j];
-                const double2 qj = sp.Qs[j][idx];
-                acc.x += a * (-D * qj.x);
-                acc.y += a * (-D * qj.y);
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const double a = c_ai[S * 6 + j];
+                acc.x += a * (-D * qq[j].x);
+                acc.y += a * (-D * qq[j].y);
             }
             const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
-            const double2 q0 = q[idx];
-            qv[l] = make_double2(Mq * (q0.x + dt * acc.x), Mq * (q0.y + dt * acc.y));
+            qv[l] = make_double2(Mq * (qq[0].x + dt * acc.x), Mq * (qq[0].y + dt * acc.y));
         }
     }
     modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
@@ -244,58 +250,63 @@ template <int POW>
 __global__ void __launch_bounds__(256) k_parseval(Geom g, const double2* __restrict__ f, double* __restrict__ partial) {
     __shared__ double red[8];
     const size_t P = (size_t)g.nkx * g.nky;
-    for (int l = 0; l < g.nz; ++l) {
-        double acc = 0.0;
-        for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
-            int kx, m;
-            double k2;
-            point_k(g, p, kx, m, k2);
-            const double w = kpow<POW>(k2);
-            const double2 v = f[(size_t)l * P + p];
-            if (kx > 0) {
-                acc += 2.0 * w * (v.x * v.x + v.y * v.y);
-            } else {
-                const int j = g.jfull(m);
-                const int jp = (g.ny - j) % g.ny;
-                const bool pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
-                double2 fp = make_double2(0.0, 0.0);
-                if (pk) fp = f[(size_t)l * P + (jp < g.kylo ? jp : jp - g.kyshift)];
-                const double hx = 0.5 * (v.x + fp.x), hy = 0.5 * (v.y - fp.y);
-                acc += (pk ? 1.0 : 2.0) * w * (hx * hx + hy * hy);
-            }
+    const int l = blockIdx.y;
+    double acc = 0.0;
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+        int kx, m;
+        double k2;
+        point_k(g, p, kx, m, k2);
+        const double w = kpow<POW>(k2);
+        const double2 v = f[(size_t)l * P + p];
+        if (kx > 0) {
+            acc += 2.0 * w * (v.x * v.x + v.y * v.y);
+        } else {
+            const int j = g.jfull(m);
+            const int jp = (g.ny - j) % g.ny;
+            const bool pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
+            double2 fp = make_double2(0.0, 0.0);
+            if (pk) fp = f[(size_t)l * P + (jp < g.kylo ? jp : jp - g.kyshift)];
+            const double hx = 0.5 * (v.x + fp.x), hy = 0.5 * (v.y - fp.y);
+            acc += (pk ? 1.0 : 2.0) * w * (hx * hx + hy * hy);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-            partial[(size_t)blockIdx.x * g.nz + l] = t;
-        }
-        __syncthreads();
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        partial[(size_t)l * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// warp-parallel fixed-order sum of one layer's partials (deterministic)
+__device__ __forceinline__ double layer_sum(const double* __restrict__ partial, int l, int nblocks) {
+    double s = 0.0;
+    for (int b = threadIdx.x & 31; b < nblocks; b += 32) s += partial[(size_t)l * nblocks + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
 }
 
 // A8L(k) = (1.3*Lx/(nx*pi))**12 * sqrt(mean(q*d))  with mean(q*d) = S/(nx ny)^2  (ARK43_QGLeith.f90:71-73)
 __global__ void k_leith_final(Geom g, const double* __restrict__ partial, int nblocks, double c12, DevScalars* sc) {
-    const int l = threadIdx.x;
+    const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (l >= g.nz) return;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * g.nz + l];
+    const double s = layer_sum(partial, l, nblocks);
     const double N = (double)g.nx * (double)g.ny;
-    sc->A8L[l] = c12 * sqrt((s / N) / N);
+    if ((threadIdx.x & 31) == 0) sc->A8L[l] = c12 * sqrt((s / N) / N);
 }
 
 // layer KE = 0.5 * S/(nx ny)^2 * H_k/Htot with S the k^2-weighted Parseval sum of psi
 __global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nblocks, const double* __restrict__ Hw,
                            double* __restrict__ ke) {
-    const int l = threadIdx.x;
+    const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (l >= g.nz) return;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * g.nz + l];
+    const double s = layer_sum(partial, l, nblocks);
     const double N = (double)g.nx * (double)g.ny;
-    ke[l] = 0.5 * ((s / N) / N) * Hw[l];
+    if ((threadIdx.x & 31) == 0) ke[l] = 0.5 * ((s / N) / N) * Hw[l];
 }
 
 // isotropic KE spectrum per layer in integer shells round(sqrt(i^2 + jj^2))
@@ -372,18 +383,31 @@ __global__ void k_advance_time(DevScalars* sc) { sc->t = sc->t + sc->dt; }
 // ------------------------------------------------------------------------------------------
 static inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+template <int S>
+static void launch_stage_s(const Geom& g, const Buffers& b, const StagePtrs& sp, dim3 grid, double nb,
+                           cudaStream_t st) {
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 2><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 4><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 8><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 16><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 0><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+    }
+}
+
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
     StagePtrs sp{};
     for (int j = 0; j < 6; ++j) { sp.N[j] = b.N[j]; sp.Qs[j] = b.Qs[j]; }
     const size_t P = (size_t)g.nkx * g.nky;
     dim3 grid(blocks_for(P, 256));
     const double nb = 16.0 * (double)g.csize() * (2.0 * s + 2.0);
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<2><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<4><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
-        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<8><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
-        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<16><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
-        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<0><<<grid, 256, 0, st>>>(g, s, sp, b.q, b.Qs[s], b.psi, b.mc, b.lc, b.sc)); break;
+    switch (s) {
+        case 1: launch_stage_s<1>(g, b, sp, grid, nb, st); break;
+        case 2: launch_stage_s<2>(g, b, sp, grid, nb, st); break;
+        case 3: launch_stage_s<3>(g, b, sp, grid, nb, st); break;
+        case 4: launch_stage_s<4>(g, b, sp, grid, nb, st); break;
+        case 5: launch_stage_s<5>(g, b, sp, grid, nb, st); break;
+        default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
@@ -418,23 +442,29 @@ cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStr
     return cudaGetLastError();
 }
 
+// blocks per layer of the Parseval reductions (the partial buffer holds 512*kMaxNZ doubles)
 static int parseval_blocks(const Geom& g) {
     const size_t P = (size_t)g.nkx * g.nky;
+    const size_t want = (size_t)(2 * 148 + g.nz - 1) / g.nz;   // ~2 blocks per SM over all layers
     size_t nb = (P + 255) / 256;
-    return (int)(nb < 296 ? nb : 296);
+    if (nb > want) nb = want;
+    if (nb > 512) nb = 512;
+    return (int)(nb > 0 ? nb : 1);
 }
 
 cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t st) {
     const int nb = parseval_blocks(g);
-    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st, k_parseval<4><<<nb, 256, 0, st>>>(g, q, b.red));
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_leith_final<<<1, 32, 0, st>>>(g, b.red, nb, c12, b.sc));
+    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
+               k_parseval<4><<<dim3(nb, g.nz), 256, 0, st>>>(g, q, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_leith_final<<<(g.nz + 7) / 8, 256, 0, st>>>(g, b.red, nb, c12, b.sc));
     return cudaGetLastError();
 }
 
 cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t st) {
     const int nb = parseval_blocks(g);
-    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st, k_parseval<1><<<nb, 256, 0, st>>>(g, psi, b.red));
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_ke_final<<<1, 32, 0, st>>>(g, b.red, nb, Hw, ke));
+    QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
+               k_parseval<1><<<dim3(nb, g.nz), 256, 0, st>>>(g, psi, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_ke_final<<<(g.nz + 7) / 8, 256, 0, st>>>(g, b.red, nb, Hw, ke));
     return cudaGetLastError();
 }
 
