@@ -9,6 +9,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <utility>
@@ -140,15 +141,28 @@ int read_scalars(qgn_ctx* ctx, DevScalars* out) {
     return QGN_OK;
 }
 
+// new state from the host: set t, dt and clear a previous failure (halt, status)
 int write_time(qgn_ctx* ctx, double t, double dt) {
-    // t and dt are the first two members of DevScalars
-    double* pin = ctx->host_pin;
-    CK(cudaStreamSynchronize(ctx->stream));
-    pin[0] = t;
-    pin[1] = dt;
-    CK(cudaMemcpyAsync(ctx->b.sc, pin, 2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DevScalars s;
+    RET(read_scalars(ctx, &s));
+    s.t = t;
+    s.dt = dt;
+    s.nonfinite = 0;
+    s.halt = 0;
+    s.status = 0;
+    s.rejects_step = 0;
+    std::memcpy(ctx->host_pin, &s, sizeof(s));
+    CK(cudaMemcpyAsync(ctx->b.sc, ctx->host_pin, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return QGN_OK;
+}
+
+const char* status_text(int st) {
+    switch (st) {
+        case QGN_ERR_NONFINITE: return "non-finite embedded error estimate";
+        case QGN_ERR_REJECT_LIMIT: return "adaptive step rejected max_rejects times in a row";
+        default: return "step failed";
+    }
 }
 
 bool drag_on(const qgn_ctx* ctx) { return ctx->p.C_d != 0.0; }
@@ -168,7 +182,24 @@ int rhs_of(qgn_ctx* ctx, const double2* q, const double2* psi, double2* out) {
 int max_rejects(const qgn_ctx* ctx) { return ctx->p.max_rejects > 0 ? ctx->p.max_rejects : 64; }
 
 // ---- ARK4(3)6L[2]SA, ARK43_QGLeith.f90 / ARK43.f90 ------------------------------------------
-int step_ark(qgn_ctx* ctx, bool leith) {
+// Kernel sequence of one attempt (stages 2..6 with their RHS, update + error combination,
+// error transform, controller).  Shared by the eager path and the graph capture.
+int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop) {
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    for (int s = 1; s < 6; ++s) {
+        CK(launch_ark_stage(g, b, s, st));
+        RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
+    }
+    CK(launch_ark_update(g, b, st));
+    CK(launch_zero_scalar_max(b.sc, st));
+    CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
+    CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, max_rejects(ctx), loop, st));
+    return QGN_OK;
+}
+
+int ark_prologue(qgn_ctx* ctx, bool leith) {
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
@@ -176,28 +207,161 @@ int step_ark(qgn_ctx* ctx, bool leith) {
     b.Qs[0] = b.q;
     CK(launch_modal(g, b.mc, b.q, b.psi, st));
     RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
-    int nrej = 0;
+    return QGN_OK;
+}
+
+int step_ark(qgn_ctx* ctx, bool leith) {
+    Buffers& b = ctx->b;
+    CK(launch_step_gate(b.sc, nullptr, ctx->stream));
+    RET(ark_prologue(ctx, leith));
     for (;;) {
-        for (int s = 1; s < 6; ++s) {
-            CK(launch_ark_stage(g, b, s, st));
-            RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
-        }
-        CK(launch_ark_update(g, b, st));
-        CK(launch_zero_scalar_max(b.sc, st));
-        CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
-        CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, st));
+        RET(ark_attempt(ctx, leith, nullptr));
         DevScalars s;
         RET(read_scalars(ctx, &s));
-        if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite embedded error estimate");
+        if (s.halt) {
+            ctx->halted = true;
+            return set_err(ctx, s.status, status_text(s.status));
+        }
         if (s.accept) {
             std::swap(b.q, b.qnew);
             b.Qs[0] = b.q;
             return QGN_OK;
         }
-        ++ctx->rejects;
-        if (++nrej >= max_rejects(ctx))
-            return set_err(ctx, QGN_ERR_REJECT_LIMIT, "adaptive step rejected max_rejects times in a row");
     }
+}
+
+// ---- CUDA-graph steps for the ARK schemes ------------------------------------------------
+// One executable graph = one TimeStep: a gate kernel opens an IF node while the run is not
+// halted; its body is the prologue (Leith, GetPsi, N1) and a WHILE node whose body is one
+// attempt; the controller kernel sets the WHILE condition (1 = rejected, retry).  The two
+// executables differ only in which state buffer holds q_hat and which receives the update,
+// so consecutive steps alternate between them and no buffer is copied.
+int add_conditional(qgn_ctx* ctx, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &graph, &deps, &nd));
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, graph, deps, nd, &np));
+    CK(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    *body = np.conditional.phGraph_out[0];
+    return QGN_OK;
+}
+
+void snapshot(const qgn_ctx* ctx, long long* out) {
+    for (int k = 0; k < KID_COUNT; ++k) out[k] = ctx->prof.launches[k];
+}
+
+int capture_ark(qgn_ctx* ctx, bool leith, int variant, cudaGraphExec_t* out) {
+    Buffers& b = ctx->b;
+    const Buffers saved = b;
+    b.q = ctx->gbuf[variant];
+    b.qnew = ctx->gbuf[variant ^ 1];
+    b.Qs[0] = b.q;
+    cudaStream_t st = ctx->stream;
+    long long c0[KID_COUNT], c1[KID_COUNT], c2[KID_COUNT], c3[KID_COUNT];
+    int rc = QGN_OK;
+    cudaGraph_t root = nullptr;
+    auto run = [&]() -> int {
+        CK(cudaGraphCreate(&root, 0));
+        cudaGraphConditionalHandle hgate, hloop;
+        CK(cudaGraphConditionalHandleCreate(&hgate, root, 0, 0));
+        snapshot(ctx, c0);
+        CK(cudaStreamBeginCaptureToGraph(st, root, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        CK(launch_step_gate(b.sc, &hgate, st));
+        cudaGraph_t ifbody = nullptr;
+        int r = add_conditional(ctx, hgate, cudaGraphCondTypeIf, &ifbody);
+        cudaGraph_t tmp = nullptr;
+        CK(cudaStreamEndCapture(st, &tmp));
+        if (r != QGN_OK) return r;
+        snapshot(ctx, c1);
+        CK(cudaGraphConditionalHandleCreate(&hloop, ifbody, 0, 0));
+        CK(cudaStreamBeginCaptureToGraph(st, ifbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        r = ark_prologue(ctx, leith);
+        if (r == QGN_OK) {
+            cudaError_t e = launch_set_cond(hloop, 1u, st);
+            if (e != cudaSuccess) r = cuda_err(ctx, "launch_set_cond", e);
+        }
+        cudaGraph_t wbody = nullptr;
+        if (r == QGN_OK) r = add_conditional(ctx, hloop, cudaGraphCondTypeWhile, &wbody);
+        CK(cudaStreamEndCapture(st, &tmp));
+        if (r != QGN_OK) return r;
+        snapshot(ctx, c2);
+        CK(cudaStreamBeginCaptureToGraph(st, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        r = ark_attempt(ctx, leith, &hloop);
+        CK(cudaStreamEndCapture(st, &tmp));
+        if (r != QGN_OK) return r;
+        snapshot(ctx, c3);
+        CK(cudaGraphInstantiate(out, root, 0));
+        return QGN_OK;
+    };
+    const bool timing = ctx->prof.timing;
+    ctx->prof.timing = false;
+    rc = run();
+    ctx->prof.timing = timing;
+    if (root) cudaGraphDestroy(root);
+    // captured launches did not run: take them out of the counters, keep them per graph part
+    for (int k = 0; k < KID_COUNT; ++k) {
+        ctx->g_pro[k] = c2[k] - c1[k] + (c1[k] - c0[k]);   // gate + prologue, once per executed step
+        ctx->g_body[k] = c3[k] - c2[k];                     // once per attempt
+        ctx->prof.launches[k] = c0[k];
+    }
+    b = saved;
+    return rc;
+}
+
+int ensure_ark_graphs(qgn_ctx* ctx, bool leith) {
+    if (ctx->graphs_ready) return QGN_OK;
+    ctx->gbuf[0] = ctx->b.q;
+    ctx->gbuf[1] = ctx->b.qnew;
+    for (int v = 0; v < 2; ++v) {
+        int rc = capture_ark(ctx, leith, v, &ctx->gexec[v]);
+        if (rc != QGN_OK) {
+            for (int w = 0; w < 2; ++w)
+                if (ctx->gexec[w]) { cudaGraphExecDestroy(ctx->gexec[w]); ctx->gexec[w] = nullptr; }
+            cudaGetLastError();
+            ctx->graphs_off = true;
+            return rc;
+        }
+    }
+    ctx->graphs_ready = true;
+    return QGN_OK;
+}
+
+int advance_ark_graph(qgn_ctx* ctx, bool leith, int nsteps) {
+    Buffers& b = ctx->b;
+    DevScalars s0, s1;
+    RET(read_scalars(ctx, &s0));
+    if (s0.halt) {
+        ctx->halted = true;
+        return set_err(ctx, s0.status, status_text(s0.status));
+    }
+    const int par0 = (b.q == ctx->gbuf[0]) ? 0 : 1;
+    int par = par0;
+    for (int i = 0; i < nsteps; ++i) {
+        CK(cudaGraphLaunch(ctx->gexec[par], ctx->stream));
+        par ^= 1;
+    }
+    RET(read_scalars(ctx, &s1));
+    const long long acc = s1.accepted - s0.accepted;
+    const long long att = s1.attempts - s0.attempts;
+    const long long runs = acc + (s1.halt ? 1 : 0);
+    for (int k = 0; k < KID_COUNT; ++k) ctx->prof.launches[k] += runs * ctx->g_pro[k] + att * ctx->g_body[k];
+    ctx->prof.launches[KID_SCALAR] += nsteps - runs;   // gate kernels of skipped steps
+    b.q = ctx->gbuf[par0 ^ (int)(acc & 1)];
+    b.qnew = ctx->gbuf[par0 ^ 1 ^ (int)(acc & 1)];
+    b.Qs[0] = b.q;
+    if (s1.halt) {
+        ctx->halted = true;
+        return set_err(ctx, s1.status, status_text(s1.status));
+    }
+    return QGN_OK;
 }
 
 // ---- Bogacki-Shampine 3(2), BSRK3.f90 -----------------------------------------------------
@@ -210,7 +374,7 @@ int step_bsrk3(qgn_ctx* ctx) {
         RET(rhs_of(ctx, b.q, b.psi, b.N[0]));     // RHS0 (kept between calls, FSAL)
         ctx->first_call = false;
     }
-    int nrej = 0;
+    CK(launch_step_gate(b.sc, nullptr, st));
     for (;;) {
         Combo c1{{b.N[0]}, {0.5}, 1};
         CK(launch_combo(g, b, c1, b.q, b.Qs[1], b.psi, true, st));
@@ -225,18 +389,18 @@ int step_bsrk3(qgn_ctx* ctx) {
         CK(launch_lincomb(g, ce, b.err, st));
         CK(launch_zero_scalar_max(b.sc, st));
         CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
-        CK(launch_controller(g, b, 2, ctx->p.TOL, ctx->p.dt_max, st));
+        CK(launch_controller(g, b, 2, ctx->p.TOL, ctx->p.dt_max, max_rejects(ctx), nullptr, st));
         DevScalars s;
         RET(read_scalars(ctx, &s));
-        if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite embedded error estimate");
+        if (s.halt) {
+            ctx->halted = true;
+            return set_err(ctx, s.status, status_text(s.status));
+        }
         if (s.accept) {
             std::swap(b.q, b.Qs[3]);      // q_hat = q_tmp
             std::swap(b.N[0], b.N[3]);    // RHS0 = RHS3
             return QGN_OK;
         }
-        ++ctx->rejects;
-        if (++nrej >= max_rejects(ctx))
-            return set_err(ctx, QGN_ERR_REJECT_LIMIT, "adaptive step rejected max_rejects times in a row");
     }
 }
 
@@ -311,7 +475,30 @@ int check_state(qgn_ctx* ctx) {
     return QGN_OK;
 }
 
+bool use_graphs(const qgn_ctx* ctx) {
+    if (ctx->graphs_off || ctx->prof.timing) return false;
+    if (ctx->scheme != QGN_SCHEME_ARK43_QGLEITH && ctx->scheme != QGN_SCHEME_ARK43) return false;
+    const char* env = std::getenv("QGN_NO_GRAPHS");
+    return !(env && env[0] && env[0] != '0');
+}
+
 int advance_n(qgn_ctx* ctx, int nsteps) {
+    if (ctx->halted) return set_err(ctx, QGN_ERR_CONFIG, "a previous step failed; upload a new state first");
+    if (nsteps > 0 && use_graphs(ctx)) {
+        const bool leith = ctx->scheme == QGN_SCHEME_ARK43_QGLEITH;
+        if (!ctx->graphs_ready) {
+            // one eager step first: it sets kernel attributes and loads every module function
+            RET(step_once(ctx));
+            --nsteps;
+            if (nsteps == 0) return QGN_OK;
+            if (ensure_ark_graphs(ctx, leith) != QGN_OK) {
+                ctx->last_error.clear();
+                for (int i = 0; i < nsteps; ++i) RET(step_once(ctx));
+                return QGN_OK;
+            }
+        }
+        return advance_ark_graph(ctx, leith, nsteps);
+    }
     for (int i = 0; i < nsteps; ++i) RET(step_once(ctx));
     return QGN_OK;
 }
@@ -324,6 +511,8 @@ bool finite_all(const double* a, size_t n) {
 
 void free_all(qgn_ctx* ctx) {
     ctx->prof.release();
+    for (int w = 0; w < 2; ++w)
+        if (ctx->gexec[w]) { cudaGraphExecDestroy(ctx->gexec[w]); ctx->gexec[w] = nullptr; }
     // stage buffers are swapped between roles while stepping, so memory is released
     // through the ownership list recorded at creation, never through the role pointers
     for (void* p : ctx->owned) cudaFree(p);
@@ -502,6 +691,7 @@ int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt) {
     RET(upload_kept(ctx, q_hat, ctx->b.q));
     ctx->b.Qs[0] = ctx->b.q;
     RET(write_time(ctx, t, dt));
+    ctx->halted = false;
     return QGN_OK;
 }
 
@@ -652,6 +842,7 @@ int qgn_set_state_physical(qgn_ctx* ctx, const double* q_phys, double t, double 
     CK(launch_from_phys(g, b, b.phys, b.q, ctx->stream));
     b.Qs[0] = b.q;
     RET(write_time(ctx, t, dt));
+    ctx->halted = false;
     return QGN_OK;
 }
 
@@ -714,7 +905,9 @@ int qgn_stream(qgn_ctx* ctx, void** stream) {
 
 int qgn_rejects(qgn_ctx* ctx, long long* count) {
     if (!ctx || !count) return QGN_ERR_ARG;
-    *count = ctx->rejects;
+    DevScalars s;
+    RET(read_scalars(ctx, &s));
+    *count = s.rejected;
     return QGN_OK;
 }
 

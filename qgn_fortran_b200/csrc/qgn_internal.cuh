@@ -50,12 +50,20 @@ struct ModalConst {
     double Htot;
 };
 
-// Device scalars of the adaptive controllers.
+// Device scalars of the adaptive controllers.  The controller kernel makes every
+// accept/reject/halt decision on the device, so a step can run without host round trips.
 struct DevScalars {
     double t, dt, err0, err1;
     unsigned long long maxbits;   // bit pattern of max|err_phys| (non-negative doubles)
     int accept;                   // 1 accepted, 0 rejected
     int nonfinite;
+    int halt;                     // sticky: set with status, cleared by a state upload
+    int status;                   // QGN_ERR_* of the failure that set halt
+    int rejects_step;             // consecutive rejections in the current step
+    int pad0;
+    long long accepted;           // accepted steps since creation
+    long long attempts;           // attempts (accepted + rejected) since creation
+    long long rejected;           // rejected attempts since creation
     double A8L[kMaxNZ];
 };
 
@@ -98,11 +106,19 @@ struct qgn_ctx {
     // live in b.N[0..1], err0 / r0 in the device scalars
     bool first_call = true;
     int ab_calls = 0;
-    long long rejects = 0;
+    bool halted = false;           // a step failed; cleared by the next state upload
     double* host_pin = nullptr;    // pinned scalar readback
     std::vector<void*> owned;      // every device allocation made at creation
     std::string last_error;
     qgn::Prof prof;                // launch counts and per-kernel event timing
+    // graph-launched steps (ARK schemes): one executable per role of the two state buffers
+    bool graphs_ready = false;
+    bool graphs_off = false;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    double2* gbuf[2] = {nullptr, nullptr};
+    cudaStream_t body_stream = nullptr;
+    long long g_pro[qgn::KID_COUNT] = {};   // kernel launches per executed step prologue
+    long long g_body[qgn::KID_COUNT] = {};  // kernel launches per attempt
 };
 
 namespace qgn {
@@ -136,7 +152,10 @@ cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t s);
 cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const double2* q, double2* out,
                          double2* psi, bool want_psi, cudaStream_t s);
 cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStream_t s);
-cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, cudaStream_t s);
+cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, int max_rejects,
+                              const cudaGraphConditionalHandle* loop, cudaStream_t s);
+cudaError_t launch_step_gate(DevScalars* sc, const cudaGraphConditionalHandle* gate, cudaStream_t s);
+cudaError_t launch_set_cond(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t s);
 cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t s);
 cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t s);
 cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t s);

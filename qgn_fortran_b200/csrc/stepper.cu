@@ -343,33 +343,58 @@ __global__ void k_ke_spectrum(Geom g, const double2* __restrict__ psi, const dou
 
 // ---- PI controllers (ARK43_QGLeith.f90:124-138, ARK43.f90:108-124, BSRK3.f90:35-48) ----------
 // kind 0: ARK43_QGLeith (reject x0.5, safety 0.2); 1: ARK43 (x0.75, 0.75); 2: BSRK3.
-__global__ void k_controller(int kind, double inv_n, double TOL, double dt_max, DevScalars* sc) {
+// Besides the reference's accept/reject, the device keeps the bounded-retry and NaN checks:
+// a non-finite error estimate or max_rejects consecutive rejections halt the run with a
+// status.  With a loop handle the kernel also sets the condition of the graph's retry loop.
+__global__ void k_controller(int kind, double inv_n, double TOL, double dt_max, int max_rejects,
+                             cudaGraphConditionalHandle loop, int has_loop, DevScalars* sc) {
     const double M = __longlong_as_double((long long)sc->maxbits);
     const double dt = sc->dt;
     double err1;
     if (kind == 2) err1 = dt * (M * inv_n);
     else err1 = dt * M * inv_n;
     sc->err1 = err1;
+    sc->attempts += 1;
+    unsigned int again = 0;
     if (!(err1 == err1) || isinf(err1)) {
         sc->nonfinite = 1;
         sc->accept = 0;
-        return;
-    }
-    if (err1 > TOL) {
+        sc->halt = 1;
+        sc->status = QGN_ERR_NONFINITE;
+    } else if (err1 > TOL) {
         sc->dt = (kind == 0 ? 0.5 : 0.75) * dt;
         sc->accept = 0;
-        return;
+        sc->rejected += 1;
+        sc->rejects_step += 1;
+        if (sc->rejects_step >= max_rejects) {
+            sc->halt = 1;
+            sc->status = QGN_ERR_REJECT_LIMIT;
+        } else {
+            again = 1;
+        }
+    } else {
+        sc->accept = 1;
+        sc->accepted += 1;
+        sc->t = sc->t + dt;
+        const double err0 = sc->err0;
+        double nd;
+        if (kind == 0) nd = dt * pow(0.2 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
+        else if (kind == 1) nd = dt * pow(0.75 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
+        else nd = dt * pow(0.75 * TOL / err1, 0.1) * pow(err0 / err1, 0.4 / 3.0);
+        sc->dt = nd < dt_max ? nd : dt_max;
+        sc->err0 = err1;
     }
-    sc->accept = 1;
-    sc->t = sc->t + dt;
-    const double err0 = sc->err0;
-    double nd;
-    if (kind == 0) nd = dt * pow(0.2 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
-    else if (kind == 1) nd = dt * pow(0.75 * TOL / err1, 0.075) * pow(err0 / err1, 0.1);
-    else nd = dt * pow(0.75 * TOL / err1, 0.1) * pow(err0 / err1, 0.4 / 3.0);
-    sc->dt = nd < dt_max ? nd : dt_max;
-    sc->err0 = err1;
+    if (has_loop) cudaGraphSetConditional(loop, again);
 }
+
+// start of a step: clears the per-step reject count; with a gate handle it also opens the
+// graph's step body only while the run is not halted
+__global__ void k_step_gate(DevScalars* sc, cudaGraphConditionalHandle gate, int has_gate) {
+    sc->rejects_step = 0;
+    if (has_gate) cudaGraphSetConditional(gate, sc->halt == 0 ? 1u : 0u);
+}
+
+__global__ void k_set_cond(cudaGraphConditionalHandle h, unsigned int v) { cudaGraphSetConditional(h, v); }
 
 __global__ void k_zero_max(DevScalars* sc) {
     sc->maxbits = 0ULL;
@@ -477,8 +502,21 @@ cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* 
     return cudaGetLastError();
 }
 
-cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_controller<<<1, 1, 0, st>>>(kind, g.inv_nxny, TOL, dt_max, b.sc));
+cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, int max_rejects,
+                              const cudaGraphConditionalHandle* loop, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st,
+               k_controller<<<1, 1, 0, st>>>(kind, g.inv_nxny, TOL, dt_max, max_rejects, loop ? *loop : 0,
+                                             loop ? 1 : 0, b.sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_gate(DevScalars* sc, const cudaGraphConditionalHandle* gate, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_step_gate<<<1, 1, 0, st>>>(sc, gate ? *gate : 0, gate ? 1 : 0));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_cond(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_set_cond<<<1, 1, 0, st>>>(h, v));
     return cudaGetLastError();
 }
 
