@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     return ap.parse_args()
 
 
@@ -270,6 +271,40 @@ def ours_arm(args):
         e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
                "d2h_bytes_per_step": kept, "ms_per_step": ems / args.steps}
 
+    # ---- the same workload in the mixed mode (FP32 transforms/RHS/stages, FP64 state and control)
+    mixed = None
+    if not args.no_mixed:
+        gm = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme, precision="mixed")
+        gm.initialize(w.qp, 0.0, w.dt0)
+        if args.warmup > 0:
+            gm.advance_resident(args.warmup)
+        smp = _lib.C.c_void_p()
+        gm.lib.qgn_stream(gm.ctx, _lib.C.byref(smp))
+        mstream = torch.cuda.ExternalStream(smp.value)
+        tm0, _ = gm.time()
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(mstream)
+        gm.advance_resident(args.steps)
+        m1.record(mstream)
+        m1.synchronize()
+        mms = m0.elapsed_time(m1)
+        tm1, _ = gm.time()
+        mdays = (tm1 - tm0) / DAY
+        if ws > 1:
+            tt = torch.tensor([mms, mdays], dtype=torch.float64, device="cuda")
+            mx = tt.clone()
+            torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+            sm = tt.clone()
+            torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
+            mms, mdays = float(mx[0]), float(sm[1])
+        mixed = {"value": mdays / (mms / 1000.0), "unit": UNIT, "ms_per_step": mms / args.steps,
+                 "ms_per_step_vs_fp64": (ms_all / args.steps) / (mms / args.steps),
+                 "dtype": "f32 transforms/RHS/stage storage, f64 state/GetPsi/error norm/controller"}
+        gm.cleanup()
+
     if rank != 0:
         g.cleanup()
         if ws > 1:
@@ -303,7 +338,7 @@ def ours_arm(args):
                        "scheme": w.scheme, "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
                        "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects()},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "gpu_launches": launches,
             "clocks": clk, "kernels": kernels}
     print(json.dumps(line), flush=True)
     g.cleanup()

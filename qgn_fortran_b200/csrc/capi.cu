@@ -184,15 +184,26 @@ int max_rejects(const qgn_ctx* ctx) { return ctx->p.max_rejects > 0 ? ctx->p.max
 // ---- ARK4(3)6L[2]SA, ARK43_QGLeith.f90 / ARK43.f90 ------------------------------------------
 // Kernel sequence of one attempt (stages 2..6 with their RHS, update + error combination,
 // error transform, controller).  Shared by the eager path and the graph capture.
+bool mixed(const qgn_ctx* ctx) { return ctx->precision == QGN_PREC_MIXED; }
+
+template <class T>
+float2* f32(T* p) { return reinterpret_cast<float2*>(p); }
+
 int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop) {
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
     for (int s = 1; s < 6; ++s) {
-        CK(launch_ark_stage(g, b, s, st));
-        RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
+        if (mixed(ctx)) {
+            CK(launch_ark_stage_mixed(g, b, s, st));
+            CK(launch_rhs32(g, b, f32(b.Qs[s]), f32(b.psi), f32(b.N[s]), drag_on(ctx), st));
+        } else {
+            CK(launch_ark_stage(g, b, s, st));
+            RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
+        }
     }
-    CK(launch_ark_update(g, b, st));
+    if (mixed(ctx)) CK(launch_ark_update_mixed(g, b, st));
+    else CK(launch_ark_update(g, b, st));
     CK(launch_zero_scalar_max(b.sc, st));
     CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
     CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, max_rejects(ctx), loop, st));
@@ -205,8 +216,14 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
     cudaStream_t st = ctx->stream;
     if (leith) CK(launch_leith(g, b, b.q, leith_c12(ctx->p), st));
     b.Qs[0] = b.q;
-    CK(launch_modal(g, b.mc, b.q, b.psi, st));
-    RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
+    if (mixed(ctx)) {
+        // FP32 copy of q_hat for the FP32 RHS lives in the error buffer until the update
+        CK(launch_modal_mixed(g, b, b.q, f32(b.err), f32(b.psi), st));
+        CK(launch_rhs32(g, b, f32(b.err), f32(b.psi), f32(b.N[0]), drag_on(ctx), st));
+    } else {
+        CK(launch_modal(g, b.mc, b.q, b.psi, st));
+        RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
+    }
     return QGN_OK;
 }
 
@@ -542,7 +559,10 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
         return QGN_ERR_CONFIG;
     if (p->nz < 2 || p->nz > kMaxNZ) return QGN_ERR_CONFIG;
     if (scheme < 0 || scheme > 4) return QGN_ERR_CONFIG;
-    if (precision != QGN_PREC_FP64) return QGN_ERR_CONFIG;
+    if (precision != QGN_PREC_FP64 && precision != QGN_PREC_MIXED) return QGN_ERR_CONFIG;
+    // the mixed mode is built for the ARK4(3)6L[2]SA schemes
+    if (precision == QGN_PREC_MIXED && scheme != QGN_SCHEME_ARK43_QGLEITH && scheme != QGN_SCHEME_ARK43)
+        return QGN_ERR_CONFIG;
     if (!(p->Lx > 0) || !(p->Ly > 0) || !(p->Htot > 0)) return QGN_ERR_CONFIG;
     const int nz = p->nz;
     if (!finite_all(H, nz) || !finite_all(uBar, nz) || !finite_all(qyBar, nz) || !finite_all(Modes, (size_t)nz * nz) ||
@@ -604,6 +624,7 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     AL(b.hpd, (size_t)2 * g.ny * g.nkxp);
     AL(b.xfer, C);
     AL(b.twx, (size_t)g.nx); AL(b.twy, (size_t)g.ny);
+    AL(b.twx32, (size_t)g.nx); AL(b.twy32, (size_t)g.ny);
     AL(b.red, (size_t)512 * kMaxNZ);
     AL(b.Hw, (size_t)kMaxNZ);
     AL(b.lc, 1); AL(b.mc, 1); AL(b.sc, 1);
@@ -636,10 +657,19 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     }
     if (rc == QGN_OK) {
         std::vector<double2> tw;
+        std::vector<float2> tw32;
+        auto to32 = [&]() {
+            tw32.resize(tw.size());
+            for (size_t i = 0; i < tw.size(); ++i) tw32[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+        };
         make_twiddles(g.nx, tw);
+        to32();
         cudaError_t e = cudaMemcpy(b.twx, tw.data(), sizeof(double2) * g.nx, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b.twx32, tw32.data(), sizeof(float2) * g.nx, cudaMemcpyHostToDevice);
         make_twiddles(g.ny, tw);
+        to32();
         if (e == cudaSuccess) e = cudaMemcpy(b.twy, tw.data(), sizeof(double2) * g.ny, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b.twy32, tw32.data(), sizeof(float2) * g.ny, cudaMemcpyHostToDevice);
         LayerConst lc;
         std::memset(&lc, 0, sizeof(lc));
         for (int k = 0; k < nz; ++k) {
@@ -749,6 +779,15 @@ int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
     CK(cudaSetDevice(ctx->device));
     Buffers& b = ctx->b;
     RET(upload_kept(ctx, q_hat, b.err));
+    if (mixed(ctx)) {
+        // FP32 RHS: the FP32 state copy goes to N[5], the FP32 result to qnew, widened into err
+        CK(launch_modal_mixed(ctx->g, b, b.err, f32(b.N[5]), f32(b.psi), ctx->stream));
+        CK(launch_rhs32(ctx->g, b, f32(b.N[5]), f32(b.psi), f32(b.qnew), drag_on(ctx), ctx->stream));
+        CK(launch_f2d(ctx->g.csize(), f32(b.qnew), b.err, ctx->stream));
+        RET(download_full(ctx, b.err, rhs));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return QGN_OK;
+    }
     CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
     RET(rhs_of(ctx, b.err, b.psi, b.qnew));
     RET(download_full(ctx, b.qnew, rhs));

@@ -18,15 +18,27 @@
 
 namespace qgn {
 
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// complex arithmetic on double2 (FP64 path) and float2 (FP32 path of the mixed mode)
+template <class CT> struct CTraits;
+template <> struct CTraits<double2> {
+    using R = double;
+    __host__ __device__ static double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <> struct CTraits<float2> {
+    using R = float;
+    __host__ __device__ static float2 make(float a, float b) { return make_float2(a, b); }
+};
+template <class CT>
+__device__ __forceinline__ CT cmk(typename CTraits<CT>::R a, typename CTraits<CT>::R b) {
+    return CTraits<CT>::make(a, b);
 }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-// (i * s) * a for real s
-__device__ __forceinline__ double2 cmul_i(double2 a, double s) { return make_double2(-s * a.y, s * a.x); }
+template <class CT> __device__ __forceinline__ CT cadd(CT a, CT b) { return cmk<CT>(a.x + b.x, a.y + b.y); }
+template <class CT> __device__ __forceinline__ CT csub(CT a, CT b) { return cmk<CT>(a.x - b.x, a.y - b.y); }
+template <class CT> __device__ __forceinline__ CT cmul(CT a, CT b) {
+    return cmk<CT>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <class CT> __device__ __forceinline__ CT cconj(CT a) { return cmk<CT>(a.x, -a.y); }
+template <class CT> __device__ __forceinline__ CT czero() { return cmk<CT>(0, 0); }
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
 
@@ -36,23 +48,24 @@ __device__ __forceinline__ int fpad(int p) { return p + (p >> 4); }
 __host__ __device__ constexpr int fpadlen(int N) { return N + (N >> 4); }
 
 // Multiply by exp(DIR * 2*pi*i * m/16); m is a compile-time constant after unrolling.
-template <int DIR>
-__device__ __forceinline__ double2 rot16(double2 a, int m) {
-    constexpr double C1 = 0.92387953251128675613;  // cos(pi/8)
-    constexpr double S1 = 0.38268343236508977173;  // sin(pi/8)
-    constexpr double HH = 0.70710678118654752440;  // sqrt(2)/2
+template <int DIR, class CT>
+__device__ __forceinline__ CT rot16(CT a, int m) {
+    using R = typename CTraits<CT>::R;
+    constexpr R C1 = (R)0.92387953251128675613;  // cos(pi/8)
+    constexpr R S1 = (R)0.38268343236508977173;  // sin(pi/8)
+    constexpr R HH = (R)0.70710678118654752440;  // sqrt(2)/2
     switch (m & 15) {
         case 0: return a;
-        case 4: return DIR > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
-        case 8: return make_double2(-a.x, -a.y);
-        case 12: return DIR > 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
-        case 2: { double s = DIR * HH; return make_double2(HH * a.x - s * a.y, s * a.x + HH * a.y); }
-        case 6: { double s = DIR * HH; return make_double2(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
-        case 10: { double s = -DIR * HH; return make_double2(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
-        case 14: { double s = -DIR * HH; return make_double2(HH * a.x - s * a.y, s * a.x + HH * a.y); }
+        case 4: return DIR > 0 ? cmk<CT>(-a.y, a.x) : cmk<CT>(a.y, -a.x);
+        case 8: return cmk<CT>(-a.x, -a.y);
+        case 12: return DIR > 0 ? cmk<CT>(a.y, -a.x) : cmk<CT>(-a.y, a.x);
+        case 2: { R s = DIR * HH; return cmk<CT>(HH * a.x - s * a.y, s * a.x + HH * a.y); }
+        case 6: { R s = DIR * HH; return cmk<CT>(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
+        case 10: { R s = -DIR * HH; return cmk<CT>(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
+        case 14: { R s = -DIR * HH; return cmk<CT>(HH * a.x - s * a.y, s * a.x + HH * a.y); }
         default: break;
     }
-    double c, s;
+    R c, s;
     switch (m & 15) {
         case 1: c = C1; s = S1; break;
         case 3: c = S1; s = C1; break;
@@ -64,21 +77,22 @@ __device__ __forceinline__ double2 rot16(double2 a, int m) {
         default: c = C1; s = -S1; break;  // 15
     }
     s = DIR * s;
-    return make_double2(a.x * c - a.y * s, a.x * s + a.y * c);
+    return cmk<CT>(a.x * c - a.y * s, a.x * s + a.y * c);
 }
 
 // In-register DFT of length R (1,2,4,8,16), natural order in and out, sign DIR.
 template <int R, int DIR>
 struct RegDFT {
-    __device__ __forceinline__ static void run(double2* v) {
-        double2 e[R / 2], o[R / 2];
+    template <class CT>
+    __device__ __forceinline__ static void run(CT* v) {
+        CT e[R / 2], o[R / 2];
 #pragma unroll
         for (int i = 0; i < R / 2; ++i) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
         RegDFT<R / 2, DIR>::run(e);
         RegDFT<R / 2, DIR>::run(o);
 #pragma unroll
         for (int k = 0; k < R / 2; ++k) {
-            double2 t = rot16<DIR>(o[k], k * (16 / R));
+            CT t = rot16<DIR>(o[k], k * (16 / R));
             v[k] = cadd(e[k], t);
             v[k + R / 2] = csub(e[k], t);
         }
@@ -86,12 +100,14 @@ struct RegDFT {
 };
 template <int DIR>
 struct RegDFT<1, DIR> {
-    __device__ __forceinline__ static void run(double2*) {}
+    template <class CT>
+    __device__ __forceinline__ static void run(CT*) {}
 };
 template <int DIR>
 struct RegDFT<2, DIR> {
-    __device__ __forceinline__ static void run(double2* v) {
-        double2 a = v[0], b = v[1];
+    template <class CT>
+    __device__ __forceinline__ static void run(CT* v) {
+        CT a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     }
@@ -106,31 +122,31 @@ struct FFTShape {
 // Inter-pass twiddles of one radix-R butterfly: v[r] *= w^r, w = exp(DIR 2 pi i k/(NS R)).
 // w^(2^q) come from the table tw[m] = exp(-2 pi i m/N) (conjugated for DIR=+1); the other
 // powers are products of at most three table values, formed just before use.
-template <int N, int NS, int R, int DIR>
-__device__ __forceinline__ void apply_twiddles(double2* v, int k, const double2* __restrict__ tw) {
+template <int N, int NS, int R, int DIR, class CT>
+__device__ __forceinline__ void apply_twiddles(CT* v, int k, const CT* __restrict__ tw) {
     if constexpr (NS > 1) {
         constexpr int S = N / (NS * R);
         const int kS = k * S;
         auto ldw = [&](int r) {
-            const double2 t = __ldg(&tw[r * kS]);
+            const CT t = __ldg(&tw[r * kS]);
             return DIR > 0 ? cconj(t) : t;
         };
-        const double2 w1 = ldw(1);
+        const CT w1 = ldw(1);
         v[1] = cmul(v[1], w1);
         if constexpr (R > 2) {
-            const double2 w2 = ldw(2);
-            const double2 w3 = cmul(w2, w1);
+            const CT w2 = ldw(2);
+            const CT w3 = cmul(w2, w1);
             v[2] = cmul(v[2], w2);
             v[3] = cmul(v[3], w3);
             if constexpr (R > 4) {
-                const double2 w4 = ldw(4);
-                const double2 w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+                const CT w4 = ldw(4);
+                const CT w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
                 v[4] = cmul(v[4], w4);
                 v[5] = cmul(v[5], w5);
                 v[6] = cmul(v[6], w6);
                 v[7] = cmul(v[7], w7);
                 if constexpr (R > 8) {
-                    const double2 w8 = ldw(8);
+                    const CT w8 = ldw(8);
                     v[8] = cmul(v[8], w8);
                     v[9] = cmul(v[9], cmul(w8, w1));
                     v[10] = cmul(v[10], cmul(w8, w2));
@@ -155,15 +171,14 @@ enum FftDst { DST_SMEM = 0, DST_FN = 1 };
 // the shared buffer it overwrites syncs between its reads and writes, and a pass that
 // writes the shared buffer syncs after its writes.  With SRC_FN the caller guarantees
 // that no thread still reads x when the pass starts writing it.
-template <int N, int NS, int DIR, int SRC, int DST, class Ld, class St>
-__device__ __forceinline__ void fft_pass_io(double2* x, int lane, bool active, const double2* __restrict__ tw,
-                                            Ld& ld, St& st) {
+template <int N, int NS, int DIR, int SRC, int DST, class CT, class Ld, class St>
+__device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
     constexpr int T = FFTShape<N>::T;
     constexpr int G = FFTShape<N>::G;
     constexpr int R = (N / NS >= 16) ? 16 : N / NS;
     constexpr int BPT = T / R;
     constexpr int STRIDE = N / R;
-    double2 v[T];
+    CT v[T];
     if (active) {
 #pragma unroll
         for (int b = 0; b < BPT; ++b) {
@@ -196,9 +211,8 @@ __device__ __forceinline__ void fft_pass_io(double2* x, int lane, bool active, c
     if constexpr (DST == DST_SMEM) __syncthreads();
 }
 
-template <int N, int NS, int DIR, int SRC0, int DSTL, class Ld, class St>
-__device__ __forceinline__ void fft_rec(double2* x, int lane, bool active, const double2* __restrict__ tw, Ld& ld,
-                                        St& st) {
+template <int N, int NS, int DIR, int SRC0, int DSTL, class CT, class Ld, class St>
+__device__ __forceinline__ void fft_rec(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
     constexpr int R = (N / NS >= 16) ? 16 : N / NS;
     constexpr bool FIRST = (NS == 1);
     constexpr bool LAST = (NS * R == N);
@@ -208,25 +222,26 @@ __device__ __forceinline__ void fft_rec(double2* x, int lane, bool active, const
     if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
 }
 
-struct NoIO {
-    __device__ double2 operator()(int) const { return make_double2(0.0, 0.0); }
-    __device__ void operator()(int, double2) const {}
+template <class CT>
+struct NoIOT {
+    __device__ CT operator()(int) const { return czero<CT>(); }
+    __device__ void operator()(int, CT) const {}
 };
+using NoIO = NoIOT<double2>;
 
 // N-point transform of one slot by the G threads with lane in [0,G), reading its input
 // through ld (SRC0 = SRC_FN / SRC_FN_SMEM) or from x (SRC_SMEM, written and synced by the
 // caller) and delivering its output through st (DSTL = DST_FN) or into x (DST_SMEM, synced
 // on return).  Every thread of the block calls this (it may contain __syncthreads).
-template <int N, int DIR, int SRC0, int DSTL, class Ld, class St>
-__device__ __forceinline__ void fft_fused(double2* x, int lane, bool active, const double2* __restrict__ tw, Ld ld,
-                                          St st) {
+template <int N, int DIR, int SRC0, int DSTL, class CT, class Ld, class St>
+__device__ __forceinline__ void fft_fused(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld ld, St st) {
     fft_rec<N, 1, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
 }
 
 // In-place N-point transform of the padded array x (caller syncs before; ends with a barrier).
-template <int N, int DIR>
-__device__ __forceinline__ void fft_block(double2* x, int lane, bool active, const double2* __restrict__ tw) {
-    NoIO io;
+template <int N, int DIR, class CT>
+__device__ __forceinline__ void fft_block(CT* x, int lane, bool active, const CT* __restrict__ tw) {
+    NoIOT<CT> io;
     fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM>(x, lane, active, tw, io, io);
 }
 

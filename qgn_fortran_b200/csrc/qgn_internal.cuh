@@ -84,6 +84,8 @@ struct Buffers {
     double* phys = nullptr;      // physical field [nz][ny][nx] (lazy)
     double2* twx = nullptr;      // twiddles exp(-2 pi i m/nx)
     double2* twy = nullptr;      // twiddles exp(-2 pi i m/ny)
+    float2* twx32 = nullptr;     // the same rounded to FP32 (mixed mode)
+    float2* twy32 = nullptr;
     double* red = nullptr;       // reduction partials
     double* Hw = nullptr;        // H(k)/Htot per layer
     double* diag = nullptr;      // diagnostics output (lazy)
@@ -127,6 +129,8 @@ namespace qgn {
 cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, double2* psi, cudaStream_t s);
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
                        bool do_drag, cudaStream_t s);
+cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const float2* psi, float2* out, bool do_drag,
+                         cudaStream_t s);
 // y-inverse + x-pass of one compact field with a max|.| reduction into sc->maxbits
 cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s);
 // physical field (c2r/(nx*ny)) of a compact field into b.phys ([nz][ny][nx])
@@ -149,6 +153,11 @@ struct Combo {
 cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t s);
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
 cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t s);
+cudaError_t launch_ark_stage_mixed(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
+cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_t s);
+cudaError_t launch_modal_mixed(const Geom& g, const Buffers& b, const double2* q, float2* q32, float2* psi32,
+                               cudaStream_t s);
+cudaError_t launch_f2d(size_t n, const float2* a, double2* b, cudaStream_t s);
 cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const double2* q, double2* out,
                          double2* psi, bool want_psi, cudaStream_t s);
 cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStream_t s);

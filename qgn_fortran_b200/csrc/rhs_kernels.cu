@@ -1,4 +1,4 @@
-// rhs_kernels.cu -- the spectral right-hand side of QGN on sm_100a (FP64).
+// rhs_kernels.cu -- the spectral right-hand side of QGN on sm_100a (FP64, and FP32 for the mixed mode).
 //
 // One GetRHS (QGN_Module.f90:258-296) = GetPsi + Jacobian + linear terms + drag +
 // DeAlias is evaluated as three streaming passes over HBM plus the modal inversion
@@ -30,47 +30,55 @@ namespace qgn {
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
 
-// slot stride of a padded transform such that slot*stride spreads 16-byte bank groups
-__host__ __device__ constexpr int slot_stride(int N, int target_mod8) {
-    return fpadlen(N) + ((target_mod8 - (fpadlen(N) % 8)) + 8) % 8;
+// slot stride (in elements) of a padded transform such that slot*stride spreads the bank
+// groups of one shared-memory wavefront: W = 128 bytes / element size elements per wavefront
+// (8 for double2, 16 for float2); target is the stride's residue mod W.
+__host__ __device__ constexpr int slot_stride(int N, int target, int elem_bytes = 16) {
+    return fpadlen(N) + ((target - (fpadlen(N) % (128 / elem_bytes))) + (128 / elem_bytes)) % (128 / elem_bytes);
+}
+// residue for `slots` lane-interleaved slots: consecutive threads hit different slots
+__host__ __device__ constexpr int interleave_target(int slots, int elem_bytes) {
+    return slots >= 128 / elem_bytes ? 1 : (128 / elem_bytes) / slots;
 }
 
 // minimum resident CTAs for __launch_bounds__ such that a thread keeps up to maxregs registers
 __host__ __device__ constexpr int minb(int threads, int maxregs = 128) {
     return cmax(1, cmin(8, 65536 / (threads * maxregs)));
 }
+// register budget per thread: an FP32 transform holds half the register bytes of an FP64 one
+template <class CT>
+__host__ __device__ constexpr int regcap(int fp64 = 128, int fp32 = 64) { return sizeof(CT) == 16 ? fp64 : fp32; }
 
 // y-pass tiles: TKX kx columns per CTA, lane-interleaved (slot = tid % TKX) so that one
 // warp touches 8 consecutive y rows of TKX adjacent columns: 16*TKX-byte segments in the
 // half-transformed row layout, 128-byte segments in the compact column layout.
-template <int NY>
+template <int NY, class CT = double2>
 struct YInvCfg {
     static constexpr int G = FFTShape<NY>::G;
-    // <= 16 so that the row partner of a lane (thread tid ^ TKX) is in the same warp
     static constexpr int TKX = cmin(cmax(4, 128 / G), 16);
     static constexpr int THREADS = TKX * G;
-    static constexpr int TS = slot_stride(NY, TKX >= 8 ? 1 : 8 / TKX);
-    static constexpr int SMEM = TKX * TS * (int)sizeof(double2);
+    static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT));
+    static constexpr int SMEM = TKX * TS * (int)sizeof(CT);
 };
 
-template <int NX, bool DRAG>
+template <int NX, bool DRAG, class CT = double2>
 struct XCfg {
     static constexpr int G = FFTShape<NX>::G;
     static constexpr int RP = cmax(1, 64 / G);         // row pairs per CTA
     static constexpr int SP = DRAG ? 4 : 3;             // slots per row pair
     static constexpr int THREADS = SP * RP * G;
     static constexpr int TS = slot_stride(NX, 2);
-    static constexpr int SMEM = SP * RP * TS * (int)sizeof(double2);
+    static constexpr int SMEM = SP * RP * TS * (int)sizeof(CT);
 };
 
-template <int NY, bool DRAG>
+template <int NY, bool DRAG, class CT = double2>
 struct YFwdCfg {
     static constexpr int G = FFTShape<NY>::G;
     static constexpr int TKX = cmin(cmax(2, 64 / G), 16);   // tid ^ TKX stays in the warp
     static constexpr int SLOTS = 2 * TKX;
     static constexpr int THREADS = SLOTS * G;
-    static constexpr int TS = slot_stride(NY, SLOTS >= 8 ? 1 : 8 / SLOTS);
-    static constexpr int SMEM = SLOTS * TS * (int)sizeof(double2);
+    static constexpr int TS = slot_stride(NY, interleave_target(SLOTS, (int)sizeof(CT)), (int)sizeof(CT));
+    static constexpr int SMEM = SLOTS * TS * (int)sizeof(CT);
 };
 
 // ------------------------------------------------------------------------------------
@@ -117,7 +125,7 @@ __device__ __forceinline__ void modal_invert(const double* __restrict__ proj, co
 }
 
 template <int NZ>
-__global__ void __launch_bounds__(256) k_modal(Geom g, const ModalConst* __restrict__ mc,
+__global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __restrict__ mc,
                                                const double2* __restrict__ q, double2* __restrict__ psi) {
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
@@ -152,11 +160,13 @@ __global__ void __launch_bounds__(256) k_modal(Geom g, const ModalConst* __restr
 // way, which the forward y pass splits into (uq)^ = (P[k] + conj P[nx-k])/2 and
 // (vq)^ = (P[k] - conj P[nx-k])/(2i).
 // ------------------------------------------------------------------------------------
-__device__ __forceinline__ double2 pack_lo(double2 f1, double2 f2, bool k0) {
-    return k0 ? make_double2(f1.x, f2.x) : make_double2(f1.x - f2.y, f1.y + f2.x);
+template <class CT>
+__device__ __forceinline__ CT pack_lo(CT f1, CT f2, bool k0) {
+    return k0 ? cmk<CT>(f1.x, f2.x) : cmk<CT>(f1.x - f2.y, f1.y + f2.x);
 }
-__device__ __forceinline__ double2 pack_hi(double2 f1, double2 f2) {
-    return make_double2(f1.x + f2.y, f2.x - f1.y);
+template <class CT>
+__device__ __forceinline__ CT pack_hi(CT f1, CT f2) {
+    return cmk<CT>(f1.x + f2.y, f2.x - f1.y);
 }
 
 // ------------------------------------------------------------------------------------
@@ -166,12 +176,14 @@ __device__ __forceinline__ double2 pack_hi(double2 f1, double2 f2) {
 // band); the transformed column stays in shared memory, where a packing loop pairs rows
 // y and y+1 and writes the two packed arrays with TKX-wide coalesced stores.
 // ------------------------------------------------------------------------------------
-template <int NY, int NF>
-__global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREADS))
-    k_yinv(Geom g, const double2* __restrict__ q, const double2* __restrict__ psi, double2* __restrict__ pq,
-           double2* __restrict__ pv, double2* __restrict__ pu, const double2* __restrict__ twy) {
-    using C = YInvCfg<NY>;
-    extern __shared__ double2 sm[];
+template <int NY, int NF, class CT>
+__global__ void __launch_bounds__(YInvCfg<NY, CT>::THREADS, minb(YInvCfg<NY, CT>::THREADS, regcap<CT>()))
+    k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
+           CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
+    using C = YInvCfg<NY, CT>;
+    using RT = typename CTraits<CT>::R;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    CT* sm = reinterpret_cast<CT*>(sm_raw);
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
     const int kx0 = blockIdx.x * C::TKX;
@@ -179,37 +191,37 @@ __global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREAD
     const int kx = kx0 + slot;
     const bool colok = kx < g.nkx;
     const size_t colbase = ((size_t)l * g.nkx + kx) * g.nky;
-    const double kxv = g.dkx * kx;
-    double2* xs = sm + slot * C::TS;
-    NoIO none;
+    const RT kxv = (RT)(g.dkx * kx);
+    CT* xs = sm + slot * C::TS;
+    NoIOT<CT> none;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-        const double2* src = (f == 0) ? q : psi;
-        double2* dst = (f == 0) ? pq : (f == 1 ? pu : pv);
-        auto ld = [&](int j) -> double2 {
+        const CT* src = (f == 0) ? q : psi;
+        CT* dst = (f == 0) ? pq : (f == 1 ? pu : pv);
+        auto ld = [&](int j) -> CT {
             const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
-            if (!colok || !kept) return make_double2(0.0, 0.0);
-            double2 v = src[colbase + (j < g.kylo ? j : j - g.kyshift)];
+            if (!colok || !kept) return cmk<CT>(0.0, 0.0);
+            CT v = src[colbase + (j < g.kylo ? j : j - g.kyshift)];
             if (f == 1) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
-                const double kyv = g.kyval(j);
-                v = make_double2(kyv * v.y, -kyv * v.x);
+                const RT kyv = (RT)g.kyval(j);
+                v = cmk<CT>(kyv * v.y, -kyv * v.x);
             } else if (f == 2) {   // v_hat = i kx psi_hat  (QGN_Module.f90:224)
-                v = make_double2(-kxv * v.y, kxv * v.x);
+                v = cmk<CT>(-kxv * v.y, kxv * v.x);
             }
             return v;
         };
         fft_fused<NY, +1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
         // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
-        double2* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
+        CT* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
         for (int e = tid; e < (NY / 2) * C::TKX; e += C::THREADS) {
             const int p = e / C::TKX, c = e % C::TKX;
             const int k = kx0 + c;
             if (k >= g.nkxp) continue;
-            const double2 f1 = sm[c * C::TS + fpad(2 * p)], f2 = sm[c * C::TS + fpad(2 * p + 1)];
+            const CT f1 = sm[c * C::TS + fpad(2 * p)], f2 = sm[c * C::TS + fpad(2 * p + 1)];
             const bool ok = k < g.nkx;
-            double2* row = dl + (size_t)p * 2 * g.nkxp;
-            row[k] = ok ? pack_lo(f1, f2, k == 0) : make_double2(0.0, 0.0);
-            row[g.nkxp + k] = (ok && k > 0) ? pack_hi(f1, f2) : make_double2(0.0, 0.0);
+            CT* row = dl + (size_t)p * 2 * g.nkxp;
+            row[k] = ok ? pack_lo(f1, f2, k == 0) : cmk<CT>(0.0, 0.0);
+            row[g.nkxp + k] = (ok && k > 0) ? pack_hi(f1, f2) : cmk<CT>(0.0, 0.0);
         }
         if (f + 1 < NF) __syncthreads();   // the next field's first pass reuses the slots
     }
@@ -222,13 +234,15 @@ __global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREAD
 // transforms, r2c of p = uq + i vq per row, whose last pass writes P[k] and P[nx-k] for the
 // kept kx straight to HBM.
 // ------------------------------------------------------------------------------------
-template <int NX, bool DRAG>
-__global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS, minb(XCfg<NX, DRAG>::THREADS))
-    k_xpass(Geom g, int layer0, const double2* __restrict__ pq, const double2* __restrict__ pv,
-            const double2* __restrict__ pu, double2* __restrict__ pp, double2* __restrict__ pd,
-            const double2* __restrict__ twx) {
-    using C = XCfg<NX, DRAG>;
-    extern __shared__ double2 sm[];
+template <int NX, bool DRAG, class CT>
+__global__ void __launch_bounds__(XCfg<NX, DRAG, CT>::THREADS, minb(XCfg<NX, DRAG, CT>::THREADS, regcap<CT>(128, 80)))
+    k_xpass(Geom g, int layer0, const CT* __restrict__ pq, const CT* __restrict__ pv,
+            const CT* __restrict__ pu, CT* __restrict__ pp, CT* __restrict__ pd,
+            const CT* __restrict__ twx) {
+    using C = XCfg<NX, DRAG, CT>;
+    using RT = typename CTraits<CT>::R;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    CT* sm = reinterpret_cast<CT*>(sm_raw);
     const int tid = threadIdx.x;
     const int l = layer0 + blockIdx.y;
     const int npairs = g.ny / 2;
@@ -237,35 +251,35 @@ __global__ void __launch_bounds__(XCfg<NX, DRAG>::THREADS, minb(XCfg<NX, DRAG>::
     const int r_of = slot / C::SP, s_of = slot % C::SP;
     const int rp = blockIdx.x * C::RP + r_of;
     const bool pair_ok = rp < npairs;
-    double2* base = sm + (r_of * C::SP) * C::TS;
-    double2* xs = sm + slot * C::TS;
+    CT* base = sm + (r_of * C::SP) * C::TS;
+    CT* xs = sm + slot * C::TS;
 
     // ---- inverse: slot 0 = q1+iq2, 1 = u1+iu2, 2 = v1+iv2
-    const double2* F = (s_of == 0 ? pq : (s_of == 1 ? pu : pv)) + ((size_t)l * npairs + rp) * 2 * g.nkxp;
-    auto ld_inv = [&](int k) -> double2 {
+    const CT* F = (s_of == 0 ? pq : (s_of == 1 ? pu : pv)) + ((size_t)l * npairs + rp) * 2 * g.nkxp;
+    auto ld_inv = [&](int k) -> CT {
         if (k < nkx) return F[k];
         if (k > NX - nkx) return F[g.nkxp + (NX - k)];
-        return make_double2(0.0, 0.0);
+        return cmk<CT>(0.0, 0.0);
     };
-    NoIO none;
+    NoIOT<CT> none;
     fft_fused<NX, +1, SRC_FN, DST_SMEM>(xs, lane, pair_ok && s_of < 3, twx, ld_inv, none);
 
     // ---- forward: slot 0 = u1 q1 + i v1 q1, 1 = u2 q2 + i v2 q2 (grid/(nx*ny) scaling as in
     //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
-    const double sc = g.inv_nxny;
-    auto ld_fwd = [&](int x) -> double2 {
-        const double2 a = base[fpad(x)], bu = base[C::TS + fpad(x)], cv = base[2 * C::TS + fpad(x)];
+    const RT sc = (RT)g.inv_nxny;
+    auto ld_fwd = [&](int x) -> CT {
+        const CT a = base[fpad(x)], bu = base[C::TS + fpad(x)], cv = base[2 * C::TS + fpad(x)];
         const bool second = (s_of & 1) != 0;
-        const double qv = (second ? a.y : a.x) * sc;
-        const double uv = (second ? bu.y : bu.x) * sc;
-        const double vv = (second ? cv.y : cv.x) * sc;
-        if (s_of < 2) return make_double2(uv * qv, vv * qv);
-        const double m = sqrt(uv * uv + vv * vv);   // URMS, QGN_Module.f90:285
-        return make_double2(m * uv, m * vv);
+        const RT qv = (second ? a.y : a.x) * sc;
+        const RT uv = (second ? bu.y : bu.x) * sc;
+        const RT vv = (second ? cv.y : cv.x) * sc;
+        if (s_of < 2) return cmk<CT>(uv * qv, vv * qv);
+        const RT m = sqrt(uv * uv + vv * vv);   // URMS, QGN_Module.f90:285
+        return cmk<CT>(m * uv, m * vv);
     };
     const int y = 2 * rp + (s_of & 1);
-    double2* out = (s_of < 2) ? pp + ((size_t)l * g.ny + y) * 2 * g.nkxp : pd + (size_t)y * 2 * g.nkxp;
-    auto st_fwd = [&](int k, double2 v) {
+    CT* out = (s_of < 2) ? pp + ((size_t)l * g.ny + y) * 2 * g.nkxp : pd + (size_t)y * 2 * g.nkxp;
+    auto st_fwd = [&](int k, CT v) {
         if (k < nkx) out[k] = v;
         else if (k > NX - nkx) out[g.nkxp + (NX - k)] = v;
     };
@@ -285,26 +299,28 @@ __device__ __forceinline__ double2 unpack_p(const double2* __restrict__ row, int
                     : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
 }
 
-__device__ __forceinline__ double2 unpack_pair(const double2* __restrict__ row, int nkxp, int kx, int fld, bool ok,
-                                               int partner) {
-    double2 mine = make_double2(0.0, 0.0);
+template <class CT>
+__device__ __forceinline__ CT unpack_pair(const CT* __restrict__ row, int nkxp, int kx, int fld, bool ok, int partner) {
+    CT mine = cmk<CT>(0.0, 0.0);
     if (ok && (fld == 0 || kx > 0)) mine = row[fld == 0 ? kx : nkxp + kx];
-    double2 other;
+    CT other;
     other.x = __shfl_xor_sync(0xffffffffu, mine.x, partner);
     other.y = __shfl_xor_sync(0xffffffffu, mine.y, partner);
-    const double2 X = fld == 0 ? mine : other;
-    const double2 Y = kx == 0 ? cconj(X) : cconj(fld == 0 ? other : mine);
-    return fld == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
-                    : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
+    const CT X = fld == 0 ? mine : other;
+    const CT Y = kx == 0 ? cconj(X) : cconj(fld == 0 ? other : mine);
+    return fld == 0 ? cmk<CT>((typename CTraits<CT>::R)0.5 * (X.x + Y.x), (typename CTraits<CT>::R)0.5 * (X.y + Y.y))
+                    : cmk<CT>((typename CTraits<CT>::R)0.5 * (X.y - Y.y), -(typename CTraits<CT>::R)0.5 * (X.x - Y.x));
 }
 
-template <int NY, bool DRAG>
-__global__ void __launch_bounds__(YFwdCfg<NY, DRAG>::THREADS, minb(YFwdCfg<NY, DRAG>::THREADS))
-    k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const double2* __restrict__ q,
-           const double2* __restrict__ psi, const double2* __restrict__ pp, const double2* __restrict__ pd,
-           double2* __restrict__ out, const double2* __restrict__ twy) {
-    using C = YFwdCfg<NY, DRAG>;
-    extern __shared__ double2 sm[];
+template <int NY, bool DRAG, class CT>
+__global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT>::THREADS, minb(YFwdCfg<NY, DRAG, CT>::THREADS, regcap<CT>()))
+    k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const CT* __restrict__ q,
+           const CT* __restrict__ psi, const CT* __restrict__ pp, const CT* __restrict__ pd,
+           CT* __restrict__ out, const CT* __restrict__ twy) {
+    using C = YFwdCfg<NY, DRAG, CT>;
+    using RT = typename CTraits<CT>::R;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    CT* sm = reinterpret_cast<CT*>(sm_raw);
     const int tid = threadIdx.x;
     const int l = layer0 + blockIdx.y;
     const int kx0 = blockIdx.x * C::TKX;
@@ -314,71 +330,71 @@ __global__ void __launch_bounds__(YFwdCfg<NY, DRAG>::THREADS, minb(YFwdCfg<NY, D
     const int nky = g.nky;
     const size_t colbase = (size_t)l * g.nkx;
     const bool bottom = (l == g.nz - 1);
-    double2* xs = sm + slot * C::TS;
-    NoIO none;
+    CT* xs = sm + slot * C::TS;
+    NoIOT<CT> none;
 
     if (DRAG) {
         // drag_hat = i ky (|u|u)^ - i kx (|u|v)^ on the bottom layer (QGN_Module.f90:284-292)
-        auto ldd = [&](int y) -> double2 {
+        auto ldd = [&](int y) -> CT {
             return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, colok, C::TKX);
         };
         fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ldd, none);
-        const double dc = lc->dragc;
+        const RT dc = (RT)lc->dragc;
         for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
             const int cc = e / nky, m = e % nky;
             const int kx = kx0 + cc;
             if (kx >= g.nkx) continue;
             const int j = g.jfull(m);
-            const double kxv = g.dkx * kx, kyv = g.kyval(j);
-            const double2 fu = sm[cc * C::TS + fpad(j)], fv = sm[(C::TKX + cc) * C::TS + fpad(j)];
-            double2 d = make_double2(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
-            d = make_double2(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
-            out[(colbase + kx) * nky + m] = make_double2(dc * d.x, dc * d.y);
+            const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
+            const CT fu = sm[cc * C::TS + fpad(j)], fv = sm[(C::TKX + cc) * C::TS + fpad(j)];
+            CT d = cmk<CT>(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
+            d = cmk<CT>(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
+            out[(colbase + kx) * nky + m] = cmk<CT>(dc * d.x, dc * d.y);
         }
         __syncthreads();
     }
 
     // the (uq)^ and (vq)^ slots of one column load P[k] and P[nx-k] respectively and swap
     // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
-    auto ld = [&](int y) -> double2 { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
+    auto ld = [&](int y) -> CT { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
                                                          fld, colok, C::TKX); };
     fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
 
-    const double ub = lc->uBar[l], bq = lc->betaq[l];
-    const double ek = lc->ekman;
+    const RT ub = (RT)lc->uBar[l], bq = (RT)lc->betaq[l];
+    const RT ek = (RT)lc->ekman;
     const bool expl = lc->explicit_diss != 0;
     for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
         const int cc = e / nky, m = e % nky;
         const int kx = kx0 + cc;
         if (kx >= g.nkx) continue;
         const int j = g.jfull(m);
-        const double kxv = g.dkx * kx, kyv = g.kyval(j);
+        const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
         const size_t idx = (colbase + kx) * nky + m;
-        const double2 fuq = sm[cc * C::TS + fpad(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad(j)];
-        const double2 qv = q[idx], pv = psi[idx];
+        const CT fuq = sm[cc * C::TS + fpad(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad(j)];
+        const CT qv = q[idx], pv = psi[idx];
         // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)
-        const double2 jac = make_double2(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);
-        double2 r = make_double2(-jac.x, -jac.y);
+        const CT jac = cmk<CT>(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);
+        CT r = cmk<CT>(-jac.x, -jac.y);
         // - uBar i kx q_hat - (beta+qyBar) v_hat   (QGN_Module.f90:270-273)
-        const double uk = ub * kxv;
-        const double2 vh = make_double2(-kxv * pv.y, kxv * pv.x);
-        r = make_double2(r.x + uk * qv.y, r.y - uk * qv.x);
-        r = make_double2(r.x - bq * vh.x, r.y - bq * vh.y);
-        const double k2 = kxv * kxv + kyv * kyv;
+        const RT uk = ub * kxv;
+        const CT vh = cmk<CT>(-kxv * pv.y, kxv * pv.x);
+        r = cmk<CT>(r.x + uk * qv.y, r.y - uk * qv.x);
+        r = cmk<CT>(r.x - bq * vh.x, r.y - bq * vh.y);
+        const RT k2 = kxv * kxv + kyv * kyv;
         if (expl) {   // QGN_Module.f90:275-280
-            const double k4 = k2 * k2, k8 = k4 * k4;
-            const double dcoef = lc->A2 * k2 + lc->A8 * k8;
-            r = make_double2(r.x - dcoef * qv.x, r.y - dcoef * qv.y);
+            const RT k4 = k2 * k2, k8 = k4 * k4;
+            const RT dcoef = (RT)lc->A2 * k2 + (RT)lc->A8 * k8;
+            r = cmk<CT>(r.x - dcoef * qv.x, r.y - dcoef * qv.y);
         }
         if (bottom) {   // Ekman, QGN_Module.f90:282
-            const double ekk = ek * k2;
-            r = make_double2(r.x + ekk * pv.x, r.y + ekk * pv.y);
+            const RT ekk = ek * k2;
+            r = cmk<CT>(r.x + ekk * pv.x, r.y + ekk * pv.y);
             if (DRAG) {
-                const double2 d = out[idx];
-                r = make_double2(r.x + d.x, r.y + d.y);
+                const CT d = out[idx];
+                r = cmk<CT>(r.x + d.x, r.y + d.y);
             }
         }
-        if (kx == 0 && m == 0) r = make_double2(0.0, 0.0);
+        if (kx == 0 && m == 0) r = cmk<CT>(0.0, 0.0);
         out[idx] = r;
     }
 }
@@ -402,7 +418,8 @@ __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
     k_xinv1(Geom g, const double2* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
             const double2* __restrict__ twx) {
     using C = X1Cfg<NX>;
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = reinterpret_cast<double2*>(sm_raw);
     __shared__ double smax[32];
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
@@ -463,7 +480,8 @@ template <int NX>
 __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
     k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx) {
     using C = X1Cfg<NX>;
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = reinterpret_cast<double2*>(sm_raw);
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
     const int npairs = g.ny / 2;
@@ -490,7 +508,8 @@ template <int NY>
 __global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREADS))
     k_yfwd1(Geom g, const double2* __restrict__ hq, double2* __restrict__ out, const double2* __restrict__ twy) {
     using C = YInvCfg<NY>;
-    extern __shared__ double2 sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* sm = reinterpret_cast<double2*>(sm_raw);
     const int tid = threadIdx.x;
     const int l = blockIdx.y;
     const int slot = tid % C::TKX, lane = tid / C::TKX;
@@ -558,78 +577,83 @@ cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, 
     return cudaGetLastError();
 }
 
-static cudaError_t launch_yinv(const Geom& g, int nf, const double2* q, const double2* psi, double2* hq,
-                               double2* hp, double2* hu, const double2* twy, cudaStream_t s) {
+template <class CT>
+static cudaError_t launch_yinv(const Geom& g, int nf, const CT* q, const CT* psi, CT* hq, CT* hp, CT* hu, const CT* twy,
+                               cudaStream_t s) {
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
-        using C = YInvCfg<NY>;
+        using C = YInvCfg<NY, CT>;
         dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
         cudaError_t e;
-        const double Cb = 16.0 * (double)g.csize(), Hb = 16.0 * (double)g.nz * NY * g.nkx;
+        const double es = (double)sizeof(CT);
+        const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
         if (nf == 3) {
-            if ((e = set_smem(k_yinv<NY, 3>, C::SMEM)) != cudaSuccess) return e;
+            if ((e = set_smem(k_yinv<NY, 3, CT>, C::SMEM)) != cudaSuccess) return e;
             QGN_LAUNCH(KID_YINV, 2.0 * Cb + 3.0 * Hb, s,
-                       k_yinv<NY, 3><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
+                       k_yinv<NY, 3, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
         } else {
-            if ((e = set_smem(k_yinv<NY, 1>, C::SMEM)) != cudaSuccess) return e;
+            if ((e = set_smem(k_yinv<NY, 1, CT>, C::SMEM)) != cudaSuccess) return e;
             QGN_LAUNCH(KID_YINV, Cb + Hb, s,
-                       k_yinv<NY, 1><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
+                       k_yinv<NY, 1, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
         }
         return cudaGetLastError();
     });
 }
 
-static cudaError_t launch_xpass(const Geom& g, const Buffers& b, bool drag, cudaStream_t s) {
+template <class CT>
+static cudaError_t launch_xpass(const Geom& g, const CT* hq, const CT* hp, const CT* hu, CT* hpp, CT* hpd, const CT* twx,
+                                bool drag, cudaStream_t s) {
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
         cudaError_t e;
+        const double es = (double)sizeof(CT);
         const int nplain = drag ? g.nz - 1 : g.nz;
         if (nplain > 0) {
-            using C = XCfg<NX, false>;
-            if ((e = set_smem(k_xpass<NX, false>, C::SMEM)) != cudaSuccess) return e;
+            using C = XCfg<NX, false, CT>;
+            if ((e = set_smem(k_xpass<NX, false, CT>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, nplain);
-            QGN_LAUNCH(KID_XPASS, 5.0 * 16.0 * (double)nplain * g.ny * g.nkx, s,
-                       k_xpass<NX, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.hq, b.hp, b.hu, b.hpp, b.hpd,
-                                                                             b.twx));
+            QGN_LAUNCH(KID_XPASS, 5.0 * es * (double)nplain * g.ny * g.nkx, s,
+                       k_xpass<NX, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, hq, hp, hu, hpp, hpd, twx));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (drag) {
-            using C = XCfg<NX, true>;
-            if ((e = set_smem(k_xpass<NX, true>, C::SMEM)) != cudaSuccess) return e;
+            using C = XCfg<NX, true, CT>;
+            if ((e = set_smem(k_xpass<NX, true, CT>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 1);
-            QGN_LAUNCH(KID_XPASS, 7.0 * 16.0 * (double)g.ny * g.nkx, s,
-                       k_xpass<NX, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.hq, b.hp, b.hu, b.hpp,
-                                                                            b.hpd, b.twx));
+            QGN_LAUNCH(KID_XPASS, 7.0 * es * (double)g.ny * g.nkx, s,
+                       k_xpass<NX, true, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, hq, hp, hu, hpp, hpd,
+                                                                                twx));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         return cudaSuccess;
     });
 }
 
-static cudaError_t launch_yfwd(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
-                               double2* out, bool drag, cudaStream_t s) {
+template <class CT>
+static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q, const CT* psi, const CT* hpp,
+                               const CT* hpd, CT* out, const CT* twy, bool drag, cudaStream_t s) {
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
         cudaError_t e;
+        const double es = (double)sizeof(CT);
         const int nplain = drag ? g.nz - 1 : g.nz;
         if (nplain > 0) {
-            using C = YFwdCfg<NY, false>;
-            if ((e = set_smem(k_yfwd<NY, false>, C::SMEM)) != cudaSuccess) return e;
+            using C = YFwdCfg<NY, false, CT>;
+            if ((e = set_smem(k_yfwd<NY, false, CT>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.nkx + C::TKX - 1) / C::TKX, nplain);
-            const double lb = 16.0 * (double)nplain * g.nkx;
+            const double lb = es * (double)nplain * g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (2.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, false><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, b.lc, q, psi, b.hpp, b.hpd, out,
-                                                                            b.twy));
+                       k_yfwd<NY, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, lc, q, psi, hpp, hpd, out, twy));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (drag) {
-            using C = YFwdCfg<NY, true>;
-            if ((e = set_smem(k_yfwd<NY, true>, C::SMEM)) != cudaSuccess) return e;
+            using C = YFwdCfg<NY, true, CT>;
+            if ((e = set_smem(k_yfwd<NY, true, CT>, C::SMEM)) != cudaSuccess) return e;
             dim3 grid((g.nkx + C::TKX - 1) / C::TKX, 1);
-            const double lb = 16.0 * (double)g.nkx;
+            const double lb = es * (double)g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (4.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, true><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, b.lc, q, psi, b.hpp,
-                                                                           b.hpd, out, b.twy));
+                       k_yfwd<NY, true, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, lc, q, psi, hpp, hpd, out,
+                                                                               twy));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -639,9 +663,24 @@ static cudaError_t launch_yfwd(const Geom& g, const Buffers& b, const double2* q
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
                        bool do_drag, cudaStream_t s) {
     cudaError_t e;
-    if ((e = launch_yinv(g, 3, q, psi, b.hq, b.hp, b.hu, b.twy, s)) != cudaSuccess) return e;
-    if ((e = launch_xpass(g, b, do_drag, s)) != cudaSuccess) return e;
-    return launch_yfwd(g, b, q, psi, out, do_drag, s);
+    if ((e = launch_yinv<double2>(g, 3, q, psi, b.hq, b.hp, b.hu, b.twy, s)) != cudaSuccess) return e;
+    if ((e = launch_xpass<double2>(g, b.hq, b.hp, b.hu, b.hpp, b.hpd, b.twx, do_drag, s)) != cudaSuccess) return e;
+    return launch_yfwd<double2>(g, b.lc, q, psi, b.hpp, b.hpd, out, b.twy, do_drag, s);
+}
+
+// FP32 right-hand side of the mixed mode: compact FP32 q, psi in, compact FP32 RHS out; the
+// half-transformed fields live in the (larger) FP64 buffers.
+cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const float2* psi, float2* out, bool do_drag,
+                         cudaStream_t s) {
+    float2* hq = reinterpret_cast<float2*>(b.hq);
+    float2* hp = reinterpret_cast<float2*>(b.hp);
+    float2* hu = reinterpret_cast<float2*>(b.hu);
+    float2* hpp = reinterpret_cast<float2*>(b.hpp);
+    float2* hpd = reinterpret_cast<float2*>(b.hpd);
+    cudaError_t e;
+    if ((e = launch_yinv<float2>(g, 3, q, psi, hq, hp, hu, b.twy32, s)) != cudaSuccess) return e;
+    if ((e = launch_xpass<float2>(g, hq, hp, hu, hpp, hpd, b.twx32, do_drag, s)) != cudaSuccess) return e;
+    return launch_yfwd<float2>(g, b.lc, q, psi, hpp, hpd, out, b.twy32, do_drag, s);
 }
 
 template <int EPI>
@@ -661,7 +700,7 @@ static cudaError_t launch_xinv1(const Geom& g, const Buffers& b, DevScalars* sc,
 
 cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s) {
     cudaError_t e;
-    if ((e = launch_yinv(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
+    if ((e = launch_yinv<double2>(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
     return launch_xinv1<0>(g, b, sc, nullptr, s);
 }
 
@@ -691,7 +730,7 @@ cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys
 
 cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, double* out, cudaStream_t s) {
     cudaError_t e;
-    if ((e = launch_yinv(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
+    if ((e = launch_yinv<double2>(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
     return launch_xinv1<1>(g, b, nullptr, out, s);
 }
 

@@ -85,7 +85,7 @@ __device__ __forceinline__ void point_k(const Geom& g, size_t p, int& kx, int& m
 // ---- ARK stage s (1..5): q_s and psi_s -----------------------------------------------------
 // S and NZ are template parameters so that every load of the stage is unrolled and in flight.
 template <int S, int NZ>
-__global__ void __launch_bounds__(256) k_ark_stage(Geom g, StagePtrs sp, const double2* __restrict__ q,
+__global__ void __launch_bounds__(256, 2) k_ark_stage(Geom g, StagePtrs sp, const double2* __restrict__ q,
                                                    double2* __restrict__ qout, double2* __restrict__ psi,
                                                    const ModalConst* __restrict__ mc,
                                                    const LayerConst* __restrict__ lc,
@@ -178,9 +178,172 @@ __global__ void __launch_bounds__(256) k_ark_update(Geom g, StagePtrs sp, const 
     qnew[e] = (p == 0) ? make_double2(0.0, 0.0) : make_double2(q0.x + dt * uc.x, q0.y + dt * uc.y);
 }
 
+// ---- mixed precision (QGN_PREC_MIXED) ----------------------------------------------------------
+// Stage values N_j and q_j are stored in FP32.  The stage sums
+//   sum_j ae_sj N_j + sum_j ai_sj L_j
+// are formed in FP32 with Kahan-compensated summation (tableau coefficients rounded to FP32);
+// the FP64 term L_1 = -D q_hat enters as its FP32 head plus its FP32 remainder.
+// q_s = Mq (q_hat + dt * sum) is formed in FP64 from the compensated sum, GetPsi runs in FP64,
+// and q_s, psi_s are stored in FP32.
+struct Comp32 {
+    float s = 0.f, c = 0.f;     // running sum and the negated lost low part
+    __device__ __forceinline__ void add(float x) {
+        const float y = __fsub_rn(x, c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+__device__ __forceinline__ void comp_add_prod(Comp32& acc, double a, float v) { acc.add(__fmul_rn((float)a, v)); }
+__device__ __forceinline__ void comp_add_double(Comp32& acc, double x) {
+    const float hi = (float)x;
+    acc.add(hi);
+    acc.add((float)(x - (double)hi));
+}
+
+struct StagePtrs32 {
+    const float2* N[6];
+    const float2* Qs[6];
+};
+
+template <int S, int NZ>
+__global__ void __launch_bounds__(256, 2) k_ark_stage_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
+                                                         float2* __restrict__ qout, float2* __restrict__ psi,
+                                                         const ModalConst* __restrict__ mc,
+                                                         const LayerConst* __restrict__ lc,
+                                                         const DevScalars* __restrict__ sc) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ], s_a8[kMaxNZ];
+    const int nz = g.nz;
+    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) { s_ev[i] = mc->evals[i]; s_a8[i] = sc->A8L[i]; }
+    __syncthreads();
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double dt = sc->dt;
+    const double A2 = lc->A2;
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    double2 qv[NZC], pv[NZC];
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            const size_t idx = (size_t)l * P + p;
+            float2 nn[S], qq[S];
+#pragma unroll
+            for (int j = 0; j < S; ++j) nn[j] = sp.N[j][idx];
+#pragma unroll
+            for (int j = 1; j < S; ++j) qq[j] = sp.Qs[j][idx];
+            const double2 q0 = q[idx];
+            const double D = A2 * k2 + s_a8[l] * k8;
+            const float Df = (float)D;
+            Comp32 ax, ay;
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                comp_add_prod(ax, c_ae[S * 6 + j], nn[j].x);
+                comp_add_prod(ay, c_ae[S * 6 + j], nn[j].y);
+            }
+            comp_add_double(ax, c_ai[S * 6] * (-D * q0.x));      // L_1 from the FP64 state
+            comp_add_double(ay, c_ai[S * 6] * (-D * q0.y));
+#pragma unroll
+            for (int j = 1; j < S; ++j) {
+                comp_add_prod(ax, c_ai[S * 6 + j], -Df * qq[j].x);
+                comp_add_prod(ay, c_ai[S * 6 + j], -Df * qq[j].y);
+            }
+            const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
+            qv[l] = make_double2(Mq * (q0.x + dt * ax.value()), Mq * (q0.y + dt * ay.value()));
+        }
+    }
+    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            qout[(size_t)l * P + p] = make_float2((float)qv[l].x, (float)qv[l].y);
+            psi[(size_t)l * P + p] = make_float2((float)pv[l].x, (float)pv[l].y);
+        }
+    }
+}
+
+// update + embedded error in FP64 from FP32 stage values (ARK43_QGLeith.f90:120-134)
+__global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
+                                                          double2* __restrict__ qnew, double2* __restrict__ err,
+                                                          const LayerConst* __restrict__ lc,
+                                                          const DevScalars* __restrict__ sc) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t total = P * g.nz;
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int l = (int)(e / P);
+    const size_t p = e % P;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double D = lc->A2 * k2 + sc->A8L[l] * k8;
+    const double dt = sc->dt;
+    const double2 q0 = q[e];
+    double2 ec = make_double2(0.0, 0.0), uc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        if (i == 1) continue;   // b(2) = be(2) = 0
+        const float2 n = sp.N[i][e];
+        double qx, qy;
+        if (i == 0) { qx = q0.x; qy = q0.y; }
+        else { const float2 qi = sp.Qs[i][e]; qx = qi.x; qy = qi.y; }
+        const double nlx = (double)n.x + (-D * qx), nly = (double)n.y + (-D * qy);
+        ec.x += c_be[i] * nlx;
+        ec.y += c_be[i] * nly;
+        uc.x += c_b[i] * nlx;
+        uc.y += c_b[i] * nly;
+    }
+    err[e] = ec;
+    qnew[e] = (p == 0) ? make_double2(0.0, 0.0) : make_double2(q0.x + dt * uc.x, q0.y + dt * uc.y);
+}
+
+// FP32 copy of the FP64 state and its GetPsi (FP64 arithmetic, FP32 result)
+template <int NZ>
+__global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const ModalConst* __restrict__ mc,
+                                                     const double2* __restrict__ q, float2* __restrict__ q32,
+                                                     float2* __restrict__ psi32) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    const int nz = g.nz;
+    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
+    __syncthreads();
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    double2 qv[NZC], pv[NZC];
+#pragma unroll
+    for (int l = 0; l < NZC; ++l)
+        if (l < nz) qv[l] = q[(size_t)l * P + p];
+    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            q32[(size_t)l * P + p] = make_float2((float)qv[l].x, (float)qv[l].y);
+            psi32[(size_t)l * P + p] = make_float2((float)pv[l].x, (float)pv[l].y);
+        }
+    }
+}
+
+__global__ void k_f2d(size_t n, const float2* __restrict__ a, double2* __restrict__ b) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) b[e] = make_double2(a[e].x, a[e].y);
+}
+
 // ---- explicit combinations: out = q + sum_j (a_j dt) R_j, then optionally psi = GetPsi(out) ---
 template <int NZ>
-__global__ void __launch_bounds__(256) k_combo(Geom g, Combo cb, const double2* __restrict__ q,
+__global__ void __launch_bounds__(256, 2) k_combo(Geom g, Combo cb, const double2* __restrict__ q,
                                                double2* __restrict__ out, double2* __restrict__ psi,
                                                const ModalConst* __restrict__ mc,
                                                const DevScalars* __restrict__ sc, int want_psi) {
@@ -434,6 +597,74 @@ cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_
         case 5: launch_stage_s<5>(g, b, sp, grid, nb, st); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+static StagePtrs32 stage_ptrs32(const Buffers& b) {
+    StagePtrs32 sp{};
+    for (int j = 0; j < 6; ++j) {
+        sp.N[j] = reinterpret_cast<const float2*>(b.N[j]);
+        sp.Qs[j] = reinterpret_cast<const float2*>(b.Qs[j]);
+    }
+    return sp;
+}
+
+template <int S>
+static void launch_stage_mixed_s(const Geom& g, const Buffers& b, const StagePtrs32& sp, dim3 grid, double nb,
+                                 cudaStream_t st) {
+    float2* qo = reinterpret_cast<float2*>(b.Qs[S]);
+    float2* ps = reinterpret_cast<float2*>(b.psi);
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 2><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 4><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
+        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 8><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
+        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 16><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
+        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 0><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
+    }
+}
+
+cudaError_t launch_ark_stage_mixed(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    const StagePtrs32 sp = stage_ptrs32(b);
+    const size_t P = (size_t)g.nkx * g.nky;
+    dim3 grid(blocks_for(P, 256));
+    const double c32 = 8.0 * (double)g.csize();
+    const double nb = 16.0 * (double)g.csize() + c32 * (2.0 * s - 1.0 + 2.0);
+    switch (s) {
+        case 1: launch_stage_mixed_s<1>(g, b, sp, grid, nb, st); break;
+        case 2: launch_stage_mixed_s<2>(g, b, sp, grid, nb, st); break;
+        case 3: launch_stage_mixed_s<3>(g, b, sp, grid, nb, st); break;
+        case 4: launch_stage_mixed_s<4>(g, b, sp, grid, nb, st); break;
+        case 5: launch_stage_mixed_s<5>(g, b, sp, grid, nb, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_t st) {
+    const StagePtrs32 sp = stage_ptrs32(b);
+    const double C = (double)g.csize();
+    QGN_LAUNCH(KID_UPDATE, 16.0 * C * 3.0 + 8.0 * C * 9.0, st,
+               k_ark_update_mixed<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_modal_mixed(const Geom& g, const Buffers& b, const double2* q, float2* q32, float2* psi32,
+                               cudaStream_t st) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    dim3 grid(blocks_for(P, 256));
+    const double nb = 32.0 * (double)g.csize();
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<2><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<4><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<8><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<16><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<0><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_f2d(size_t n, const float2* a, double2* b, cudaStream_t st) {
+    QGN_LAUNCH(KID_LAYOUT, 24.0 * (double)n, st, k_f2d<<<blocks_for(n, 256), 256, 0, st>>>(n, a, b));
     return cudaGetLastError();
 }
 
