@@ -79,10 +79,11 @@ int qgn_create(const qgn_params* p, const double* H, const double* S,
 /*
  * One call of TimeStep(q_hat,t,dt) (QGN_Module.f90:302-309) with the scheme chosen
  * at qgn_create.  q_hat is the host spectral array (interleaved complex, Fortran
- * order).  Only the modes that DeAlias keeps are read and written: the entries
- * DeAlias zeroes (QGN_Module.f90:194-204) are treated as zero on input and left
- * untouched on output (the reference's TimeStep zeroes them with its trailing
- * DeAlias call).  t and dt are updated exactly as by the reference scheme.
+ * order).  Only the modes that DeAlias keeps are read: the entries DeAlias zeroes
+ * (QGN_Module.f90:194-204) are treated as zero on input.  On output the whole array is
+ * written, with zeros where DeAlias zeroes (as after the reference's TimeStep, whose
+ * trailing DeAlias call zeroes them).  t and dt are updated exactly as by the reference
+ * scheme.
  * Stepper memory (FSAL stage, AB history, err0) persists in the context like the
  * reference's `save` variables.
  */

@@ -110,15 +110,21 @@ int upload_kept(qgn_ctx* ctx, const double* host, double2* dst) {
     return QGN_OK;
 }
 
-// compact device field -> host q_hat (kept modes only)
-int download_kept(qgn_ctx* ctx, const double2* src, double* host) {
-    CK(launch_compact_to_xfer(ctx->g, src, ctx->b.xfer, ctx->stream));
-    RET(copy_kept(ctx, host, false));
+int ensure_full(qgn_ctx* ctx) {
+    if (!ctx->b.full) CK(dalloc(&ctx->b.full, (size_t)ctx->g.nz * ctx->g.ny * ctx->g.nxh));
     return QGN_OK;
 }
 
-int ensure_full(qgn_ctx* ctx) {
-    if (!ctx->b.full) CK(dalloc(&ctx->b.full, (size_t)ctx->g.nz * ctx->g.ny * ctx->g.nxh));
+// compact device field -> host q_hat: the whole array in one contiguous copy, with zeros
+// where DeAlias zeroes (QGN_Module.f90:194-204) -- the values the reference's trailing
+// DeAlias in TimeStep leaves there
+int download_kept(qgn_ctx* ctx, const double2* src, double* host) {
+    RET(ensure_full(ctx));
+    const Geom& g = ctx->g;
+    CK(launch_compact_to_xfer(g, src, ctx->b.xfer, ctx->stream));
+    CK(launch_xfer_to_full(g, ctx->b.xfer, ctx->b.full, ctx->stream));
+    CK(cudaMemcpyAsync(host, ctx->b.full, sizeof(double2) * (size_t)g.nz * g.ny * g.nxh, cudaMemcpyDeviceToHost,
+                       ctx->stream));
     return QGN_OK;
 }
 
@@ -141,19 +147,9 @@ int read_scalars(qgn_ctx* ctx, DevScalars* out) {
     return QGN_OK;
 }
 
-// new state from the host: set t, dt and clear a previous failure (halt, status)
+// new state from the host: set t, dt and clear a previous failure (halt, status); stream-ordered
 int write_time(qgn_ctx* ctx, double t, double dt) {
-    DevScalars s;
-    RET(read_scalars(ctx, &s));
-    s.t = t;
-    s.dt = dt;
-    s.nonfinite = 0;
-    s.halt = 0;
-    s.status = 0;
-    s.rejects_step = 0;
-    std::memcpy(ctx->host_pin, &s, sizeof(s));
-    CK(cudaMemcpyAsync(ctx->b.sc, ctx->host_pin, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(launch_set_time(ctx->b.sc, t, dt, ctx->stream));
     return QGN_OK;
 }
 
@@ -761,7 +757,10 @@ int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps) 
     if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
     RET(qgn_set_state(ctx, q_hat, *t, *dt));
     RET(advance_n(ctx, nsteps));
-    RET(check_state(ctx));
+    // the adaptive schemes' controller already halts on a non-finite error estimate
+    const bool adaptive = ctx->scheme == QGN_SCHEME_ARK43_QGLEITH || ctx->scheme == QGN_SCHEME_ARK43 ||
+                          ctx->scheme == QGN_SCHEME_BSRK3;
+    if (!adaptive) RET(check_state(ctx));
     RET(download_kept(ctx, ctx->b.q, q_hat));
     DevScalars s;
     RET(read_scalars(ctx, &s));

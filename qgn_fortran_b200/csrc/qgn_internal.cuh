@@ -167,6 +167,7 @@ cudaError_t launch_step_gate(DevScalars* sc, const cudaGraphConditionalHandle* g
 cudaError_t launch_set_cond(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t s);
 cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t s);
 cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t s);
+cudaError_t launch_set_time(DevScalars* sc, double t, double dt, cudaStream_t s);
 cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t s);
 cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* Hw, int nbins, double* spec,
                                cudaStream_t s);

@@ -82,68 +82,6 @@ __device__ __forceinline__ void point_k(const Geom& g, size_t p, int& kx, int& m
     k2 = kxv * kxv + kyv * kyv;
 }
 
-// ---- ARK stage s (1..5): q_s and psi_s -----------------------------------------------------
-// S and NZ are template parameters so that every load of the stage is unrolled and in flight.
-template <int S, int NZ>
-__global__ void __launch_bounds__(256, 2) k_ark_stage(Geom g, StagePtrs sp, const double2* __restrict__ q,
-                                                   double2* __restrict__ qout, double2* __restrict__ psi,
-                                                   const ModalConst* __restrict__ mc,
-                                                   const LayerConst* __restrict__ lc,
-                                                   const DevScalars* __restrict__ sc) {
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ], s_a8[kMaxNZ];
-    const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) { s_ev[i] = mc->evals[i]; s_a8[i] = sc->A8L[i]; }
-    __syncthreads();
-    const size_t P = (size_t)g.nkx * g.nky;
-    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P) return;
-    int kx, m;
-    double k2;
-    point_k(g, p, kx, m, k2);
-    const double k8 = (k2 * k2) * (k2 * k2);
-    const double dt = sc->dt;
-    const double A2 = lc->A2;
-    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
-    double2 qv[NZC], pv[NZC];
-#pragma unroll
-    for (int l = 0; l < NZC; ++l) {
-        if (l < nz) {
-            const size_t idx = (size_t)l * P + p;
-            double2 nn[S], qq[S];
-#pragma unroll
-            for (int j = 0; j < S; ++j) nn[j] = sp.N[j][idx];
-            qq[0] = q[idx];
-#pragma unroll
-            for (int j = 1; j < S; ++j) qq[j] = sp.Qs[j][idx];
-            const double D = A2 * k2 + s_a8[l] * k8;
-            double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-            for (int j = 0; j < S; ++j) {
-                const double a = c_ae[S * 6 + j];
-                acc.x += a * nn[j].x;
-                acc.y += a * nn[j].y;
-            }
-#pragma unroll
-            for (int j = 0; j < S; ++j) {
-                const double a = c_ai[S * 6 + j];
-                acc.x += a * (-D * qq[j].x);
-                acc.y += a * (-D * qq[j].y);
-            }
-            const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
-            qv[l] = make_double2(Mq * (qq[0].x + dt * acc.x), Mq * (qq[0].y + dt * acc.y));
-        }
-    }
-    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
-#pragma unroll
-    for (int l = 0; l < NZC; ++l) {
-        if (l < nz) {
-            qout[(size_t)l * P + p] = qv[l];
-            psi[(size_t)l * P + p] = pv[l];
-        }
-    }
-}
-
 // ---- ARK update + embedded error combination (ARK43_QGLeith.f90:120-134) ---------------------
 __global__ void __launch_bounds__(256) k_ark_update(Geom g, StagePtrs sp, const double2* __restrict__ q,
                                                     double2* __restrict__ qnew, double2* __restrict__ err,
@@ -203,21 +141,92 @@ __device__ __forceinline__ void comp_add_double(Comp32& acc, double x) {
     acc.add((float)(x - (double)hi));
 }
 
-struct StagePtrs32 {
-    const float2* N[6];
-    const float2* Qs[6];
+// ---- ARK stage s as two streaming kernels ------------------------------------------------------
+// k_ark_comb: one thread per (layer, mode): q_s = Mq (q + dt (sum ae N_j + sum ai L_j)), the
+// sums in FP64 (FP64 storage) or Kahan-compensated FP32 (FP32 storage, mixed mode), q in FP64.
+// GetPsi of q_s follows as a separate all-layers kernel (k_modal / k_modal_f32).
+template <class T> struct StoreT;
+template <> struct StoreT<double2> {
+    __device__ static double2 put(double x, double y) { return make_double2(x, y); }
+};
+template <> struct StoreT<float2> {
+    __device__ static float2 put(double x, double y) { return make_float2((float)x, (float)y); }
 };
 
-template <int S, int NZ>
-__global__ void __launch_bounds__(256, 2) k_ark_stage_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
-                                                         float2* __restrict__ qout, float2* __restrict__ psi,
-                                                         const ModalConst* __restrict__ mc,
-                                                         const LayerConst* __restrict__ lc,
-                                                         const DevScalars* __restrict__ sc) {
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ], s_a8[kMaxNZ];
+template <class T>
+struct CombPtrs {
+    const T* N[6];
+    const T* Q[6];
+};
+
+template <int S, class T>
+__global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const double2* __restrict__ q,
+                                                  T* __restrict__ qout, const LayerConst* __restrict__ lc,
+                                                  const DevScalars* __restrict__ sc) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t total = P * g.nz;
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int l = (int)(e / P);
+    const size_t p = e % P;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double D = lc->A2 * k2 + sc->A8L[l] * k8;
+    const double dt = sc->dt;
+    T nn[S], qq[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) nn[j] = cp.N[j][e];
+#pragma unroll
+    for (int j = 1; j < S; ++j) qq[j] = cp.Q[j][e];
+    const double2 q0 = q[e];
+    double ax, ay;
+    if constexpr (sizeof(T) == 16) {
+        ax = 0.0;
+        ay = 0.0;
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            ax += c_ae[S * 6 + j] * nn[j].x;
+            ay += c_ae[S * 6 + j] * nn[j].y;
+        }
+        ax += c_ai[S * 6] * (-D * q0.x);
+        ay += c_ai[S * 6] * (-D * q0.y);
+#pragma unroll
+        for (int j = 1; j < S; ++j) {
+            ax += c_ai[S * 6 + j] * (-D * qq[j].x);
+            ay += c_ai[S * 6 + j] * (-D * qq[j].y);
+        }
+    } else {
+        Comp32 cx, cy;
+        const float Df = (float)D;
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            comp_add_prod(cx, c_ae[S * 6 + j], nn[j].x);
+            comp_add_prod(cy, c_ae[S * 6 + j], nn[j].y);
+        }
+        comp_add_double(cx, c_ai[S * 6] * (-D * q0.x));   // L_1 from the FP64 state
+        comp_add_double(cy, c_ai[S * 6] * (-D * q0.y));
+#pragma unroll
+        for (int j = 1; j < S; ++j) {
+            comp_add_prod(cx, c_ai[S * 6 + j], -Df * qq[j].x);
+            comp_add_prod(cy, c_ai[S * 6 + j], -Df * qq[j].y);
+        }
+        ax = cx.value();
+        ay = cy.value();
+    }
+    const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
+    qout[e] = StoreT<T>::put(Mq * (q0.x + dt * ax), Mq * (q0.y + dt * ay));
+}
+
+// GetPsi of an FP32 field with FP64 arithmetic (mixed mode)
+template <int NZ>
+__global__ void __launch_bounds__(256, 2) k_modal_f32(Geom g, const ModalConst* __restrict__ mc,
+                                                      const float2* __restrict__ q, float2* __restrict__ psi) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) { s_ev[i] = mc->evals[i]; s_a8[i] = sc->A8L[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
     __syncthreads();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,49 +234,25 @@ __global__ void __launch_bounds__(256, 2) k_ark_stage_mixed(Geom g, StagePtrs32 
     int kx, m;
     double k2;
     point_k(g, p, kx, m, k2);
-    const double k8 = (k2 * k2) * (k2 * k2);
-    const double dt = sc->dt;
-    const double A2 = lc->A2;
     constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
     double2 qv[NZC], pv[NZC];
 #pragma unroll
-    for (int l = 0; l < NZC; ++l) {
+    for (int l = 0; l < NZC; ++l)
         if (l < nz) {
-            const size_t idx = (size_t)l * P + p;
-            float2 nn[S], qq[S];
-#pragma unroll
-            for (int j = 0; j < S; ++j) nn[j] = sp.N[j][idx];
-#pragma unroll
-            for (int j = 1; j < S; ++j) qq[j] = sp.Qs[j][idx];
-            const double2 q0 = q[idx];
-            const double D = A2 * k2 + s_a8[l] * k8;
-            const float Df = (float)D;
-            Comp32 ax, ay;
-#pragma unroll
-            for (int j = 0; j < S; ++j) {
-                comp_add_prod(ax, c_ae[S * 6 + j], nn[j].x);
-                comp_add_prod(ay, c_ae[S * 6 + j], nn[j].y);
-            }
-            comp_add_double(ax, c_ai[S * 6] * (-D * q0.x));      // L_1 from the FP64 state
-            comp_add_double(ay, c_ai[S * 6] * (-D * q0.y));
-#pragma unroll
-            for (int j = 1; j < S; ++j) {
-                comp_add_prod(ax, c_ai[S * 6 + j], -Df * qq[j].x);
-                comp_add_prod(ay, c_ai[S * 6 + j], -Df * qq[j].y);
-            }
-            const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
-            qv[l] = make_double2(Mq * (q0.x + dt * ax.value()), Mq * (q0.y + dt * ay.value()));
+            const float2 v = q[(size_t)l * P + p];
+            qv[l] = make_double2(v.x, v.y);
         }
-    }
     modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
-    for (int l = 0; l < NZC; ++l) {
-        if (l < nz) {
-            qout[(size_t)l * P + p] = make_float2((float)qv[l].x, (float)qv[l].y);
-            psi[(size_t)l * P + p] = make_float2((float)pv[l].x, (float)pv[l].y);
-        }
-    }
+    for (int l = 0; l < NZC; ++l)
+        if (l < nz) psi[(size_t)l * P + p] = make_float2((float)pv[l].x, (float)pv[l].y);
 }
+
+
+struct StagePtrs32 {
+    const float2* N[6];
+    const float2* Qs[6];
+};
 
 // update + embedded error in FP64 from FP32 stage values (ARK43_QGLeith.f90:120-134)
 __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
@@ -566,38 +551,68 @@ __global__ void k_zero_max(DevScalars* sc) {
 
 __global__ void k_advance_time(DevScalars* sc) { sc->t = sc->t + sc->dt; }
 
+// a new state from the host: set t and dt and clear a previous failure
+__global__ void k_set_time(DevScalars* sc, double t, double dt) {
+    sc->t = t;
+    sc->dt = dt;
+    sc->nonfinite = 0;
+    sc->halt = 0;
+    sc->status = 0;
+    sc->rejects_step = 0;
+}
+
 // ------------------------------------------------------------------------------------------
 // launch wrappers
 // ------------------------------------------------------------------------------------------
 static inline unsigned blocks_for(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-template <int S>
-static void launch_stage_s(const Geom& g, const Buffers& b, const StagePtrs& sp, dim3 grid, double nb,
-                           cudaStream_t st) {
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 2><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 4><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
-        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 8><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
-        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 16><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
-        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage<S, 0><<<grid, 256, 0, st>>>(g, sp, b.q, b.Qs[S], b.psi, b.mc, b.lc, b.sc)); break;
+template <class T>
+static CombPtrs<T> comb_ptrs(const Buffers& b) {
+    CombPtrs<T> cp{};
+    for (int j = 0; j < 6; ++j) {
+        cp.N[j] = reinterpret_cast<const T*>(b.N[j]);
+        cp.Q[j] = reinterpret_cast<const T*>(b.Qs[j]);
     }
+    return cp;
 }
 
-cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
-    StagePtrs sp{};
-    for (int j = 0; j < 6; ++j) { sp.N[j] = b.N[j]; sp.Qs[j] = b.Qs[j]; }
-    const size_t P = (size_t)g.nkx * g.nky;
-    dim3 grid(blocks_for(P, 256));
-    const double nb = 16.0 * (double)g.csize() * (2.0 * s + 2.0);
+template <class T>
+static cudaError_t launch_comb(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    const CombPtrs<T> cp = comb_ptrs<T>(b);
+    T* qout = reinterpret_cast<T*>(b.Qs[s]);
+    const double es = (double)sizeof(T), C = (double)g.csize();
+    const double nb = 16.0 * C + es * C * (2.0 * s - 1.0 + 1.0);
+    const unsigned nbk = blocks_for(g.csize(), 256);
     switch (s) {
-        case 1: launch_stage_s<1>(g, b, sp, grid, nb, st); break;
-        case 2: launch_stage_s<2>(g, b, sp, grid, nb, st); break;
-        case 3: launch_stage_s<3>(g, b, sp, grid, nb, st); break;
-        case 4: launch_stage_s<4>(g, b, sp, grid, nb, st); break;
-        case 5: launch_stage_s<5>(g, b, sp, grid, nb, st); break;
+        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<1, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<2, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<3, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<4, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<5, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, float2* psi, cudaStream_t st) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    dim3 grid(blocks_for(P, 256));
+    const double nb = 16.0 * (double)g.csize();
+    switch (g.nz) {
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<2><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<4><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<8><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<16><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<0><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+    }
+    return cudaGetLastError();
+}
+
+// stage s of ARK4(3)6L[2]SA: q_s (streaming combination), then psi_s = GetPsi(q_s)
+cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    cudaError_t e = launch_comb<double2>(g, b, s, st);
+    if (e != cudaSuccess) return e;
+    return launch_modal(g, b.mc, b.Qs[s], b.psi, st);
 }
 
 static StagePtrs32 stage_ptrs32(const Buffers& b) {
@@ -609,35 +624,10 @@ static StagePtrs32 stage_ptrs32(const Buffers& b) {
     return sp;
 }
 
-template <int S>
-static void launch_stage_mixed_s(const Geom& g, const Buffers& b, const StagePtrs32& sp, dim3 grid, double nb,
-                                 cudaStream_t st) {
-    float2* qo = reinterpret_cast<float2*>(b.Qs[S]);
-    float2* ps = reinterpret_cast<float2*>(b.psi);
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 2><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 4><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
-        case 8: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 8><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
-        case 16: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 16><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
-        default: QGN_LAUNCH(KID_STAGE, nb, st, k_ark_stage_mixed<S, 0><<<grid, 256, 0, st>>>(g, sp, b.q, qo, ps, b.mc, b.lc, b.sc)); break;
-    }
-}
-
 cudaError_t launch_ark_stage_mixed(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
-    const StagePtrs32 sp = stage_ptrs32(b);
-    const size_t P = (size_t)g.nkx * g.nky;
-    dim3 grid(blocks_for(P, 256));
-    const double c32 = 8.0 * (double)g.csize();
-    const double nb = 16.0 * (double)g.csize() + c32 * (2.0 * s - 1.0 + 2.0);
-    switch (s) {
-        case 1: launch_stage_mixed_s<1>(g, b, sp, grid, nb, st); break;
-        case 2: launch_stage_mixed_s<2>(g, b, sp, grid, nb, st); break;
-        case 3: launch_stage_mixed_s<3>(g, b, sp, grid, nb, st); break;
-        case 4: launch_stage_mixed_s<4>(g, b, sp, grid, nb, st); break;
-        case 5: launch_stage_mixed_s<5>(g, b, sp, grid, nb, st); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+    cudaError_t e = launch_comb<float2>(g, b, s, st);
+    if (e != cudaSuccess) return e;
+    return launch_modal_f32(g, b, reinterpret_cast<const float2*>(b.Qs[s]), reinterpret_cast<float2*>(b.psi), st);
 }
 
 cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_t st) {
@@ -753,6 +743,11 @@ cudaError_t launch_set_cond(cudaGraphConditionalHandle h, unsigned int v, cudaSt
 
 cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t st) {
     QGN_LAUNCH(KID_SCALAR, 0.0, st, k_zero_max<<<1, 1, 0, st>>>(sc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_time(DevScalars* sc, double t, double dt, cudaStream_t st) {
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_set_time<<<1, 1, 0, st>>>(sc, t, dt));
     return cudaGetLastError();
 }
 

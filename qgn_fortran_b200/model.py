@@ -146,8 +146,9 @@ class QGNModule:
         """TimeStep(q_hat, t, dt): advances q_hat in place; returns the new (t, dt)."""
         q_hat = self._spec(q_hat, writable=True)
         tt, dd = C.c_double(t), C.c_double(dt)
+        # qgn_step writes the whole array with zeros where TimeStep's trailing DeAlias
+        # (QGN_Module.f90:307) zeroes, so no host-side DeAlias pass is needed
         self._check(self.lib.qgn_step(self.ctx, dptr(q_hat), C.byref(tt), C.byref(dd)), "qgn_step")
-        self._dealias_host(q_hat)      # TimeStep's trailing DeAlias (QGN_Module.f90:307)
         self.t, self.dt = tt.value, dd.value
         return tt.value, dd.value
 
@@ -156,15 +157,8 @@ class QGNModule:
         tt, dd = C.c_double(t), C.c_double(dt)
         self._check(self.lib.qgn_advance(self.ctx, dptr(q_hat), C.byref(tt), C.byref(dd), int(nsteps)),
                     "qgn_advance")
-        self._dealias_host(q_hat)
         self.t, self.dt = tt.value, dd.value
         return tt.value, dd.value
-
-    def _dealias_host(self, q_hat):
-        nx, ny = self.nx, self.ny
-        q_hat[:, :, nx // 3: nx // 2 + 1] = 0.0
-        q_hat[:, ny // 3: 2 * (ny // 3) + 1, :] = 0.0
-        q_hat[:, 0, 0] = 0.0
 
     def write_qp(self, q_hat, rec_no: int, nt: int, directory: str = "."):
         """WriteQP: q.%09d.dat and p.%09d.dat raw float64 physical fields (QGN_Module.f90:348-377)."""
