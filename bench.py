@@ -7,10 +7,12 @@ peak wavenumber 16, rms 1e-6 s^-1).  A step is one accepted TimeStep (6 RHS eval
 plus any rejected attempts).  Data are synthetic; the spin-up of the named configuration
 (10 model years) is not run -- timing starts from the seeded state after the warm-up steps.
 
-``value``: device-resident stepping (qgn_advance_resident), CUDA events on the library's
-stream.  ``e2e``: the drop-in path qgn_step (TimeStep) with the host q_hat in pinned memory,
-i.e. every step copies the kept modes host->device and back.  ``--impl reference`` times the
-CPU restatement of the reference (the oracle) on the host cores.
+``value``: device-resident stepping (qgn_advance_resident, graph-launched steps), CUDA
+events on the library's stream.  ``e2e``: the drop-in path TimeStep (QGNModule.time_step ->
+qgn_step) with the host q_hat in pinned memory: every step copies the kept modes host->device
+and the whole array back.  ``mixed``: the same workload in the mixed-precision mode.
+``cpu_baseline`` and ``--impl reference`` time the FP64 C/OpenMP restatement of the reference
+(oracle/qgn_ref.c) on all host threads.
 
 Multi-GPU (torchrun): the path does not shard -- each rank advances an independent replica
 ("replicas only"); value = total simulated days of all ranks / max-over-ranks time.
@@ -43,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="strat1024x8")
-    ap.add_argument("--cpu-sample-steps", type=int, default=1)
+    ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -124,24 +126,21 @@ def cpu_threads():
 
 
 def run_oracle(w, warmup, steps):
-    """Time the FP64 CPU restatement (oracle) on the host cores."""
-    from oracle import qgn_oracle as O
+    """Time the FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c) on the host cores."""
+    from oracle.qgn_oracle import Params
+    from oracle.qgn_ref_c import RefC
 
-    nthr = cpu_threads()
-    O.set_fft_workers(nthr)
-    m = O.QGNOracle(O.Params(**w.params), w.H, w.S, w.U)
-    q = m.initialize_spec(w.qp)
-    st = O.SCHEMES[w.scheme](m)
+    c = RefC(Params(**w.params), w.H, w.S, w.U, scheme=w.scheme)
+    q = c.initialize_spec(w.qp)
     t, dt = 0.0, w.dt0
     for _ in range(warmup):
-        q, t, dt = st.step(q, t, dt)
+        t, dt = c.step(q, t, dt)
     t0 = t
     c0 = time.perf_counter()
     for _ in range(steps):
-        q, t, dt = st.step(q, t, dt)
+        t, dt = c.step(q, t, dt)
     sec = time.perf_counter() - c0
-    O.set_fft_workers(None)
-    return (t - t0) / DAY / sec, sec, steps, nthr
+    return (t - t0) / DAY / sec, sec, steps, c.threads()
 
 
 def reference_arm(args):
@@ -151,10 +150,10 @@ def reference_arm(args):
     from qgn_fortran_b200.inputs import workload
     w = workload(args.workload)
     warm = min(args.warmup, 1)
-    steps = max(1, min(args.steps, 3))
+    steps = max(1, min(args.steps, 10))
     val, sec, n, nthr = run_oracle(w, warm, steps)
-    sample = (f"{n} {w.scheme} steps of {args.workload} after {warm} warm-up step(s), FP64 numpy/scipy "
-              f"restatement (oracle), scipy.fft workers={nthr}")
+    sample = (f"{n} {w.scheme} steps of {args.workload} after {warm} warm-up step(s), FP64 C/OpenMP "
+              f"restatement of the reference (oracle/qgn_ref.c), {nthr} threads, {sec:.1f} s")
     line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": n,
             "warmup": warm, "ms_per_step": 1000.0 * sec / n, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -326,10 +325,11 @@ def ours_arm(args):
 
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
-        val, sec, n, nthr = run_oracle(w, 0, args.cpu_sample_steps)
+        val, sec, n, nthr = run_oracle(w, 1, args.cpu_sample_steps)
         cpu = {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
-               "sample": f"{n} {w.scheme} step(s) of {args.workload} from the seeded IC, FP64 numpy/scipy "
-                         f"restatement (oracle), scipy.fft workers={nthr}, {sec:.1f} s"}
+               "sample": f"{n} {w.scheme} steps of {args.workload} after 1 warm-up step from the seeded IC, "
+                         f"FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c), {nthr} threads, "
+                         f"{sec:.1f} s"}
 
     line = {"metric": METRIC, "value": days_all / (ms_all / 1000.0), "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all / args.steps,
