@@ -59,6 +59,21 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_over_ranks(ms, units, ws, device="cuda"):
+    """Whole-job numbers of the replicas: the slowest rank's time and the sum of the units
+    (simulated days) of all ranks.  ws == 1 returns the inputs."""
+    if ws <= 1:
+        return ms, units
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([ms, units], dtype=torch.float64, device=device)
+    mx = tt.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = tt.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(sm[1])
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -231,15 +246,7 @@ def ours_arm(args):
     g.lib.qgn_profile_enable(g.ctx, 0)
     roof_ms = sum(f[0] for f in fam)
 
-    if ws > 1:
-        tt = torch.tensor([ms, days], dtype=torch.float64, device="cuda")
-        mx = tt.clone()
-        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        sm = tt.clone()
-        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-        ms_all, days_all = float(mx[0]), float(sm[1])
-    else:
-        ms_all, days_all = ms, days
+    ms_all, days_all = reduce_over_ranks(ms, days, ws)
 
     # end-to-end through the drop-in TimeStep (qgn_step) with pinned host q_hat
     e2e = None
@@ -259,13 +266,7 @@ def ours_arm(args):
         e1.synchronize()
         ems = e0.elapsed_time(e1)
         edays = (t - te0) / DAY
-        if ws > 1:
-            tt = torch.tensor([ems, edays], dtype=torch.float64, device="cuda")
-            mx = tt.clone()
-            torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-            sm = tt.clone()
-            torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-            ems, edays = float(mx[0]), float(sm[1])
+        ems, edays = reduce_over_ranks(ems, edays, ws)
         kept = 16 * (w.params["nx"] // 3) * (w.params["ny"] - w.params["ny"] // 3 - 1) * w.params["nz"]
         full = 16 * (w.params["nx"] // 2 + 1) * w.params["ny"] * w.params["nz"]
         e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
@@ -293,13 +294,7 @@ def ours_arm(args):
         mms = m0.elapsed_time(m1)
         tm1, _ = gm.time()
         mdays = (tm1 - tm0) / DAY
-        if ws > 1:
-            tt = torch.tensor([mms, mdays], dtype=torch.float64, device="cuda")
-            mx = tt.clone()
-            torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-            sm = tt.clone()
-            torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-            mms, mdays = float(mx[0]), float(sm[1])
+        mms, mdays = reduce_over_ranks(mms, mdays, ws)
         mixed = {"value": mdays / (mms / 1000.0), "unit": UNIT, "ms_per_step": mms / args.steps,
                  "ms_per_step_vs_fp64": (ms_all / args.steps) / (mms / args.steps),
                  "dtype": "f32 transforms/RHS/stage storage, f64 state/GetPsi/error norm/controller"}
