@@ -127,6 +127,15 @@ int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins)
 int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_phys);
 
 /*
+ * The fields WriteQPmodal writes (QGN_Module.f90:381-440): q_mode, p_mode (psi_mode) and
+ * J_mode -- the vertical-mode projections of q_hat, of psi_hat and of the full (undealiased)
+ * Jacobian spectrum -- in physical space, real(dp)(nx,ny,nz) column-major each.  q_hat is a
+ * host spectral array (the reference's q_hat(nx/2+1,ny,nz), dealiased), or NULL for the
+ * resident state; the resident state and the stepper's history are left unchanged.
+ */
+int qgn_physical_modal(qgn_ctx* ctx, const double* q_hat, double* q_mode, double* p_mode, double* J_mode);
+
+/*
  * Set the resident state from a physical PV field real(dp) q(nx,ny,nz): the forward
  * transform and DeAlias of Initialize (QGN_Module.f90:179-183), as used for the IC and
  * for restarts from q.%09d.dat (QGN_Driver.f90:21-30).

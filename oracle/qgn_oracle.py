@@ -283,6 +283,33 @@ class QGNOracle:
         v = self.s2g_scaled((1j * self.kx)[None] * psi)
         return 0.5 * np.mean(u ** 2 + v ** 2, axis=(1, 2)) * self.H / p.Htot
 
+    # -- WriteQPmodal (QGN_Module.f90:381-440) -----------------------------------
+    def write_qp_modal(self, q_hat):
+        """The three physical fields WriteQPmodal writes: q_mode, p_mode, J_mode, each (nz, ny, nx).
+
+        The Jacobian is the full undealiased spectrum of i kx (uq)^ + i ky (vq)^
+        (QGN_Module.f90:388), projected on the vertical modes like q_hat (lines 392-398);
+        psi_mode = q_mode / (-k2 + EVals) with the (0,0) mode zero (lines 399-400).
+        """
+        p = self.p
+        nz = p.nz
+        H, Modes, EVals = self.H, self.Modes, self.EVals
+        jaco = self.jacobian(q_hat)
+        q_mode = np.zeros_like(q_hat)
+        j_mode = np.zeros_like(q_hat)
+        psi_mode = np.empty_like(q_hat)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            for k in range(nz):
+                for kk in range(nz):
+                    q_mode[k] = q_mode[k] + (H[kk] * Modes[kk, k]) * q_hat[kk]
+                    j_mode[k] = j_mode[k] + (H[kk] * Modes[kk, k]) * jaco[kk]
+                q_mode[k] = q_mode[k] / p.Htot
+                j_mode[k] = j_mode[k] / p.Htot
+                psi_mode[k] = q_mode[k] / (-self.k2 + EVals[k])
+                psi_mode[k, 0, 0] = 0.0
+        shape = (p.ny, p.nx)
+        return _irfft2(q_mode, shape), _irfft2(psi_mode, shape), _irfft2(j_mode, shape)
+
 
 # ---------------------------------------------------------------------------
 # Time steppers (the include files selected at QGN_Module.f90:306)

@@ -65,6 +65,7 @@ SIGNATURES = {
     "qgn_diagnostics": (C.c_int, [_ctxp, _dp, _dp, C.c_int]),
     "qgn_physical": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_set_state_physical": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
+    "qgn_physical_modal": (C.c_int, [_ctxp, _dp, _dp, _dp, _dp]),
     "qgn_rejects": (C.c_int, [_ctxp, C.POINTER(C.c_longlong)]),
     "qgn_profile_enable": (C.c_int, [_ctxp, C.c_int]),
     "qgn_profile_read": (C.c_int, [_ctxp, C.c_int, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

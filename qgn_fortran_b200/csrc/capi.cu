@@ -534,6 +534,7 @@ void free_all(qgn_ctx* ctx) {
     if (b.full) cudaFree(b.full);
     if (b.phys) cudaFree(b.phys);
     if (b.diag) cudaFree(b.diag);
+    if (b.modal_scratch) cudaFree(b.modal_scratch);
     b = Buffers{};
     if (ctx->host_pin) cudaFreeHost(ctx->host_pin);
     ctx->host_pin = nullptr;
@@ -863,6 +864,37 @@ int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_
         CK(launch_to_phys(g, b, b.psi, b.phys, ctx->stream));
         CK(cudaMemcpyAsync(psi_phys, b.phys, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
     }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
+int qgn_physical_modal(qgn_ctx* ctx, const double* q_hat, double* q_mode, double* p_mode, double* J_mode) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!q_mode || !p_mode || !J_mode) return set_err(ctx, QGN_ERR_ARG, "NULL output");
+    CK(cudaSetDevice(ctx->device));
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    const Geom gf = full_geom(g);
+    const size_t np = (size_t)g.nz * g.ny * g.nx;
+    const size_t half = gf.hsize(), fc = gf.csize();
+    // scratch: 3 outputs + 3 physical work fields (doubles), full half field + 2 full spectra (double2)
+    const size_t need = 6 * np + 2 * (half + 2 * fc);
+    if (!b.modal_scratch) CK(dalloc(&b.modal_scratch, need));
+    double* outs = b.modal_scratch;
+    double* phys3 = outs + 3 * np;
+    double2* full_half = reinterpret_cast<double2*>(outs + 6 * np);
+    double2* fa = full_half + half;
+    double2* fb = fa + fc;
+    const double2* src = b.q;
+    if (q_hat) {
+        RET(upload_kept(ctx, q_hat, b.err));
+        src = b.err;
+    }
+    CK(launch_modal_fields(g, b, src, outs, outs + np, outs + 2 * np, full_half, fa, fb, phys3, ctx->stream));
+    CK(cudaMemcpyAsync(q_mode, outs, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(p_mode, outs + np, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(J_mode, outs + 2 * np, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return QGN_OK;
 }

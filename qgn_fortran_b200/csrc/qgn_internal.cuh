@@ -89,6 +89,7 @@ struct Buffers {
     double* red = nullptr;       // reduction partials
     double* Hw = nullptr;        // H(k)/Htot per layer
     double* diag = nullptr;      // diagnostics output (lazy)
+    double* modal_scratch = nullptr;  // WriteQPmodal work space (lazy)
     LayerConst* lc = nullptr;
     ModalConst* mc = nullptr;
     DevScalars* sc = nullptr;
@@ -135,6 +136,13 @@ cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const
 cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s);
 // physical field (c2r/(nx*ny)) of a compact field into b.phys ([nz][ny][nx])
 cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, double* out, cudaStream_t s);
+// the fields of WriteQPmodal (QGN_Module.f90:381-440): q_mode, psi_mode and J_mode in physical
+// space (out_* [nz][ny][nx]); scratch: full_half [nz][ny][round4(nxh)], fa/fb full compact
+// [nz][nxh][ny], phys3 three physical fields
+Geom full_geom(const Geom& g);
+cudaError_t launch_modal_fields(const Geom& g, const Buffers& b, const double2* q, double* out_q, double* out_p,
+                                double* out_j, double2* full_half, double2* fa, double2* fb, double* phys3,
+                                cudaStream_t s);
 // forward transform + dealias of a physical field [nz][ny][nx] into a compact field
 cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys, double2* out, cudaStream_t s);
 

@@ -220,7 +220,8 @@ __global__ void __launch_bounds__(YInvCfg<NY, CT>::THREADS, minb(YInvCfg<NY, CT>
             const CT f1 = sm[c * C::TS + fpad(2 * p)], f2 = sm[c * C::TS + fpad(2 * p + 1)];
             const bool ok = k < g.nkx;
             CT* row = dl + (size_t)p * 2 * g.nkxp;
-            row[k] = ok ? pack_lo(f1, f2, k == 0) : cmk<CT>(0.0, 0.0);
+            // Re parts at kx = 0 and at the kx Nyquist column (kept only in the full-spectrum geometry)
+            row[k] = ok ? pack_lo(f1, f2, k == 0 || 2 * k == g.nx) : cmk<CT>(0.0, 0.0);
             row[g.nkxp + k] = (ok && k > 0) ? pack_hi(f1, f2) : cmk<CT>(0.0, 0.0);
         }
         if (f + 1 < NF) __syncthreads();   // the next field's first pass reuses the slots
@@ -732,6 +733,122 @@ cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, do
     cudaError_t e;
     if ((e = launch_yinv<double2>(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
     return launch_xinv1<1>(g, b, nullptr, out, s);
+}
+
+
+// ------------------------------------------------------------------------------------
+// WriteQPmodal support (QGN_Module.f90:381-440): the reference's Jacobian there is the full,
+// undealiased spectrum of i kx (uq)^ + i ky (vq)^.  The transform kernels above run on it
+// with a "full" geometry -- every kx up to Nyquist and every ky kept, compact index = ky index.
+// ------------------------------------------------------------------------------------
+Geom full_geom(const Geom& g) {
+    Geom f = g;
+    f.nkx = g.nxh;
+    f.nkxp = (g.nxh + 3) / 4 * 4;
+    f.kylo = g.ny;
+    f.kyshift = 0;
+    f.nky = g.ny;
+    return f;
+}
+
+__global__ void k_uv_hat(Geom g, const double2* __restrict__ psi, double2* __restrict__ uh, double2* __restrict__ vh) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t total = P * g.nz;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t p = e % P;
+        const int kx = (int)(p / g.nky), m = (int)(p % g.nky);
+        const double kxv = g.dkx * kx, kyv = g.kyval(g.jfull(m));
+        const double2 v = psi[e];
+        uh[e] = make_double2(kyv * v.y, -kyv * v.x);      // -i ky psi_hat (QGN_Module.f90:223)
+        vh[e] = make_double2(-kxv * v.y, kxv * v.x);      //  i kx psi_hat (QGN_Module.f90:224)
+    }
+}
+
+__global__ void k_products(size_t n, const double* __restrict__ q, double* __restrict__ u, double* __restrict__ v) {
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const double qq = q[e];
+        u[e] = u[e] * qq;     // u_phys*q_phys
+        v[e] = v[e] * qq;     // v_phys*q_phys
+    }
+}
+
+// jaco_hat = i kx uq_hat + i ky vq_hat on the full spectrum (QGN_Module.f90:244-247), in place into uq
+__global__ void k_jac_full(Geom gf, double2* __restrict__ uq, const double2* __restrict__ vq) {
+    const size_t P = (size_t)gf.nkx * gf.nky;
+    const size_t total = P * gf.nz;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t p = e % P;
+        const int kx = (int)(p / gf.nky), j = (int)(p % gf.nky);
+        const double kxv = gf.dkx * kx, kyv = gf.kyval(j);
+        const double2 a = uq[e], b = vq[e];
+        uq[e] = make_double2(-kxv * a.y - kyv * b.y, kxv * a.x + kyv * b.x);
+    }
+}
+
+// modal projection x_mode(k) = sum_kk H(kk) Modes(kk,k) x(kk) / Htot (QGN_Module.f90:392-398), and
+// optionally psi_mode = q_mode / (-k^2 + EVals(k)) with psi_mode(1,1) = 0 (QGN_Module.f90:399-400)
+__global__ void k_modal_proj(Geom g, const ModalConst* __restrict__ mc, const double2* __restrict__ x,
+                             double2* __restrict__ xm, double2* __restrict__ pm) {
+    const size_t P = (size_t)g.nkx * g.nky;
+    const int nz = g.nz;
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(p / g.nky), m = (int)(p % g.nky);
+        const double kxv = g.dkx * kx, kyv = g.kyval(g.jfull(m));
+        const double k2 = kxv * kxv + kyv * kyv;
+        for (int k = 0; k < nz; ++k) {
+            double2 acc = make_double2(0.0, 0.0);
+            for (int kk = 0; kk < nz; ++kk) {
+                const double c = mc->proj[k * nz + kk];
+                const double2 v = x[(size_t)kk * P + p];
+                acc.x += c * v.x;
+                acc.y += c * v.y;
+            }
+            const double2 qm = make_double2(acc.x / mc->Htot, acc.y / mc->Htot);
+            xm[(size_t)k * P + p] = qm;
+            if (pm) {
+                const double den = -k2 + mc->evals[k];
+                pm[(size_t)k * P + p] = (p == 0) ? make_double2(0.0, 0.0) : make_double2(qm.x / den, qm.y / den);
+            }
+        }
+    }
+}
+
+cudaError_t launch_modal_fields(const Geom& g, const Buffers& b, const double2* q, double* out_q, double* out_p,
+                                double* out_j, double2* full_half, double2* fa, double2* fb, double* phys3,
+                                cudaStream_t s) {
+    // fa and fb (full spectra) are larger than a compact field: they hold u_hat, v_hat first and
+    // the compact q_mode, psi_mode last; b.psi is overwritten, nothing else of b is touched
+    cudaError_t e;
+    const int blocks = 148 * 8;
+    const size_t np = (size_t)g.nz * g.ny * g.nx;
+    double* Pq = phys3;
+    double* Pu = phys3 + np;
+    double* Pv = phys3 + 2 * np;
+    // GetPsi, u_hat, v_hat and the physical fields of the Jacobian (QGN_Module.f90:218-234)
+    if ((e = launch_modal(g, b.mc, q, b.psi, s)) != cudaSuccess) return e;
+    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)g.csize(), s, k_uv_hat<<<blocks, 256, 0, s>>>(g, b.psi, fa, fb));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_to_phys(g, b, q, Pq, s)) != cudaSuccess) return e;
+    if ((e = launch_to_phys(g, b, fa, Pu, s)) != cudaSuccess) return e;
+    if ((e = launch_to_phys(g, b, fb, Pv, s)) != cudaSuccess) return e;
+    QGN_LAUNCH(KID_LAYOUT, 40.0 * (double)np, s, k_products<<<blocks, 256, 0, s>>>(np, Pq, Pu, Pv));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // full-spectrum r2c of u*q and v*q and the undealiased Jacobian (QGN_Module.f90:235-247)
+    const Geom gf = full_geom(g);
+    Buffers bf = b;
+    bf.hq = full_half;
+    if ((e = launch_from_phys(gf, bf, Pu, fa, s)) != cudaSuccess) return e;
+    if ((e = launch_from_phys(gf, bf, Pv, fb, s)) != cudaSuccess) return e;
+    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)gf.csize(), s, k_jac_full<<<blocks, 256, 0, s>>>(gf, fa, fb));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // modal projections and their physical fields (QGN_Module.f90:390-415)
+    QGN_LAUNCH(KID_MODAL, 32.0 * (double)gf.csize(), s, k_modal_proj<<<blocks, 256, 0, s>>>(gf, b.mc, fa, fb, nullptr));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_to_phys(gf, bf, fb, out_j, s)) != cudaSuccess) return e;
+    QGN_LAUNCH(KID_MODAL, 48.0 * (double)g.csize(), s, k_modal_proj<<<blocks, 256, 0, s>>>(g, b.mc, q, fa, fb));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_to_phys(g, b, fa, out_q, s)) != cudaSuccess) return e;
+    return launch_to_phys(g, b, fb, out_p, s);
 }
 
 }  // namespace qgn

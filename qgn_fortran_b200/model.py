@@ -169,6 +169,22 @@ class QGNModule:
             np.ascontiguousarray(arr, dtype="<f8").tofile(path)
         return qphys, pphys
 
+    def physical_modal(self, q_hat=None):
+        """The physical q_mode, p_mode and J_mode fields of WriteQPmodal (QGN_Module.f90:381-440)."""
+        out = [np.empty(self.physical_shape()) for _ in range(3)]
+        src = None if q_hat is None else dptr(self._spec(q_hat))
+        self._check(self.lib.qgn_physical_modal(self.ctx, src, *(dptr(a) for a in out)), "qgn_physical_modal")
+        return tuple(out)
+
+    def write_qp_modal(self, q_hat, rec_no: int, nt: int, directory: str = "."):
+        """WriteQPmodal: q_mode/p_mode/J_mode.%09d.dat raw float64 physical fields (QGN_Module.f90:381-440)."""
+        fields = self.physical_modal(q_hat)
+        os.makedirs(directory, exist_ok=True)
+        for prefix, arr in zip(("q_mode", "p_mode", "J_mode"), fields):
+            path = os.path.join(directory, f"{prefix}.{nt:09d}.dat")
+            np.ascontiguousarray(arr, dtype="<f8").tofile(path)
+        return fields
+
     def cleanup(self):
         if getattr(self, "ctx", None):
             self.lib.qgn_destroy(self.ctx)

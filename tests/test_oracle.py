@@ -253,6 +253,33 @@ def test_leith_parseval_matches_physical():
     assert LEITH_13 == 1.2999999523162842
 
 
+def test_write_qp_modal_identities():
+    """WriteQPmodal: the modes back-project onto q, psi and the full Jacobian; a single
+    Fourier mode in one vertical mode gives that mode alone, psi_mode = q_mode/(-k^2+EVals),
+    and a zero Jacobian."""
+    nx, ny, nz = 32, 64, 3
+    m = small_model(nx=nx, ny=ny, nz=nz)
+    q = m.initialize_spec(seeded_random_pv(nx, ny, nz, 6.0, 1e-6, seed=2))
+    qm, pm, jm = m.write_qp_modal(q)
+    back = lambda f: np.einsum("ab,byx->ayx", m.Modes, f)
+    tol = 1e-12
+    assert np.allclose(back(qm), m.s2g_scaled(q), rtol=0, atol=tol * np.abs(qm).max())
+    assert np.allclose(back(pm), m.s2g_scaled(m.get_psi(q)), rtol=0, atol=tol * np.abs(pm).max())
+    assert np.allclose(back(jm), m.s2g_scaled(m.jacobian(q)), rtol=0, atol=tol * np.abs(jm).max())
+    # one Fourier mode (kx = 3, ky = 2) carried by vertical mode 1
+    x = np.arange(nx) * m.p.Lx / nx
+    y = np.arange(ny) * m.p.Ly / ny
+    kx, ky = 3 * 2 * np.pi / m.p.Lx, 2 * 2 * np.pi / m.p.Ly
+    f = np.cos(kx * x[None, :] + ky * y[:, None])
+    qp = 1e-5 * m.Modes[:, 1][:, None, None] * f[None]
+    qm, pm, jm = m.write_qp_modal(m.initialize_spec(qp))
+    assert np.allclose(qm[1], 1e-5 * f, atol=1e-18)
+    assert np.allclose(qm[[0, 2]], 0.0, atol=1e-18)
+    p1 = 1e-5 * f / (-(kx * kx + ky * ky) + m.EVals[1])
+    assert np.allclose(pm[1], p1, rtol=0, atol=1e-12 * np.abs(p1).max())
+    assert np.abs(jm).max() <= 1e-12 * (kx * kx + ky * ky) * np.abs(p1).max() * 1e-5
+
+
 # ---------------------------------------------------------------------------------------
 # Golden fixtures are reproduced by the oracle
 # ---------------------------------------------------------------------------------------
