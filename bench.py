@@ -41,7 +41,7 @@ DAY = 86400.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="strat1024x8")
@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-members", type=int, default=64)
+    ap.add_argument("--ens-steps", type=int, default=20)
     return ap.parse_args()
 
 
@@ -103,6 +106,14 @@ class ClockSampler:
                  "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait (bounded) for its first sample so the
+        # samples cover the timed region
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and self.proc.poll() is None:
+            if os.path.getsize(self.out) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -159,16 +170,19 @@ def run_oracle(w, warmup, steps):
 
 
 def reference_arm(args):
+    """The reference algorithm on the host cores over the same step window as our arm: from the
+    seeded IC, W untimed steps, then K timed steps, so both arms simulate the same days."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     from qgn_fortran_b200.inputs import workload
     w = workload(args.workload)
-    warm = min(args.warmup, 1)
-    steps = max(1, min(args.steps, 10))
+    warm = max(0, args.warmup)
+    steps = max(1, args.steps)
     val, sec, n, nthr = run_oracle(w, warm, steps)
-    sample = (f"{n} {w.scheme} steps of {args.workload} after {warm} warm-up step(s), FP64 C/OpenMP "
-              f"restatement of the reference (oracle/qgn_ref.c), {nthr} threads, {sec:.1f} s")
+    sample = (f"steps {warm + 1}..{warm + n} of {w.scheme} on {args.workload} from the seeded IC (the window our "
+              f"arm times), FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c), {nthr} threads, "
+              f"{sec:.1f} s timed")
     line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": n,
             "warmup": warm, "ms_per_step": 1000.0 * sec / n, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -248,21 +262,29 @@ def ours_arm(args):
 
     ms_all, days_all = reduce_over_ranks(ms, days, ws)
 
-    # end-to-end through the drop-in TimeStep (qgn_step) with pinned host q_hat
+    # end-to-end through the drop-in TimeStep (qgn_step) with pinned host q_hat, over the same
+    # step window from the IC in a fresh context (the controller's err0 starts at TOL again)
     e2e = None
     if not args.no_e2e:
-        qh = torch.empty(q.shape, dtype=torch.complex128, pin_memory=True).numpy()
-        g.get_state(qh)
-        t, dt = g.time()
+        gE = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme)
+        q0 = gE.initialize(w.qp, 0.0, w.dt0)
+        qh = torch.empty(q0.shape, dtype=torch.complex128, pin_memory=True).numpy()
+        qh[...] = q0
+        sE = _lib.C.c_void_p()
+        gE.lib.qgn_stream(gE.ctx, _lib.C.byref(sE))
+        estream = torch.cuda.ExternalStream(sE.value)
+        t, dt = 0.0, w.dt0
+        for _ in range(args.warmup):
+            t, dt = gE.time_step(qh, t, dt)
         te0 = t
         barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(estream)
         for _ in range(args.steps):
-            t, dt = g.time_step(qh, t, dt)
-        e1.record(stream)
+            t, dt = gE.time_step(qh, t, dt)
+        e1.record(estream)
         e1.synchronize()
         ems = e0.elapsed_time(e1)
         edays = (t - te0) / DAY
@@ -270,7 +292,9 @@ def ours_arm(args):
         kept = 16 * (w.params["nx"] // 3) * (w.params["ny"] - w.params["ny"] // 3 - 1) * w.params["nz"]
         full = 16 * (w.params["nx"] // 2 + 1) * w.params["ny"] * w.params["nz"]
         e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
-               "d2h_bytes_per_step": full, "ms_per_step": ems / args.steps}
+               "d2h_bytes_per_step": full, "ms_per_step": ems / args.steps,
+               "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the IC"}
+        gE.cleanup()
 
     # ---- the same workload in the mixed mode (FP32 transforms/RHS/stages, FP64 state and control)
     mixed = None
@@ -300,6 +324,10 @@ def ours_arm(args):
                  "dtype": "f32 transforms/RHS/stage storage, f64 state/GetPsi/error norm/controller"}
         gm.cleanup()
 
+    ensemble = None
+    if not args.no_ensemble:
+        ensemble = ensemble_bench(args, ws)
+
     if rank != 0:
         g.cleanup()
         if ws > 1:
@@ -320,11 +348,14 @@ def ours_arm(args):
 
     cpu = None
     if ws == 1 and not args.no_cpu_baseline:
-        val, sec, n, nthr = run_oracle(w, 1, args.cpu_sample_steps)
-        cpu = {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
+        # a bounded sample: seconds per step of the reference algorithm on the host cores, turned
+        # into days/s with the mean dt of the timed GPU window (both compute the same trajectory)
+        _, sec, n, nthr = run_oracle(w, 1, args.cpu_sample_steps)
+        cpu_val = (days_all / args.steps) / (sec / n)
+        cpu = {"value": cpu_val, "unit": UNIT, "cores": nthr, "kind": "port", "ms_per_step": 1000.0 * sec / n,
                "sample": f"{n} {w.scheme} steps of {args.workload} after 1 warm-up step from the seeded IC, "
                          f"FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c), {nthr} threads, "
-                         f"{sec:.1f} s"}
+                         f"{sec:.1f} s; days/s = mean dt of the timed window / CPU s per step"}
 
     line = {"metric": METRIC, "value": days_all / (ms_all / 1000.0), "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all / args.steps,
@@ -333,13 +364,74 @@ def ours_arm(args):
             "config": {"workload": args.workload, "grid": f"{w.params['nx']}x{w.params['ny']}x{w.params['nz']}",
                        "scheme": w.scheme, "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
-                       "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects()},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "gpu_launches": launches,
+                       "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects(),
+                       "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the seeded IC"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "ensemble": ensemble, "gpu_launches": launches,
             "clocks": clk, "kernels": kernels}
     print(json.dumps(line), flush=True)
     g.cleanup()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def ensemble_bench(args, ws):
+    """Batched heterogeneous ensemble: members of 128^2/256^2/512^2 x 2/4/8 layers, BSRK3 with
+    adaptive dt, one launch per pass for all members (mixed and FP64), against the same members
+    stepped one after another through their own contexts (FP64 BSRK3)."""
+    import torch
+
+    from qgn_fortran_b200 import QGNEnsemble, QGNModule
+    from qgn_fortran_b200.inputs import ensemble_members
+
+    members = ensemble_members(args.ens_members)
+    gs = [QGNModule(w.params, w.H, w.S, w.U, scheme="bsrk3") for w in members]
+    K = args.ens_steps
+    out = {"members": len(members), "steps": K,
+           "sizes": {f"{n}^2x{z}": sum(1 for w in members if w.params["nx"] == n and w.params["nz"] == z)
+                     for n in (128, 256, 512) for z in (2, 4, 8)},
+           "scheme": "bsrk3 (PI.3.4 adaptive dt)"}
+
+    def reset():
+        for g, w in zip(gs, members):
+            g.initialize(w.qp, 0.0, w.dt0)
+
+    for prec in ("mixed", "fp64"):
+        reset()
+        ens = QGNEnsemble(gs, precision=prec)
+        ens.advance(max(args.warmup, 1))          # first call: FSAL, autotune, graph capture
+        st = torch.cuda.ExternalStream(ens.stream())
+        t0 = [g.time()[0] for g in gs]
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ens.advance(K)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        days = sum(g.time()[0] - a for g, a in zip(gs, t0)) / DAY
+        ms, days = reduce_over_ranks(ms, days, ws)
+        out[prec] = {"member_days_per_s": days / (ms / 1000.0), "member_steps_per_s": len(gs) * K / (ms / 1000.0),
+                     "ms_per_ensemble_step": ms / K, "tuning": ens.tuning()}
+        ens.close()
+    # the same members one after another, each through its own context (FP64 BSRK3, qgn_advance_resident)
+    reset()
+    for g in gs:
+        g.advance_resident(max(args.warmup, 1))
+    t0 = [g.time()[0] for g in gs]
+    torch.cuda.synchronize()
+    s = time.perf_counter()
+    for g in gs:
+        g.advance_resident(K)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - s
+    days = sum(g.time()[0] - a for g, a in zip(gs, t0)) / DAY
+    out["sequential_fp64"] = {"member_days_per_s": days / sec, "member_steps_per_s": len(gs) * K / sec,
+                              "timing": "host wall clock around synchronous per-member calls"}
+    out["speedup_mixed_vs_sequential"] = out["mixed"]["member_days_per_s"] / out["sequential_fp64"]["member_days_per_s"]
+    for g in gs:
+        g.cleanup()
+    return out
 
 
 def read_traffic(workload, kernel):

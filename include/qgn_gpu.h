@@ -200,6 +200,36 @@ int qgn_rhs_static(const qgn_params* p, const double* H, const double* uBar, con
                    const double* Modes, const double* EVals, const double* q_hat_dev, double* rhs_dev,
                    void* stream);
 
+/*
+ * ---- Ensembles ------------------------------------------------------------------------
+ * No counterpart in the reference (one model per process there): independent members --
+ * contexts made by qgn_create with scheme QGN_SCHEME_BSRK3 and precision QGN_PREC_FP64 --
+ * advanced together with BSRK3.f90's scheme.  Grid sizes nx, ny in {128, 256, 512} and
+ * layer counts 2..8 or 16 may differ between members; C_d must be 0.  Each pass of an
+ * attempt is one launch for all members, the attempts run as a device-conditioned CUDA
+ * graph loop, and the first advance autotunes the tile widths and grid sizes.
+ *
+ * The ensemble borrows the contexts (they must outlive it) and works on their buffers:
+ * load states with qgn_set_state (which also restarts a member's FSAL RHS0) and read them
+ * with qgn_get_state.  `precision` QGN_PREC_MIXED runs the transforms, stage right-hand
+ * sides and stage inputs in FP32, with FP64 state, stage sums, GetPsi arithmetic, error
+ * norm and controller.
+ */
+typedef struct qgn_ens qgn_ens;
+int qgn_ens_create(qgn_ctx* const* members, int nmembers, int precision, qgn_ens** out);
+/* every member takes nsteps accepted steps (TimeStep nsteps times); members in lockstep */
+int qgn_ens_advance(qgn_ens* ens, int nsteps);
+/* autotuner's choice for pass 0 (y-inverse), 1 (x pass), 2 (y-forward): CTA threads,
+ * CTAs per SM of the persistent grid (0 = one CTA per tile) and the timed ms per launch */
+int qgn_ens_tuning(qgn_ens* ens, int pass, int* threads, int* ctas_per_sm, float* ms);
+int qgn_ens_profile_enable(qgn_ens* ens, int enable);
+int qgn_ens_profile_read(qgn_ens* ens, int kernel, double* total_ms, double* bytes,
+                         long long* timed_launches, long long* launches);
+/* the ensemble's CUDA stream (cudaStream_t): its launches run there */
+int qgn_ens_stream(qgn_ens* ens, void** stream);
+const char* qgn_ens_last_error(qgn_ens* ens);
+int qgn_ens_destroy(qgn_ens* ens);
+
 /* Message of the last failing call on this context (never NULL). */
 const char* qgn_last_error(const qgn_ctx* ctx);
 

@@ -66,6 +66,16 @@ SIGNATURES = {
     "qgn_physical": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_set_state_physical": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
     "qgn_physical_modal": (C.c_int, [_ctxp, _dp, _dp, _dp, _dp]),
+    "qgn_ens_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "qgn_ens_advance": (C.c_int, [C.c_void_p, C.c_int]),
+    "qgn_ens_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_float)]),
+    "qgn_ens_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
+    "qgn_ens_profile_read": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_longlong)]),
+    "qgn_ens_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "qgn_ens_last_error": (C.c_char_p, [C.c_void_p]),
+    "qgn_ens_destroy": (C.c_int, [C.c_void_p]),
     "qgn_rejects": (C.c_int, [_ctxp, C.POINTER(C.c_longlong)]),
     "qgn_profile_enable": (C.c_int, [_ctxp, C.c_int]),
     "qgn_profile_read": (C.c_int, [_ctxp, C.c_int, _dp, _dp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

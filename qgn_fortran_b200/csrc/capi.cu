@@ -713,6 +713,7 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
 int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);
+    ++ctx->state_version;
     if (!q_hat) return set_err(ctx, QGN_ERR_ARG, "q_hat is NULL");
     CK(cudaSetDevice(ctx->device));
     RET(upload_kept(ctx, q_hat, ctx->b.q));
@@ -743,6 +744,7 @@ int qgn_get_state(qgn_ctx* ctx, double* q_hat, double* t, double* dt) {
 int qgn_advance_resident(qgn_ctx* ctx, int nsteps) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);
+    ++ctx->state_version;
     if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
     CK(cudaSetDevice(ctx->device));
     RET(advance_n(ctx, nsteps));
@@ -754,6 +756,7 @@ int qgn_advance_resident(qgn_ctx* ctx, int nsteps) {
 int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);
+    ++ctx->state_version;
     if (!q_hat || !t || !dt) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
     RET(qgn_set_state(ctx, q_hat, *t, *dt));
@@ -775,6 +778,7 @@ int qgn_step(qgn_ctx* ctx, double* q_hat, double* t, double* dt) { return qgn_ad
 int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);
+    ++ctx->state_version;
     if (!q_hat || !rhs) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     CK(cudaSetDevice(ctx->device));
     Buffers& b = ctx->b;
@@ -902,6 +906,7 @@ int qgn_physical_modal(qgn_ctx* ctx, const double* q_hat, double* q_mode, double
 int qgn_set_state_physical(qgn_ctx* ctx, const double* q_phys, double t, double dt) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);
+    ++ctx->state_version;
     if (!q_phys) return set_err(ctx, QGN_ERR_ARG, "q_phys is NULL");
     CK(cudaSetDevice(ctx->device));
     const Geom& g = ctx->g;

@@ -110,6 +110,7 @@ struct qgn_ctx {
     bool first_call = true;
     int ab_calls = 0;
     bool halted = false;           // a step failed; cleared by the next state upload
+    long long state_version = 0;   // bumped by every call that changes the state outside an ensemble
     double* host_pin = nullptr;    // pinned scalar readback
     std::vector<void*> owned;      // every device allocation made at creation
     std::string last_error;

@@ -180,6 +180,33 @@ class Workload:
     dt0: float
 
 
+def ensemble_members(n=64, seed0=1000, sizes=(128, 256, 512), layers=(2, 4, 8), Lx=2.0e6, with_ic=True):
+    """Members of the batched-ensemble workload: grid n^2 drawn uniformly from ``sizes``, layer
+    count from ``layers``; each member's exponential stratification has its own e-folding
+    depth in [500, 1500] m (for N^2 and for the mean flow) and surface flow in
+    [0.02, 0.15] m/s.  BSRK3 with PI.3.4 adaptive dt, absolute TOL = 1e-6 x max|q_IC|,
+    explicit hyperviscosity with a 1-day grid-scale e-folding, C_d = 0.  The IC of member m
+    is the seeded random PV field (peak wavenumber 8, rms 1e-6) with seed ``seed0 + m``.
+    Returns a list of ``Workload``."""
+    out = []
+    for m in range(n):
+        rng = np.random.default_rng(seed0 + m)
+        nxy = int(rng.choice(sizes))
+        nz = int(rng.choice(layers))
+        efold = float(rng.uniform(500.0, 1500.0))
+        U0 = float(rng.uniform(0.02, 0.15))
+        H, S, U = exponential_stratification(nz, N_efold=efold, U0=U0, U_efold=efold)
+        qp = seeded_random_pv(nxy, nxy, nz, 8.0, 1.0e-6, seed0 + m) if with_ic else None
+        tol = 1.0e-6 * (float(np.max(np.abs(qp))) if qp is not None else 4.0e-6)
+        beta = 2.0e-11
+        A8 = 1.0 / (86400.0 * (math.pi * nxy / Lx) ** 8)
+        p = dict(nx=nxy, ny=nxy, nz=nz, Lx=Lx, Ly=Lx, Htot=4000.0, f0=1.0e-4, beta=beta,
+                 A2=0.0, A8=A8, r0=1.0e-7, C_d=0.0, TOL=tol, is_explicit=True,
+                 dt_max=math.pi / (beta * Lx))
+        out.append(Workload(f"member{m}_{nxy}x{nz}", p, H, S, U, qp, "bsrk3", 1800.0))
+    return out
+
+
 def workload(name: str, nx=None, nz=None, seed=None, with_ic=True) -> Workload:
     """Named synthetic workloads.
 

@@ -254,3 +254,79 @@ class QGNModule:
         n = C.c_longlong()
         self._check(self.lib.qgn_rejects(self.ctx, C.byref(n)), "qgn_rejects")
         return n.value
+
+
+class QGNEnsemble:
+    """Independent members advanced together with BSRK3 (BSRK3.f90), one launch per pass.
+
+    ``members`` are ``QGNModule`` instances made with ``scheme="bsrk3"`` (FP64 contexts;
+    nx, ny in {128, 256, 512}, nz in 2..8 or 16, C_d = 0).  The ensemble borrows their
+    device state: load states with ``member.set_state`` and read them with
+    ``member.get_state``.  ``precision="mixed"`` runs transforms, stage right-hand sides
+    and stage inputs in FP32 with FP64 state, stage sums, GetPsi, error norm and controller.
+    """
+
+    PASSES = ("yinv", "xpass", "yfwd")
+
+    def __init__(self, members, precision: str = "mixed"):
+        self.lib = _lib.load()
+        self.members = list(members)
+        n = len(self.members)
+        arr = (C.c_void_p * n)(*[m.ctx.value for m in self.members])
+        ens = C.c_void_p()
+        rc = self.lib.qgn_ens_create(arr, n, _lib.PRECISIONS[precision], C.byref(ens))
+        if rc != 0:
+            raise QGNError(rc, f"qgn_ens_create({n} members, precision={precision})")
+        self.ens = ens
+        self.precision = precision
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self.lib.qgn_ens_last_error(self.ens)
+            raise QGNError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def advance(self, nsteps: int):
+        """Every member takes ``nsteps`` accepted steps."""
+        self._check(self.lib.qgn_ens_advance(self.ens, int(nsteps)), "qgn_ens_advance")
+
+    def stream(self):
+        """The ensemble's cudaStream_t (as an integer handle)."""
+        sp = C.c_void_p()
+        self._check(self.lib.qgn_ens_stream(self.ens, C.byref(sp)), "qgn_ens_stream")
+        return sp.value
+
+    def tuning(self):
+        """The autotuner's choice per right-hand-side pass."""
+        out = {}
+        for i, name in enumerate(self.PASSES):
+            th, cps, ms = C.c_int(), C.c_int(), C.c_float()
+            self._check(self.lib.qgn_ens_tuning(self.ens, i, C.byref(th), C.byref(cps), C.byref(ms)),
+                        "qgn_ens_tuning")
+            out[name] = {"threads": th.value, "ctas_per_sm": cps.value, "ms": ms.value}
+        return out
+
+    def profile_enable(self, on: bool = True):
+        self._check(self.lib.qgn_ens_profile_enable(self.ens, int(bool(on))), "qgn_ens_profile_enable")
+
+    def profile_read(self):
+        out = {}
+        for k in range(_lib.QGN_KERNEL_FAMILIES):
+            ms, nb = C.c_double(), C.c_double()
+            timed, launches = C.c_longlong(), C.c_longlong()
+            self._check(self.lib.qgn_ens_profile_read(self.ens, k, C.byref(ms), C.byref(nb), C.byref(timed),
+                                                      C.byref(launches)), "qgn_ens_profile_read")
+            if launches.value:
+                out[self.lib.qgn_kernel_name(k).decode()] = {"ms": ms.value, "bytes": nb.value,
+                                                            "timed": timed.value, "launches": launches.value}
+        return out
+
+    def close(self):
+        if getattr(self, "ens", None):
+            self.lib.qgn_ens_destroy(self.ens)
+            self.ens = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
