@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-closure", action="store_true")
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
     return ap.parse_args()
@@ -328,6 +329,15 @@ def ours_arm(args):
     if not args.no_ensemble:
         ensemble = ensemble_bench(args, ws)
 
+    # learned closure: 1024^2 x 4 truth -> 128^2 training data -> trained network -> 128^2 runs
+    # with QG-Leith and with the closure against the coarse-grained truth (KE spectrum, days/s)
+    closure = None
+    if not args.no_closure:
+        from qgn_fortran_b200.closure_experiment import run as run_closure
+        res = run_closure()
+        res.pop("ke_spectra", None)
+        closure = res
+
     if rank != 0:
         g.cleanup()
         if ws > 1:
@@ -366,7 +376,7 @@ def ours_arm(args):
                        "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
                        "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects(),
                        "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the seeded IC"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "ensemble": ensemble, "gpu_launches": launches,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "ensemble": ensemble, "closure": closure, "gpu_launches": launches,
             "clocks": clk, "kernels": kernels}
     print(json.dumps(line), flush=True)
     g.cleanup()

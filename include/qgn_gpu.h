@@ -230,6 +230,52 @@ int qgn_ens_stream(qgn_ens* ens, void** stream);
 const char* qgn_ens_last_error(qgn_ens* ens);
 int qgn_ens_destroy(qgn_ens* ens);
 
+/*
+ * ---- Learned subgrid closure ------------------------------------------------------------
+ * No counterpart in the reference.  A network of `layers` periodic 3x3 convolutions (GELU
+ * between them) maps `cin` input channels to `cout` output channels on an H x W grid (W a
+ * multiple of 128, width 64 channels), on the BF16 tensor cores with FP32 accumulation.
+ * Tensors are NHWC in device memory: inputs BF16 with cin padded to a multiple of 16
+ * (qgn_cnn_padded_channels), outputs and targets FP32 with cout padded the same way.
+ * Weights (get/set, gradients): per layer FP32 [9][cout_p][cin_p] (tap = 3*(dy+1)+(dx+1))
+ * followed by the bias [cout_p]; qgn_cnn_num_params floats in all.
+ */
+typedef struct qgn_cnn qgn_cnn;
+int qgn_cnn_create(int cin, int width, int cout, int layers, int H, int W, int max_batch,
+                   unsigned long long seed, qgn_cnn** out);
+int qgn_cnn_padded_channels(const qgn_cnn* net, int* cin_padded, int* cout_padded);
+long long qgn_cnn_num_params(const qgn_cnn* net);
+int qgn_cnn_get_weights(qgn_cnn* net, float* host);
+int qgn_cnn_set_weights(qgn_cnn* net, const float* host);   /* also resets the Adam moments */
+int qgn_cnn_forward(qgn_cnn* net, const void* x, float* y, int batch, void* stream);
+/* MSE loss over the real output channels and its gradient at the current weights */
+int qgn_cnn_gradients(qgn_cnn* net, const void* x, const float* y, int batch, float* grads_host,
+                      double* loss);
+/* one Adam step (lr; beta 0.9/0.999, eps 1e-8) on samples idx[0..batch) (device int32) of a
+ * dataset x_all [n][H][W][cin_p] BF16, y_all [n][H][W][cout_p] FP32; loss before the update */
+int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, const int* idx, int batch,
+                       float lr, double* loss);
+int qgn_cnn_stream(qgn_cnn* net, void** stream);
+const char* qgn_cnn_last_error(const qgn_cnn* net);
+int qgn_cnn_destroy(qgn_cnn* net);
+
+/* coarse <- sharp spectral cutoff of fine's state (same nz, Lx, Ly; coarse grid not finer) */
+int qgn_coarse_grain(qgn_ctx* fine, qgn_ctx* coarse);
+/* one training sample on coarse's grid: x = scaled (q, psi) of the coarse-grained state,
+ * y = scaled subgrid tendency trunc(GetRHS_fine(q)) - GetRHS_coarse(trunc(q)); in_scale [2 nz],
+ * out_scale [nz] host; x_dev [ny][nx][cin_p] BF16, y_dev [ny][nx][cout_p] FP32 (device).
+ * Sets coarse's state to the coarse-grained one. */
+int qgn_closure_snapshot(qgn_ctx* fine, qgn_ctx* coarse, const float* in_scale, const float* out_scale,
+                         void* x_dev, float* y_dev, int cin_p, int cout_p);
+/* attach (net != NULL) or detach the closure of an ARK43_QGLeith FP64 context whose grid is the
+ * network's: each step adds the network's tendency to every stage RHS while the energy-budget
+ * check passes (then with A8 = A8_background), else runs plain QG-Leith.  The network must not
+ * be used elsewhere while this context steps. */
+int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const float* out_scale,
+                       double A8_background, double energy_limit);
+/* closure evaluations and fallbacks so far; last_budget[3] = {dE/dt, dZ/dt, E} of the last one */
+int qgn_closure_stats(qgn_ctx* ctx, long long* evaluations, long long* fallbacks, double* last_budget);
+
 /* Message of the last failing call on this context (never NULL). */
 const char* qgn_last_error(const qgn_ctx* ctx);
 

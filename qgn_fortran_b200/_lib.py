@@ -66,6 +66,26 @@ SIGNATURES = {
     "qgn_physical": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_set_state_physical": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
     "qgn_physical_modal": (C.c_int, [_ctxp, _dp, _dp, _dp, _dp]),
+    "qgn_cnn_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong,
+                                 C.POINTER(C.c_void_p)]),
+    "qgn_cnn_padded_channels": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "qgn_cnn_num_params": (C.c_longlong, [C.c_void_p]),
+    "qgn_cnn_get_weights": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "qgn_cnn_set_weights": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "qgn_cnn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "qgn_cnn_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_double)]),
+    "qgn_cnn_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                     C.POINTER(C.c_double)]),
+    "qgn_cnn_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "qgn_cnn_last_error": (C.c_char_p, [C.c_void_p]),
+    "qgn_cnn_destroy": (C.c_int, [C.c_void_p]),
+    "qgn_coarse_grain": (C.c_int, [_ctxp, _ctxp]),
+    "qgn_closure_snapshot": (C.c_int, [_ctxp, _ctxp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_void_p,
+                                       C.c_void_p, C.c_int, C.c_int]),
+    "qgn_closure_attach": (C.c_int, [_ctxp, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_double,
+                                     C.c_double]),
+    "qgn_closure_stats": (C.c_int, [_ctxp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), _dp]),
     "qgn_ens_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "qgn_ens_advance": (C.c_int, [C.c_void_p, C.c_int]),
     "qgn_ens_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -21,6 +21,16 @@ Prof*& current_prof() {
     thread_local Prof* p = nullptr;
     return p;
 }
+
+// forget the recorded step graphs (their prologue changes); the next advance records anew
+void drop_graphs(qgn_ctx* ctx) {
+    for (int w = 0; w < 2; ++w)
+        if (ctx->gexec[w]) {
+            cudaGraphExecDestroy(ctx->gexec[w]);
+            ctx->gexec[w] = nullptr;
+        }
+    ctx->graphs_ready = false;
+}
 }  // namespace qgn
 
 namespace {
@@ -170,8 +180,9 @@ double leith_c12(const qgn_params& p) {
     return x4 * x8;
 }
 
+// a stage right-hand side of the schemes: GetRHS plus the learned closure's tendency if attached
 int rhs_of(qgn_ctx* ctx, const double2* q, const double2* psi, double2* out) {
-    CK(launch_rhs(ctx->g, ctx->b, q, psi, out, drag_on(ctx), ctx->stream));
+    CK(launch_rhs(ctx->g, ctx->b, q, psi, out, drag_on(ctx), ctx->stream, closure_tendency(ctx)));
     return QGN_OK;
 }
 
@@ -218,6 +229,9 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
         CK(launch_rhs32(g, b, f32(b.err), f32(b.psi), f32(b.N[0]), drag_on(ctx), st));
     } else {
         CK(launch_modal(g, b.mc, b.q, b.psi, st));
+        // the learned closure (if attached): S of this step's state and the budget check that
+        // keeps it (background A8) or falls back to the Leith A8L just computed
+        if (ctx->closure) RET(closure_eval(ctx));
         RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
     }
     return QGN_OK;
@@ -535,6 +549,7 @@ void free_all(qgn_ctx* ctx) {
     if (b.phys) cudaFree(b.phys);
     if (b.diag) cudaFree(b.diag);
     if (b.modal_scratch) cudaFree(b.modal_scratch);
+    if (b.snap) cudaFree(b.snap);
     b = Buffers{};
     if (ctx->host_pin) cudaFreeHost(ctx->host_pin);
     ctx->host_pin = nullptr;
@@ -793,7 +808,7 @@ int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
         return QGN_OK;
     }
     CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
-    RET(rhs_of(ctx, b.err, b.psi, b.qnew));
+    CK(launch_rhs(ctx->g, b, b.err, b.psi, b.qnew, drag_on(ctx), ctx->stream));
     RET(download_full(ctx, b.qnew, rhs));
     CK(cudaStreamSynchronize(ctx->stream));
     return QGN_OK;
@@ -995,6 +1010,7 @@ int qgn_destroy(qgn_ctx* ctx) {
     if (!ctx) return QGN_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    closure_free(ctx);
     free_all(ctx);
     delete ctx;
     return QGN_OK;

@@ -1,0 +1,387 @@
+// closure.cu -- the learned subgrid closure of a coarse QGN model and its training data.
+//
+// Training data: the high-resolution model's state is coarse-grained by a sharp spectral
+// cutoff onto the coarse grid's kept modes (qgn_coarse_grain); the subgrid PV tendency is the
+// coarse-grained high-resolution right-hand side minus the coarse model's right-hand side of
+// the coarse-grained state,
+//     S = trunc(GetRHS_fine(q)) - GetRHS_coarse(trunc(q)),
+// in which every linear term cancels and the difference of the Jacobians remains.  A sample
+// is the network input (q, psi of every layer, physical, scaled, BF16) and target (S,
+// physical, scaled, FP32) on the coarse grid.
+//
+// Closure: in the ARK43_QGLeith prologue of a context with an attached network, the network
+// maps the state's physical q, psi to S; S (forward-transformed, dealiased) is added to every
+// stage right-hand side inside the y-forward assembly.  An energy-budget check on the applied
+// tendency, in FP64,
+//     dZ = sum_l H_l/Htot <q_l S_l> <= 0            (the closure removes enstrophy)
+//     dE = -sum_l H_l/Htot <psi_l S_l> <= limit * E / day,  E = -1/2 sum_l H_l/Htot <psi_l q_l>,
+// decides per step: passing, the step uses S with the background hyperviscosity A8_background;
+// failing, S is dropped and the step is plain QG-Leith (ARK43_QGLeith.f90:62-73).
+#include "qgn_internal.cuh"
+#include "cnn.cuh"
+#include "prof.cuh"
+
+#include <cuda_bf16.h>
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace qgn {
+
+struct ClosureStats {
+    long long evaluations;
+    long long fallbacks;
+    double dE, dZ, E;
+    int pass;
+    int pad;
+};
+
+struct Closure {
+    qgn_cnn* net = nullptr;
+    float* scales = nullptr;          // device: in [2 nz], out [nz]
+    __nv_bfloat16* x = nullptr;       // [ny][nx][cin_p]
+    float* y = nullptr;               // [ny][nx][cout_p]
+    double* phys = nullptr;           // 3 physical fields
+    double2* S = nullptr;             // compact closure tendency
+    double* red = nullptr;            // 3 x nblocks partial sums
+    double* flag = nullptr;           // 1 passing, 0 fallback
+    ClosureStats* stats = nullptr;
+    double A8bg = 0.0, elimit = 0.0;
+    int nblocks = 0, cin_p = 0, cout_p = 0;
+};
+
+namespace {
+
+constexpr int kBudgetBlocks = 148;
+
+// sharp spectral cutoff: coarse compact <- fine compact on the coarse grid's kept modes,
+// rescaled for the unnormalised transforms
+__global__ void k_truncate(Geom gf, Geom gc, const double2* __restrict__ src, double2* __restrict__ dst, double scale) {
+    const size_t n = gc.csize();
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(e % gc.nky);
+        const size_t r = e / gc.nky;
+        const int kx = (int)(r % gc.nkx);
+        const int l = (int)(r / gc.nkx);
+        const int jc = gc.jfull(m);
+        const int jf = jc <= gc.ny / 2 ? jc : jc - gc.ny + gf.ny;
+        const int mf = jf < gf.kylo ? jf : jf - gf.kyshift;
+        const double2 v = src[((size_t)l * gf.nkx + kx) * gf.nky + mf];
+        dst[e] = (kx == 0 && m == 0) ? make_double2(0.0, 0.0) : make_double2(v.x * scale, v.y * scale);
+    }
+}
+
+__global__ void k_copy_time(const DevScalars* __restrict__ a, DevScalars* __restrict__ b) {
+    b->t = a->t;
+    b->dt = a->dt;
+    b->halt = 0;
+    b->status = 0;
+    b->nonfinite = 0;
+}
+
+__global__ void k_sub(size_t n, const double2* __restrict__ a, const double2* __restrict__ b, double2* __restrict__ o) {
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        o[e] = make_double2(a[e].x - b[e].x, a[e].y - b[e].y);
+}
+
+// network input x[p][c]: c < nz -> q_c, nz <= c < 2 nz -> psi_{c-nz}, scaled; zeros beyond
+__global__ void k_pack_in(int nz, size_t npix, const double* __restrict__ q, const double* __restrict__ psi,
+                          const float* __restrict__ sc, int cin_p, __nv_bfloat16* __restrict__ x) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
+        __nv_bfloat16* xp = x + p * cin_p;
+        for (int c = 0; c < cin_p; ++c) {
+            float v = 0.f;
+            if (c < nz) v = (float)q[(size_t)c * npix + p] * sc[c];
+            else if (c < 2 * nz) v = (float)psi[(size_t)(c - nz) * npix + p] * sc[c];
+            xp[c] = __float2bfloat16_rn(v);
+        }
+    }
+}
+
+// training target y[p][c] = S_c * out_scale_c (c < nz), zeros beyond
+__global__ void k_pack_out(int nz, size_t npix, const double* __restrict__ s, const float* __restrict__ osc, int cout_p,
+                           float* __restrict__ y) {
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < cout_p; ++c) y[p * cout_p + c] = c < nz ? (float)s[(size_t)c * npix + p] * osc[c] : 0.f;
+}
+
+// network output -> physical S_c = y[p][c] / out_scale_c
+__global__ void k_unpack_out(int nz, size_t npix, const float* __restrict__ y, const float* __restrict__ osc,
+                             int cout_p, double* __restrict__ s) {
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < npix * nz; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e / npix);
+        const size_t p = e % npix;
+        s[e] = (double)y[p * cout_p + c] / (double)osc[c];
+    }
+}
+
+// per-block sums of sum_l w_l {psi S, q S, psi q} over the physical grid
+__global__ void __launch_bounds__(256) k_budget(int nz, size_t npix, const double* __restrict__ q,
+                                                const double* __restrict__ psi, const double* __restrict__ s,
+                                                const double* __restrict__ Hw, double* __restrict__ red) {
+    __shared__ double sm[3][8];
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int l = 0; l < nz; ++l) {
+        const double w = Hw[l];
+        const double* ql = q + (size_t)l * npix;
+        const double* pl = psi + (size_t)l * npix;
+        const double* sl = s + (size_t)l * npix;
+        double al = 0.0, bl = 0.0, cl = 0.0;
+        for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
+            al += pl[p] * sl[p];
+            bl += ql[p] * sl[p];
+            cl += pl[p] * ql[p];
+        }
+        a += w * al;
+        b += w * bl;
+        c += w * cl;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    const int wid = threadIdx.x / 32;
+    if (threadIdx.x % 32 == 0) {
+        sm[0][wid] = a;
+        sm[1][wid] = b;
+        sm[2][wid] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) t += sm[threadIdx.x][i];
+        red[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+__global__ void k_budget_decide(int nz, int nblocks, double inv_npix, double A8bg, double elimit,
+                                const double* __restrict__ red, DevScalars* __restrict__ sc,
+                                ClosureStats* __restrict__ st, double* __restrict__ flag) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = 0; i < nblocks; ++i) {
+        a += red[i];
+        b += red[nblocks + i];
+        c += red[2 * nblocks + i];
+    }
+    const double dE = -a * inv_npix, dZ = b * inv_npix, E = -0.5 * c * inv_npix;
+    const bool pass = (dZ <= 0.0) && (dE <= elimit * E / 86400.0) && (dE == dE) && (dZ == dZ);
+    st->evaluations += 1;
+    st->fallbacks += pass ? 0 : 1;
+    st->dE = dE;
+    st->dZ = dZ;
+    st->E = E;
+    st->pass = pass ? 1 : 0;
+    *flag = pass ? 1.0 : 0.0;
+    if (pass)
+        for (int l = 0; l < nz; ++l) sc->A8L[l] = A8bg;
+}
+
+__global__ void k_keep_if_passed(size_t n, const double* __restrict__ flag, double2* __restrict__ s) {
+    const double f = *flag;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        s[e] = f != 0.0 ? s[e] : make_double2(0.0, 0.0);   // a dropped tendency is exactly zero
+}
+
+int grid_of(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+cudaError_t coarse_grain_on(const qgn_ctx* fine, qgn_ctx* coarse, const double2* src, double2* dst, cudaStream_t s) {
+    const double scale = ((double)coarse->g.nx * coarse->g.ny) / ((double)fine->g.nx * fine->g.ny);
+    QGN_LAUNCH(KID_LAYOUT, 32.0 * (double)coarse->g.csize(), s,
+               k_truncate<<<grid_of(coarse->g.csize()), 256, 0, s>>>(fine->g, coarse->g, src, dst, scale));
+    return cudaGetLastError();
+}
+
+bool compatible(const qgn_ctx* f, const qgn_ctx* c) {
+    return f->g.nz == c->g.nz && c->g.nx <= f->g.nx && c->g.ny <= f->g.ny && f->p.Lx == c->p.Lx && f->p.Ly == c->p.Ly;
+}
+
+}  // namespace
+
+// the closure's tendency (compact) for the stage right-hand sides, or NULL
+const double2* closure_tendency(const qgn_ctx* ctx) { return ctx->closure ? ctx->closure->S : nullptr; }
+
+// evaluate the network on the state (b.q, with b.psi = GetPsi(b.q)) and run the budget check
+int closure_eval(qgn_ctx* ctx) {
+    Closure* c = ctx->closure;
+    const Geom& g = ctx->g;
+    const Buffers& b = ctx->b;
+    cudaStream_t st = ctx->stream;
+    const size_t npix = (size_t)g.nx * g.ny, np = npix * g.nz;
+    double* P0 = c->phys;
+    double* P1 = P0 + np;
+    double* P2 = P1 + np;
+    if (launch_to_phys(g, b, b.q, P0, st) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_to_phys(g, b, b.psi, P1, st) != cudaSuccess) return QGN_ERR_CUDA;
+    QGN_LAUNCH(KID_LAYOUT, 16.0 * np + 2.0 * npix * c->cin_p, st,
+               k_pack_in<<<grid_of(npix), 256, 0, st>>>(g.nz, npix, P0, P1, c->scales, c->cin_p, c->x));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    if (cnn::infer(c->net, c->x, c->y, 1, st) != QGN_OK) return QGN_ERR_CUDA;
+    QGN_LAUNCH(KID_LAYOUT, 4.0 * npix * c->cout_p + 8.0 * np, st,
+               k_unpack_out<<<grid_of(np), 256, 0, st>>>(g.nz, npix, c->y, c->scales + 2 * g.nz, c->cout_p, P2));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_from_phys(g, b, P2, c->S, st) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_to_phys(g, b, c->S, P2, st) != cudaSuccess) return QGN_ERR_CUDA;   // the applied (dealiased) S
+    QGN_LAUNCH(KID_PARSEVAL, 24.0 * np, st,
+               k_budget<<<c->nblocks, 256, 0, st>>>(g.nz, npix, P0, P1, P2, b.Hw, c->red));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    QGN_LAUNCH(KID_SCALAR, 0.0, st,
+               k_budget_decide<<<1, 1, 0, st>>>(g.nz, c->nblocks, 1.0 / (double)npix, c->A8bg, c->elimit, c->red, b.sc,
+                                                 c->stats, c->flag));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    QGN_LAUNCH(KID_LAYOUT, 32.0 * g.csize(), st,
+               k_keep_if_passed<<<grid_of(g.csize()), 256, 0, st>>>(g.csize(), c->flag, c->S));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    return QGN_OK;
+}
+
+void closure_free(qgn_ctx* ctx) {
+    Closure* c = ctx->closure;
+    if (!c) return;
+    cudaFree(c->scales);
+    cudaFree(c->x);
+    cudaFree(c->y);
+    cudaFree(c->phys);
+    cudaFree(c->S);
+    cudaFree(c->red);
+    cudaFree(c->flag);
+    cudaFree(c->stats);
+    delete c;
+    ctx->closure = nullptr;
+}
+
+}  // namespace qgn
+
+using namespace qgn;
+
+namespace {
+
+int snap_scratch(qgn_ctx* c, double** out) {
+    const size_t np = (size_t)c->g.nx * c->g.ny * c->g.nz;
+    if (!c->b.snap) {
+        if (cudaMalloc((void**)&c->b.snap, sizeof(double) * (3 * np + 64)) != cudaSuccess) return QGN_ERR_CUDA;
+    }
+    *out = c->b.snap;
+    return QGN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qgn_coarse_grain(qgn_ctx* fine, qgn_ctx* coarse) {
+    if (!fine || !coarse || fine == coarse) return QGN_ERR_ARG;
+    if (!compatible(fine, coarse)) return QGN_ERR_CONFIG;
+    if (cudaSetDevice(fine->device) != cudaSuccess) return QGN_ERR_CUDA;
+    if (cudaStreamSynchronize(coarse->stream) != cudaSuccess) return QGN_ERR_CUDA;
+    cudaStream_t s = fine->stream;
+    if (coarse_grain_on(fine, coarse, fine->b.q, coarse->b.q, s) != cudaSuccess) return QGN_ERR_CUDA;
+    k_copy_time<<<1, 1, 0, s>>>(fine->b.sc, coarse->b.sc);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return QGN_ERR_CUDA;
+    coarse->b.Qs[0] = coarse->b.q;
+    coarse->halted = false;
+    ++coarse->state_version;
+    return QGN_OK;
+}
+
+int qgn_closure_snapshot(qgn_ctx* fine, qgn_ctx* coarse, const float* in_scale, const float* out_scale, void* x_dev,
+                         float* y_dev, int cin_p, int cout_p) {
+    if (!fine || !coarse || !in_scale || !out_scale || !x_dev || !y_dev) return QGN_ERR_ARG;
+    const int nz = coarse->g.nz;
+    if (cin_p < 2 * nz || cin_p % 16 || cout_p < nz || cout_p % 16) return QGN_ERR_CONFIG;
+    int rc = qgn_coarse_grain(fine, coarse);
+    if (rc != QGN_OK) return rc;
+    double* P0 = nullptr;
+    if ((rc = snap_scratch(coarse, &P0)) != QGN_OK) return rc;
+    const Geom& gf = fine->g;
+    const Geom& gc = coarse->g;
+    const Buffers& bf = fine->b;
+    const Buffers& bc = coarse->b;
+    cudaStream_t s = fine->stream;
+    const size_t npix = (size_t)gc.nx * gc.ny, np = npix * nz;
+    double* P1 = P0 + np;
+    double* P2 = P1 + np;
+    float* sc = reinterpret_cast<float*>(P2 + np);
+    if (cudaMemcpyAsync(sc, in_scale, sizeof(float) * 2 * nz, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(sc + 2 * nz, out_scale, sizeof(float) * nz, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return QGN_ERR_CUDA;
+    // high-resolution GetRHS (no hyperviscosity for implicit schemes: is_explicit as configured)
+    if (launch_modal(gf, bf.mc, bf.q, bf.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_rhs(gf, bf, bf.q, bf.psi, bf.N[5], fine->p.C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (coarse_grain_on(fine, coarse, bf.N[5], bc.N[4], s) != cudaSuccess) return QGN_ERR_CUDA;
+    // coarse GetRHS of the coarse-grained state
+    if (launch_modal(gc, bc.mc, bc.q, bc.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_rhs(gc, bc, bc.q, bc.psi, bc.N[5], coarse->p.C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
+    k_sub<<<grid_of(gc.csize()), 256, 0, s>>>(gc.csize(), bc.N[4], bc.N[5], bc.err);
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_to_phys(gc, bc, bc.q, P0, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_to_phys(gc, bc, bc.psi, P1, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_to_phys(gc, bc, bc.err, P2, s) != cudaSuccess) return QGN_ERR_CUDA;
+    k_pack_in<<<grid_of(npix), 256, 0, s>>>(nz, npix, P0, P1, sc, cin_p, static_cast<__nv_bfloat16*>(x_dev));
+    k_pack_out<<<grid_of(npix), 256, 0, s>>>(nz, npix, P2, sc + 2 * nz, cout_p, y_dev);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return QGN_ERR_CUDA;
+    return QGN_OK;
+}
+
+int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const float* out_scale, double A8_background,
+                       double energy_limit) {
+    if (!ctx) return QGN_ERR_ARG;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return QGN_ERR_CUDA;
+    cudaStreamSynchronize(ctx->stream);
+    closure_free(ctx);
+    drop_graphs(ctx);
+    if (!net) return QGN_OK;
+    if (!in_scale || !out_scale) return QGN_ERR_ARG;
+    if (ctx->scheme != QGN_SCHEME_ARK43_QGLEITH || ctx->precision != QGN_PREC_FP64) return QGN_ERR_CONFIG;
+    const Geom& g = ctx->g;
+    if (cnn::height(net) != g.ny || cnn::width(net) != g.nx || cnn::padded_in(net) < 2 * g.nz ||
+        cnn::real_out(net) != g.nz)
+        return QGN_ERR_CONFIG;
+    Closure* c = new (std::nothrow) Closure();
+    if (!c) return QGN_ERR_CUDA;
+    ctx->closure = c;
+    c->net = net;
+    c->A8bg = A8_background;
+    c->elimit = energy_limit;
+    c->cin_p = cnn::padded_in(net);
+    c->cout_p = cnn::padded_out(net);
+    c->nblocks = kBudgetBlocks;
+    const size_t npix = (size_t)g.nx * g.ny, np = npix * g.nz;
+    bool ok = cudaMalloc((void**)&c->scales, sizeof(float) * 3 * g.nz) == cudaSuccess &&
+              cudaMalloc((void**)&c->x, sizeof(__nv_bfloat16) * npix * c->cin_p) == cudaSuccess &&
+              cudaMalloc((void**)&c->y, sizeof(float) * npix * c->cout_p) == cudaSuccess &&
+              cudaMalloc((void**)&c->phys, sizeof(double) * 3 * np) == cudaSuccess &&
+              cudaMalloc((void**)&c->S, sizeof(double2) * g.csize()) == cudaSuccess &&
+              cudaMalloc((void**)&c->red, sizeof(double) * 3 * c->nblocks) == cudaSuccess &&
+              cudaMalloc((void**)&c->flag, sizeof(double)) == cudaSuccess &&
+              cudaMalloc((void**)&c->stats, sizeof(ClosureStats)) == cudaSuccess;
+    ok = ok && cudaMemcpy(c->scales, in_scale, sizeof(float) * 2 * g.nz, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(c->scales + 2 * g.nz, out_scale, sizeof(float) * g.nz, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(c->stats, 0, sizeof(ClosureStats)) == cudaSuccess &&
+         cudaMemset(c->S, 0, sizeof(double2) * g.csize()) == cudaSuccess;
+    if (!ok) {
+        closure_free(ctx);
+        return QGN_ERR_CUDA;
+    }
+    return QGN_OK;
+}
+
+int qgn_closure_stats(qgn_ctx* ctx, long long* evaluations, long long* fallbacks, double* last_budget) {
+    if (!ctx) return QGN_ERR_ARG;
+    if (!ctx->closure) return QGN_ERR_CONFIG;
+    ClosureStats s;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess ||
+        cudaMemcpy(&s, ctx->closure->stats, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return QGN_ERR_CUDA;
+    if (evaluations) *evaluations = s.evaluations;
+    if (fallbacks) *fallbacks = s.fallbacks;
+    if (last_budget) {
+        last_budget[0] = s.dE;
+        last_budget[1] = s.dZ;
+        last_budget[2] = s.E;
+    }
+    return QGN_OK;
+}
+
+}  // extern "C"

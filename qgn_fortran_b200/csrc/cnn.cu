@@ -1,0 +1,769 @@
+// cnn.cu -- the learned subgrid closure's convolutional network on the tensor cores.
+//
+// Network: L periodic 3x3 convolutions (stride 1, "same" with periodic wrap, as the doubly
+// periodic QG domain), GELU after every layer but the last.  Activations are NHWC BF16 with
+// the channel count padded to a multiple of 16; weights are FP32 masters with BF16 copies in
+// two layouts (forward: [tap][cout][cin], backward-data: [tap'][cin][cout] with the taps
+// mirrored); products run on the BF16 tensor cores (mma.m16n8k16) with FP32 accumulation.
+//
+// Kernels (one CTA = 8 warps = 128 consecutive pixels of one image row, persistent over rows):
+//   k_conv<CIN,COUT,EPI>  implicit GEMM  out[p, n] = sum_{tap, k} in[p + tap, k] w[tap, n, k]
+//                         EPI_GELU:      Z = acc + bias (FP32), A = bf16(GELU(Z))
+//                         EPI_LINEAR:    Y = acc + bias (FP32)
+//                         EPI_GELU_GRAD: G = bf16(acc * GELU'(Z))   (backward through a layer)
+//   k_wgrad<CIN,COUT>     dW[tap, n, k] partials = sum_p G[p, n] in[p + tap, k] per row chunk
+//   k_reduce_*            deterministic chunk sums of dW and the bias gradient
+//   k_mse                 loss and dL/dY = 2 (Y - T)/count, as BF16 G of the last layer
+//   k_adam                Adam on the FP32 masters, refreshing both BF16 layouts
+#include "qgn_internal.cuh"
+#include "cnn.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace qgn {
+namespace cnn {
+
+constexpr int kTileP = 128;          // pixels per CTA tile (one row segment)
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kWChunkRows = 16;      // image rows per weight-gradient partial
+
+enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELU_GRAD = 2 };
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr));
+}
+
+// D += A(16x16, row) * B(16x8, col), BF16 in, FP32 accumulate
+__device__ __forceinline__ void mma_bf16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int C>
+struct RowPad {
+    static constexpr int LD = C + 8;   // bf16 elements per pixel in shared memory (16-byte skew)
+};
+
+// copy pixels [w0-1, w0+128] (periodic) of image row (b, h) into smem rows of LD elements
+template <int C>
+__device__ __forceinline__ void load_row(const __nv_bfloat16* __restrict__ src, int b, int h, int H, int W, int w0,
+                                         int halo, __nv_bfloat16* dst) {
+    constexpr int V = C / 8;   // 16-byte vectors per pixel
+    const int npix = kTileP + 2 * halo;
+    const size_t rowbase = ((size_t)b * H + h) * W;
+    for (int i = threadIdx.x; i < npix * V; i += kThreads) {
+        const int px = i / V, v = i % V;
+        int w = w0 - halo + px;
+        w = (w % W + W) % W;
+        const uint4 val = *reinterpret_cast<const uint4*>(src + (rowbase + w) * C + v * 8);
+        *reinterpret_cast<uint4*>(dst + px * RowPad<C>::LD + v * 8) = val;
+    }
+}
+
+// ---- implicit-GEMM periodic 3x3 convolution -------------------------------------------------
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_conv(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
+           int B, int H, int W, float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
+           const float* __restrict__ zin) {
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0, "channel counts are padded to 16");
+    constexpr int LDI = RowPad<CIN>::LD;
+    constexpr int NT = COUT / 8;       // n-tiles of 8 output channels per warp
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smraw);           // [9][COUT][LDI]
+    __nv_bfloat16* xs = ws + 9 * COUT * LDI;                                 // [3][130][LDI]
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    // weights once per CTA
+    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += kThreads) {
+        const int row = i / (CIN / 8), v = i % (CIN / 8);
+        *reinterpret_cast<uint4*>(ws + row * LDI + v * 8) = *reinterpret_cast<const uint4*>(wt + (size_t)row * CIN + v * 8);
+    }
+    const int segs = W / kTileP;
+    const int ntiles = B * H * segs;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int seg = tile % segs;
+        const int h = (tile / segs) % H;
+        const int b = tile / (segs * H);
+        const int w0 = seg * kTileP;
+        __syncthreads();   // previous tile's readers of xs are done (and the weights are in)
+        for (int r = 0; r < 3; ++r)
+            load_row<CIN>(x, b, (h + r - 1 + H) % H, H, W, w0, 1, xs + r * (kTileP + 2) * LDI);
+        __syncthreads();
+        float acc[NT][4];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+        const int pbase = warp * 16;
+#pragma unroll 1
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dh = tap / 3, dw = tap % 3;      // offsets +1 (halo included)
+            const __nv_bfloat16* xr = xs + dh * (kTileP + 2) * LDI;
+            const __nv_bfloat16* wr = ws + tap * COUT * LDI;
+#pragma unroll
+            for (int kc = 0; kc < CIN / 16; ++kc) {
+                uint32_t a0, a1, a2, a3;
+                {
+                    const int prow = pbase + (lane % 8) + 8 * ((lane / 8) % 2);
+                    const int kcol = kc * 16 + 8 * (lane / 16);
+                    ldsm_x4(smem_u32(xr + (prow + dw) * LDI + kcol), a0, a1, a2, a3);
+                }
+#pragma unroll
+                for (int j = 0; j < NT; j += 2) {
+                    uint32_t b0, b1, b2, b3;
+                    const int n = j * 8 + (lane % 8) + 8 * (lane / 16);
+                    const int kcol = kc * 16 + 8 * ((lane / 8) % 2);
+                    ldsm_x4(smem_u32(wr + n * LDI + kcol), b0, b1, b2, b3);
+                    mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+                    mma_bf16(acc[j + 1], a0, a1, a2, a3, b2, b3);
+                }
+            }
+        }
+        // epilogue: thread holds pixels g, g+8 of the warp's 16 and channels 2t, 2t+1 of each n-tile
+        const int g = lane / 4, t = lane % 4;
+        const size_t prow0 = ((size_t)b * H + h) * W + w0 + pbase;
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const int n = j * 8 + 2 * t;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const size_t p = prow0 + g + 8 * half;
+                float v0 = acc[j][2 * half], v1 = acc[j][2 * half + 1];
+                if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+                    v0 += bias[n];
+                    v1 += bias[n + 1];
+                    *reinterpret_cast<float2*>(outf + p * COUT + n) = make_float2(v0, v1);
+                    if (EPI == EPI_GELU)
+                        *reinterpret_cast<__nv_bfloat162*>(outb + p * COUT + n) =
+                            __floats2bfloat162_rn(gelu(v0), gelu(v1));
+                } else {
+                    const float2 z = *reinterpret_cast<const float2*>(zin + p * COUT + n);
+                    *reinterpret_cast<__nv_bfloat162*>(outb + p * COUT + n) =
+                        __floats2bfloat162_rn(v0 * gelu_grad(z.x), v1 * gelu_grad(z.y));
+                }
+            }
+        }
+    }
+}
+
+// ---- weight gradient: partial[chunk][tap][n][k] = sum over the chunk's pixels of G[p,n] in[p+tap,k]
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_wgrad(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ gr, int B, int H, int W,
+            float* __restrict__ part) {
+    constexpr int LDI = RowPad<CIN>::LD, LDG = RowPad<COUT>::LD;
+    constexpr int MT = CIN / 16, NT = COUT / 8;
+    constexpr int TILES = MT * NT;                  // 16x8 output tiles of dW[tap]
+    constexpr int PERW = (TILES + kWarps - 1) / kWarps;
+    static_assert(TILES % kWarps == 0 || TILES < kWarps, "tiles split evenly over warps");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smraw);    // [130][LDI]
+    __nv_bfloat16* gs = xs + (kTileP + 2) * LDI;                      // [128][LDG]
+    const int tap = blockIdx.y;
+    const int dh = tap / 3 - 1, dw = tap % 3 - 1;
+    const int chunk = blockIdx.x;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int segs = W / kTileP;
+    const int rows_total = B * H;
+    const int r0 = chunk * kWChunkRows, r1 = min(rows_total, r0 + kWChunkRows);
+    float acc[PERW][4];
+#pragma unroll
+    for (int i = 0; i < PERW; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    for (int row = r0; row < r1; ++row) {
+        const int b = row / H, h = row % H;
+        for (int seg = 0; seg < segs; ++seg) {
+            const int w0 = seg * kTileP;
+            __syncthreads();
+            load_row<CIN>(x, b, (h + dh + H) % H, H, W, w0, 1, xs);
+            load_row<COUT>(gr, b, h, H, W, w0, 0, gs);
+            __syncthreads();
+#pragma unroll 1
+            for (int kp = 0; kp < kTileP / 16; ++kp) {
+#pragma unroll
+                for (int i = 0; i < PERW; ++i) {
+                    const int tt = warp * PERW + i;
+                    if (tt >= TILES) break;
+                    const int mt = tt / NT, nt = tt % NT;
+                    uint32_t a0, a1, a2, a3, b0, b1, b2, b3;
+                    {
+                        // A = in^T (rows k = input channel, cols = pixel): transposed 8x8 loads
+                        const int mj = lane / 8, r = lane % 8;
+                        const int p = kp * 16 + r + 8 * (mj / 2) + 1 + dw;     // +1: halo offset
+                        const int k = mt * 16 + 8 * (mj % 2);
+                        ldsm_x4_t(smem_u32(xs + p * LDI + k), a0, a1, a2, a3);
+                    }
+                    {
+                        // B = G (rows = pixel, cols n): b0 = pixels 0-7, b1 = pixels 8-15 (transposed)
+                        const int mj = lane / 8, r = lane % 8;
+                        const int p = kp * 16 + r + 8 * (mj % 2);
+                        const int n = (nt & ~1) * 8 + 8 * (mj / 2);
+                        ldsm_x4_t(smem_u32(gs + p * LDG + n), b0, b1, b2, b3);
+                    }
+                    if (nt % 2 == 0) mma_bf16(acc[i], a0, a1, a2, a3, b0, b1);
+                    else mma_bf16(acc[i], a0, a1, a2, a3, b2, b3);
+                }
+            }
+        }
+    }
+    // acc[i]: rows k = mt*16 + g (+8), cols n = nt*8 + 2t (+1)
+    const int g = lane / 4, t = lane % 4;
+    float* out = part + ((size_t)chunk * 9 + tap) * COUT * CIN;
+#pragma unroll
+    for (int i = 0; i < PERW; ++i) {
+        const int tt = warp * PERW + i;
+        if (tt >= TILES) break;
+        const int mt = tt / NT, nt = tt % NT;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int k = mt * 16 + g + 8 * half;
+            const int n = nt * 8 + 2 * t;
+            out[(size_t)n * CIN + k] = acc[i][2 * half];
+            out[(size_t)(n + 1) * CIN + k] = acc[i][2 * half + 1];
+        }
+    }
+}
+
+__global__ void k_reduce_wgrad(const float* __restrict__ part, int nchunks, int n, float* __restrict__ dw) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int c = 0; c < nchunks; ++c) s += part[(size_t)c * n + i];
+        dw[i] = s;
+    }
+}
+
+// bias gradient: per-block column sums of G, then a chunk reduction
+__global__ void k_bias_part(const __nv_bfloat16* __restrict__ gr, long long npix, int C, int pix_per_block,
+                            float* __restrict__ part) {
+    const long long p0 = (long long)blockIdx.x * pix_per_block;
+    const long long p1 = min(npix, p0 + pix_per_block);
+    for (int c = threadIdx.x; c < C; c += blockDim.x) {
+        float s = 0.f;
+        for (long long p = p0; p < p1; ++p) s += __bfloat162float(gr[p * C + c]);
+        part[(size_t)blockIdx.x * C + c] = s;
+    }
+}
+
+// MSE over the real output channels; G = bf16(2 (Y - T) / count), zero in padded channels
+__global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tgt, long long npix, int C, int creal,
+                      double inv_count, __nv_bfloat16* __restrict__ g, double* __restrict__ loss_part) {
+    __shared__ double red[kThreads / 32];
+    double s = 0.0;
+    const long long n = npix * C;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        float gv = 0.f;
+        if (c < creal) {
+            const float d = y[i] - tgt[i];
+            s += (double)d * (double)d;
+            gv = (float)(2.0 * inv_count) * d;
+        }
+        g[i] = __float2bfloat16_rn(gv);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) tot += red[i];
+        loss_part[blockIdx.x] = tot * inv_count;
+    }
+}
+
+// Adam (bias-corrected) on FP32 masters [9][cout][cin]; refreshes the forward ([tap][cout][cin])
+// and backward-data ([8-tap][cin][cout]) BF16 copies
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, int n, int cout, int cin, float lr, float b1, float b2, float eps,
+                       float c1, float c2, __nv_bfloat16* __restrict__ wf, __nv_bfloat16* __restrict__ wb) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        if (wf) {
+            const int tap = i / (cout * cin), r = i % (cout * cin);
+            const int co = r / cin, ci = r % cin;
+            const __nv_bfloat16 bv = __float2bfloat16_rn(wi);
+            wf[i] = bv;
+            wb[((size_t)(8 - tap) * cin + ci) * cout + co] = bv;
+        }
+    }
+}
+
+__global__ void k_adam_bias(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ g, int n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_weights_bf16(const float* __restrict__ w, int n, int cout, int cin, __nv_bfloat16* __restrict__ wf,
+                               __nv_bfloat16* __restrict__ wb) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int tap = i / (cout * cin), r = i % (cout * cin);
+        const int co = r / cin, ci = r % cin;
+        const __nv_bfloat16 bv = __float2bfloat16_rn(w[i]);
+        wf[i] = bv;
+        wb[((size_t)(8 - tap) * cin + ci) * cout + co] = bv;
+    }
+}
+
+// gather batch samples: dst[b] = src[idx[b]] (rows of `bytes` bytes, 16-byte multiples)
+__global__ void k_gather(const unsigned char* __restrict__ src, const int* __restrict__ idx, int nb, size_t bytes,
+                         unsigned char* __restrict__ dst) {
+    const size_t vec = bytes / 16;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vec * nb; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = i / vec, o = i % vec;
+        reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src + (size_t)idx[b] * bytes)[o];
+    }
+}
+
+template <int CIN, int COUT>
+constexpr int conv_smem() {
+    return (9 * COUT + 3 * (kTileP + 2)) * RowPad<CIN>::LD * 2;
+}
+template <int CIN, int COUT>
+constexpr int wgrad_smem() {
+    return ((kTileP + 2) * RowPad<CIN>::LD + kTileP * RowPad<COUT>::LD) * 2;
+}
+
+}  // namespace cnn
+}  // namespace qgn
+
+using namespace qgn;
+using namespace qgn::cnn;
+
+struct qgn_cnn {
+    int cin = 0, width = 0, cout = 0, layers = 0;   // real channel counts
+    int H = 0, W = 0, max_batch = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<int> ci, co;                         // padded channel counts per layer
+    std::vector<float*> w, bias, mw, vw, mb, vb, gw, gb;
+    std::vector<__nv_bfloat16*> wf, wb;
+    std::vector<float*> z;                           // pre-activations (FP32) per layer
+    std::vector<__nv_bfloat16*> act;                 // act[0] = input batch, act[l+1] = GELU(z[l])
+    __nv_bfloat16* gA = nullptr;                     // backward: G of the current layer
+    __nv_bfloat16* gB = nullptr;
+    float* part = nullptr;                           // weight-gradient partials
+    size_t part_elems = 0;
+    double* loss_part = nullptr;
+    double* loss_host = nullptr;
+    float* ytgt = nullptr;                           // gathered targets
+    long long adam_t = 0;
+    std::vector<void*> owned;
+    std::string last_error;
+};
+
+namespace {
+
+int cnn_err(qgn_cnn* n, int code, const std::string& m) {
+    if (n) n->last_error = m;
+    return code;
+}
+
+#define NCK(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t _e = (call);                                                                       \
+        if (_e != cudaSuccess) return cnn_err(net, QGN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+int pad16(int c) { return (c + 15) / 16 * 16; }
+
+template <class T>
+cudaError_t nalloc(qgn_cnn* net, T** p, size_t count) {
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+    if (e == cudaSuccess) {
+        net->owned.push_back(*p);
+        cudaMemsetAsync(*p, 0, sizeof(T) * (count ? count : 1), net->stream);
+    }
+    return e;
+}
+
+size_t npix(const qgn_cnn* n, int batch) { return (size_t)batch * n->H * n->W; }
+
+int conv_grid(const qgn_cnn* n, int batch) {
+    const int tiles = batch * n->H * (n->W / kTileP);
+    return std::max(1, std::min(tiles, 148));
+}
+
+template <int CIN, int COUT, int EPI>
+cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat16* wt, const float* bias, int batch,
+                          float* outf, __nv_bfloat16* outb, const float* zin) {
+    constexpr int SM = conv_smem<CIN, COUT>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_conv<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    k_conv<CIN, COUT, EPI><<<conv_grid(n, batch), kThreads, SM, n->stream>>>(x, wt, bias, batch, n->H, n->W, outf,
+                                                                             outb, zin);
+    return cudaGetLastError();
+}
+
+template <int EPI>
+cudaError_t launch_conv(qgn_cnn* n, int cin, int cout, const __nv_bfloat16* x, const __nv_bfloat16* wt,
+                        const float* bias, int batch, float* outf, __nv_bfloat16* outb, const float* zin) {
+    if (cin == 16 && cout == 64) return launch_conv_t<16, 64, EPI>(n, x, wt, bias, batch, outf, outb, zin);
+    if (cin == 64 && cout == 64) return launch_conv_t<64, 64, EPI>(n, x, wt, bias, batch, outf, outb, zin);
+    if (cin == 64 && cout == 16) return launch_conv_t<64, 16, EPI>(n, x, wt, bias, batch, outf, outb, zin);
+    if (cin == 16 && cout == 16) return launch_conv_t<16, 16, EPI>(n, x, wt, bias, batch, outf, outb, zin);
+    return cudaErrorInvalidValue;
+}
+
+template <int CIN, int COUT>
+cudaError_t launch_wgrad_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat16* g, int batch, float* part,
+                           int* nchunks) {
+    constexpr int SM = wgrad_smem<CIN, COUT>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int chunks = (batch * n->H + kWChunkRows - 1) / kWChunkRows;
+    *nchunks = chunks;
+    k_wgrad<CIN, COUT><<<dim3(chunks, 9), kThreads, SM, n->stream>>>(x, g, batch, n->H, n->W, part);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad(qgn_cnn* n, int cin, int cout, const __nv_bfloat16* x, const __nv_bfloat16* g, int batch,
+                         float* part, int* nchunks) {
+    if (cin == 16 && cout == 64) return launch_wgrad_t<16, 64>(n, x, g, batch, part, nchunks);
+    if (cin == 64 && cout == 64) return launch_wgrad_t<64, 64>(n, x, g, batch, part, nchunks);
+    if (cin == 64 && cout == 16) return launch_wgrad_t<64, 16>(n, x, g, batch, part, nchunks);
+    if (cin == 16 && cout == 16) return launch_wgrad_t<16, 16>(n, x, g, batch, part, nchunks);
+    return cudaErrorInvalidValue;
+}
+
+// forward of a batch: layer 0 reads x0 (default act[0]); the last layer's FP32 output goes
+// to ylast (default z[L-1])
+int forward(qgn_cnn* net, int batch, const __nv_bfloat16* x0 = nullptr, float* ylast = nullptr) {
+    const int L = net->layers;
+    for (int l = 0; l < L; ++l) {
+        const bool last = l == L - 1;
+        const __nv_bfloat16* in = (l == 0 && x0) ? x0 : net->act[l];
+        cudaError_t e = last ? launch_conv<EPI_LINEAR>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l],
+                                                       batch, ylast ? ylast : net->z[l], nullptr, nullptr)
+                             : launch_conv<EPI_GELU>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l],
+                                                     batch, net->z[l], net->act[l + 1], nullptr);
+        NCK(e);
+    }
+    return QGN_OK;
+}
+
+// backward from the BF16 output gradient in gA; fills gw/gb of every layer
+int backward(qgn_cnn* net, int batch) {
+    const int L = net->layers;
+    __nv_bfloat16* gcur = net->gA;
+    __nv_bfloat16* gnext = net->gB;
+    const long long np = (long long)npix(net, batch);
+    for (int l = L - 1; l >= 0; --l) {
+        int chunks = 0;
+        NCK(launch_wgrad(net, net->ci[l], net->co[l], net->act[l], gcur, batch, net->part, &chunks));
+        const int nw = 9 * net->co[l] * net->ci[l];
+        k_reduce_wgrad<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->part, chunks, nw, net->gw[l]);
+        NCK(cudaGetLastError());
+        const int ppb = 1024;
+        const int nbp = (int)((np + ppb - 1) / ppb);
+        k_bias_part<<<nbp, 64, 0, net->stream>>>(gcur, np, net->co[l], ppb, net->part);
+        NCK(cudaGetLastError());
+        k_reduce_wgrad<<<1, 64, 0, net->stream>>>(net->part, nbp, net->co[l], net->gb[l]);
+        NCK(cudaGetLastError());
+        if (l > 0) {
+            NCK(launch_conv<EPI_GELU_GRAD>(net, net->co[l], net->ci[l], gcur, net->wb[l], nullptr, batch, nullptr,
+                                           gnext, net->z[l - 1]));
+            std::swap(gcur, gnext);
+        }
+    }
+    return QGN_OK;
+}
+
+int mse(qgn_cnn* net, int batch, const float* tgt) {
+    const int L = net->layers;
+    const long long np = (long long)npix(net, batch);
+    const int C = net->co[L - 1];
+    const double inv = 1.0 / ((double)np * net->cout);
+    k_mse<<<148, kThreads, 0, net->stream>>>(net->z[L - 1], tgt, np, C, net->cout, inv, net->gA, net->loss_part);
+    NCK(cudaGetLastError());
+    return QGN_OK;
+}
+
+int read_loss(qgn_cnn* net, double* loss) {
+    NCK(cudaMemcpyAsync(net->loss_host, net->loss_part, sizeof(double) * 148, cudaMemcpyDeviceToHost, net->stream));
+    NCK(cudaStreamSynchronize(net->stream));
+    double s = 0.0;
+    for (int i = 0; i < 148; ++i) s += net->loss_host[i];
+    if (loss) *loss = s;
+    return QGN_OK;
+}
+
+}  // namespace
+
+namespace qgn {
+namespace cnn {
+int padded_in(const qgn_cnn* net) { return net->ci[0]; }
+int padded_out(const qgn_cnn* net) { return net->co[net->layers - 1]; }
+int height(const qgn_cnn* net) { return net->H; }
+int width(const qgn_cnn* net) { return net->W; }
+int real_out(const qgn_cnn* net) { return net->cout; }
+int infer(qgn_cnn* net, const void* x, float* y, int batch, cudaStream_t stream) {
+    if (batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
+    cudaStream_t own = net->stream;
+    net->stream = stream;
+    const int rc = forward(net, batch, static_cast<const __nv_bfloat16*>(x), y);
+    net->stream = own;
+    return rc;
+}
+}  // namespace cnn
+}  // namespace qgn
+
+extern "C" {
+
+int qgn_cnn_create(int cin, int width, int cout, int layers, int H, int W, int max_batch, unsigned long long seed,
+                   qgn_cnn** out) {
+    if (!out) return QGN_ERR_ARG;
+    *out = nullptr;
+    if (cin < 1 || cin > 16 || cout < 1 || cout > 16 || width != 64 || layers < 2 || layers > 16) return QGN_ERR_CONFIG;
+    if (H < 1 || W < kTileP || W % kTileP != 0 || max_batch < 1) return QGN_ERR_CONFIG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return QGN_ERR_NO_DEVICE;
+    qgn_cnn* net = new (std::nothrow) qgn_cnn();
+    if (!net) return QGN_ERR_CUDA;
+    net->cin = cin;
+    net->width = width;
+    net->cout = cout;
+    net->layers = layers;
+    net->H = H;
+    net->W = W;
+    net->max_batch = max_batch;
+    cudaGetDevice(&net->device);
+    auto fail = [&](int code) {
+        qgn_cnn_destroy(net);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(QGN_ERR_CUDA);
+    for (int l = 0; l < layers; ++l) {
+        net->ci.push_back(l == 0 ? pad16(cin) : width);
+        net->co.push_back(l == layers - 1 ? pad16(cout) : width);
+    }
+    const size_t NP = npix(net, max_batch);
+    net->w.resize(layers); net->bias.resize(layers); net->mw.resize(layers); net->vw.resize(layers);
+    net->mb.resize(layers); net->vb.resize(layers); net->gw.resize(layers); net->gb.resize(layers);
+    net->wf.resize(layers); net->wb.resize(layers); net->z.resize(layers); net->act.resize(layers + 1);
+    size_t part = 0;
+    std::mt19937_64 rng(seed);
+    for (int l = 0; l < layers; ++l) {
+        const int nw = 9 * net->co[l] * net->ci[l];
+        if (nalloc(net, &net->w[l], nw) || nalloc(net, &net->mw[l], nw) || nalloc(net, &net->vw[l], nw) ||
+            nalloc(net, &net->gw[l], nw) || nalloc(net, &net->wf[l], nw) || nalloc(net, &net->wb[l], nw) ||
+            nalloc(net, &net->bias[l], net->co[l]) || nalloc(net, &net->mb[l], net->co[l]) ||
+            nalloc(net, &net->vb[l], net->co[l]) || nalloc(net, &net->gb[l], net->co[l]) ||
+            nalloc(net, &net->z[l], NP * net->co[l]) || nalloc(net, &net->act[l], NP * net->ci[l]))
+            return fail(QGN_ERR_CUDA);
+        // He initialisation over the real fan-in, zeros in padded channels
+        const int real_in = l == 0 ? cin : width, real_out = l == layers - 1 ? cout : width;
+        std::normal_distribution<float> nd(0.f, std::sqrt(2.0f / (9.0f * real_in)) * (l == layers - 1 ? 0.1f : 1.0f));
+        std::vector<float> hw(nw, 0.f);
+        for (int tap = 0; tap < 9; ++tap)
+            for (int o = 0; o < real_out; ++o)
+                for (int i = 0; i < real_in; ++i) hw[((size_t)tap * net->co[l] + o) * net->ci[l] + i] = nd(rng);
+        if (cudaMemcpyAsync(net->w[l], hw.data(), sizeof(float) * nw, cudaMemcpyHostToDevice, net->stream) !=
+            cudaSuccess)
+            return fail(QGN_ERR_CUDA);
+        cudaStreamSynchronize(net->stream);
+        k_weights_bf16<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
+                                                                  net->wb[l]);
+        const size_t chunks = (size_t)((max_batch * H + kWChunkRows - 1) / kWChunkRows);
+        part = std::max(part, chunks * nw);
+        part = std::max(part, ((NP + 1023) / 1024) * (size_t)net->co[l]);
+    }
+    if (nalloc(net, &net->act[layers], 16) || nalloc(net, &net->gA, NP * net->width) ||
+        nalloc(net, &net->gB, NP * net->width) || nalloc(net, &net->part, part) ||
+        nalloc(net, &net->loss_part, 148) || nalloc(net, &net->ytgt, NP * pad16(cout)))
+        return fail(QGN_ERR_CUDA);
+    net->part_elems = part;
+    if (cudaMallocHost((void**)&net->loss_host, sizeof(double) * 148) != cudaSuccess) return fail(QGN_ERR_CUDA);
+    if (cudaStreamSynchronize(net->stream) != cudaSuccess) return fail(QGN_ERR_CUDA);
+    *out = net;
+    return QGN_OK;
+}
+
+int qgn_cnn_padded_channels(const qgn_cnn* net, int* cin_padded, int* cout_padded) {
+    if (!net) return QGN_ERR_ARG;
+    if (cin_padded) *cin_padded = net->ci[0];
+    if (cout_padded) *cout_padded = net->co[net->layers - 1];
+    return QGN_OK;
+}
+
+// weights: per layer [9][cout_p][cin_p] FP32 then bias [cout_p], layers in order
+long long qgn_cnn_num_params(const qgn_cnn* net) {
+    if (!net) return -1;
+    long long n = 0;
+    for (int l = 0; l < net->layers; ++l) n += 9LL * net->co[l] * net->ci[l] + net->co[l];
+    return n;
+}
+
+int qgn_cnn_get_weights(qgn_cnn* net, float* host) {
+    if (!net || !host) return QGN_ERR_ARG;
+    size_t off = 0;
+    for (int l = 0; l < net->layers; ++l) {
+        const size_t nw = 9ull * net->co[l] * net->ci[l];
+        NCK(cudaMemcpyAsync(host + off, net->w[l], sizeof(float) * nw, cudaMemcpyDeviceToHost, net->stream));
+        off += nw;
+        NCK(cudaMemcpyAsync(host + off, net->bias[l], sizeof(float) * net->co[l], cudaMemcpyDeviceToHost, net->stream));
+        off += net->co[l];
+    }
+    NCK(cudaStreamSynchronize(net->stream));
+    return QGN_OK;
+}
+
+int qgn_cnn_set_weights(qgn_cnn* net, const float* host) {
+    if (!net || !host) return QGN_ERR_ARG;
+    size_t off = 0;
+    for (int l = 0; l < net->layers; ++l) {
+        const int nw = 9 * net->co[l] * net->ci[l];
+        NCK(cudaMemcpyAsync(net->w[l], host + off, sizeof(float) * nw, cudaMemcpyHostToDevice, net->stream));
+        off += nw;
+        NCK(cudaMemcpyAsync(net->bias[l], host + off, sizeof(float) * net->co[l], cudaMemcpyHostToDevice, net->stream));
+        off += net->co[l];
+        k_weights_bf16<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
+                                                                  net->wb[l]);
+        NCK(cudaGetLastError());
+    }
+    NCK(cudaStreamSynchronize(net->stream));
+    net->adam_t = 0;
+    for (int l = 0; l < net->layers; ++l) {
+        const int nw = 9 * net->co[l] * net->ci[l];
+        NCK(cudaMemsetAsync(net->mw[l], 0, sizeof(float) * nw, net->stream));
+        NCK(cudaMemsetAsync(net->vw[l], 0, sizeof(float) * nw, net->stream));
+        NCK(cudaMemsetAsync(net->mb[l], 0, sizeof(float) * net->co[l], net->stream));
+        NCK(cudaMemsetAsync(net->vb[l], 0, sizeof(float) * net->co[l], net->stream));
+    }
+    NCK(cudaStreamSynchronize(net->stream));
+    return QGN_OK;
+}
+
+// inference: x = BF16 [batch][H][W][cin_p] (device), y = FP32 [batch][H][W][cout_p] (device).
+// Runs on `stream` (NULL: the network's own stream), ordered after the caller's work there.
+int qgn_cnn_forward(qgn_cnn* net, const void* x, float* y, int batch, void* stream) {
+    if (!net || !x || !y || batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
+    return qgn::cnn::infer(net, x, y, batch, stream ? static_cast<cudaStream_t>(stream) : net->stream);
+}
+
+// gradients of the MSE loss at the current weights for x (BF16 [batch][H][W][cin_p]) and
+// targets y (FP32 [batch][H][W][cout_p]); host output in the get_weights layout
+int qgn_cnn_gradients(qgn_cnn* net, const void* x, const float* y, int batch, float* grads_host, double* loss) {
+    if (!net || !x || !y || batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
+    const size_t xb = npix(net, batch) * net->ci[0] * sizeof(__nv_bfloat16);
+    NCK(cudaMemcpyAsync(net->act[0], x, xb, cudaMemcpyDeviceToDevice, net->stream));
+    int rc = forward(net, batch);
+    if (rc == QGN_OK) rc = mse(net, batch, y);
+    if (rc == QGN_OK) rc = backward(net, batch);
+    if (rc == QGN_OK) rc = read_loss(net, loss);
+    if (rc != QGN_OK) return rc;
+    if (grads_host) {
+        size_t off = 0;
+        for (int l = 0; l < net->layers; ++l) {
+            const size_t nw = 9ull * net->co[l] * net->ci[l];
+            NCK(cudaMemcpyAsync(grads_host + off, net->gw[l], sizeof(float) * nw, cudaMemcpyDeviceToHost, net->stream));
+            off += nw;
+            NCK(cudaMemcpyAsync(grads_host + off, net->gb[l], sizeof(float) * net->co[l], cudaMemcpyDeviceToHost,
+                                net->stream));
+            off += net->co[l];
+        }
+        NCK(cudaStreamSynchronize(net->stream));
+    }
+    return QGN_OK;
+}
+
+// one Adam step on the batch idx[0..batch) (device int32) of a dataset: x_all BF16
+// [n][H][W][cin_p], y_all FP32 [n][H][W][cout_p]; loss (before the update) optional
+int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, const int* idx, int batch, float lr,
+                       double* loss) {
+    if (!net || !x_all || !y_all || !idx || batch < 1 || batch > net->max_batch || !(lr > 0)) return QGN_ERR_ARG;
+    const int L = net->layers;
+    const size_t xs = (size_t)net->H * net->W * net->ci[0] * sizeof(__nv_bfloat16);
+    const size_t ys = (size_t)net->H * net->W * net->co[L - 1] * sizeof(float);
+    k_gather<<<148 * 4, 256, 0, net->stream>>>(static_cast<const unsigned char*>(x_all), idx, batch, xs,
+                                              reinterpret_cast<unsigned char*>(net->act[0]));
+    NCK(cudaGetLastError());
+    k_gather<<<148 * 4, 256, 0, net->stream>>>(reinterpret_cast<const unsigned char*>(y_all), idx, batch, ys,
+                                              reinterpret_cast<unsigned char*>(net->ytgt));
+    NCK(cudaGetLastError());
+    int rc = forward(net, batch);
+    if (rc == QGN_OK) rc = mse(net, batch, net->ytgt);
+    if (rc == QGN_OK) rc = backward(net, batch);
+    if (rc != QGN_OK) return rc;
+    net->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float c1 = 1.f - std::pow(b1, (float)net->adam_t), c2 = 1.f - std::pow(b2, (float)net->adam_t);
+    for (int l = 0; l < L; ++l) {
+        const int nw = 9 * net->co[l] * net->ci[l];
+        k_adam<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], net->mw[l], net->vw[l], net->gw[l], nw, net->co[l],
+                                                          net->ci[l], lr, b1, b2, eps, c1, c2, net->wf[l], net->wb[l]);
+        NCK(cudaGetLastError());
+        k_adam_bias<<<1, 64, 0, net->stream>>>(net->bias[l], net->mb[l], net->vb[l], net->gb[l], net->co[l], lr, b1, b2,
+                                               eps, c1, c2);
+        NCK(cudaGetLastError());
+    }
+    if (loss) return read_loss(net, loss);
+    return QGN_OK;
+}
+
+int qgn_cnn_stream(qgn_cnn* net, void** stream) {
+    if (!net || !stream) return QGN_ERR_ARG;
+    *stream = net->stream;
+    return QGN_OK;
+}
+
+const char* qgn_cnn_last_error(const qgn_cnn* net) { return net ? net->last_error.c_str() : "NULL network"; }
+
+int qgn_cnn_destroy(qgn_cnn* net) {
+    if (!net) return QGN_OK;
+    if (net->stream) cudaStreamSynchronize(net->stream);
+    for (void* p : net->owned) cudaFree(p);
+    if (net->loss_host) cudaFreeHost(net->loss_host);
+    if (net->stream) cudaStreamDestroy(net->stream);
+    delete net;
+    return QGN_OK;
+}
+
+}  // extern "C"

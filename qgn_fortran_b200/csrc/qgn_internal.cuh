@@ -90,12 +90,17 @@ struct Buffers {
     double* Hw = nullptr;        // H(k)/Htot per layer
     double* diag = nullptr;      // diagnostics output (lazy)
     double* modal_scratch = nullptr;  // WriteQPmodal work space (lazy)
+    double* snap = nullptr;           // closure training-sample work space (lazy)
     LayerConst* lc = nullptr;
     ModalConst* mc = nullptr;
     DevScalars* sc = nullptr;
 };
 
 }  // namespace qgn
+
+namespace qgn {
+struct Closure;
+}
 
 struct qgn_ctx {
     qgn_params p{};
@@ -111,6 +116,7 @@ struct qgn_ctx {
     int ab_calls = 0;
     bool halted = false;           // a step failed; cleared by the next state upload
     long long state_version = 0;   // bumped by every call that changes the state outside an ensemble
+    qgn::Closure* closure = nullptr;   // learned closure of a coarse ARK43_QGLeith model (closure.cu)
     double* host_pin = nullptr;    // pinned scalar readback
     std::vector<void*> owned;      // every device allocation made at creation
     std::string last_error;
@@ -127,10 +133,17 @@ struct qgn_ctx {
 
 namespace qgn {
 
+// ---- learned closure (closure.cu) and graph invalidation (capi.cu) -----------------------
+int closure_eval(qgn_ctx* ctx);
+void closure_free(qgn_ctx* ctx);
+const double2* closure_tendency(const qgn_ctx* ctx);
+void drop_graphs(qgn_ctx* ctx);
+
 // ---- launch wrappers (rhs_kernels.cu) -------------------------------------------------
 cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, double2* psi, cudaStream_t s);
+// extra (optional, compact): a tendency added to the RHS on the kept modes (learned closure)
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
-                       bool do_drag, cudaStream_t s);
+                       bool do_drag, cudaStream_t s, const double2* extra = nullptr);
 cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const float2* psi, float2* out, bool do_drag,
                          cudaStream_t s);
 // y-inverse + x-pass of one compact field with a max|.| reduction into sc->maxbits

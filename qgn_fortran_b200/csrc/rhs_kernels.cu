@@ -72,8 +72,8 @@ template <int NY, bool DRAG, class CT>
 __global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT>::THREADS, minb(YFwdCfg<NY, DRAG, CT>::THREADS, regcap<CT>()))
     k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const CT* __restrict__ q,
            const CT* __restrict__ psi, const CT* __restrict__ pp, const CT* __restrict__ pd,
-           CT* __restrict__ out, const CT* __restrict__ twy) {
-    yfwd_tile<NY, DRAG, CT>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy);
+           CT* __restrict__ out, const CT* __restrict__ twy, const CT* __restrict__ extra) {
+    yfwd_tile<NY, DRAG, CT>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy, extra);
 }
 
 template <int NX, int EPI>
@@ -243,7 +243,8 @@ static cudaError_t launch_xpass(const Geom& g, const CT* hq, const CT* hp, const
 
 template <class CT>
 static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q, const CT* psi, const CT* hpp,
-                               const CT* hpd, CT* out, const CT* twy, bool drag, cudaStream_t s) {
+                               const CT* hpd, CT* out, const CT* twy, bool drag, cudaStream_t s,
+                               const CT* extra = nullptr) {
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
         cudaError_t e;
@@ -255,7 +256,8 @@ static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q,
             dim3 grid((g.nkx + C::TKX - 1) / C::TKX, nplain);
             const double lb = es * (double)nplain * g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (2.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, lc, q, psi, hpp, hpd, out, twy));
+                       k_yfwd<NY, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, lc, q, psi, hpp, hpd, out, twy,
+                                                                                 extra));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (drag) {
@@ -265,7 +267,7 @@ static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q,
             const double lb = es * (double)g.nkx;
             QGN_LAUNCH(KID_YFWD, lb * (4.0 * NY + 3.0 * g.nky), s,
                        k_yfwd<NY, true, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, lc, q, psi, hpp, hpd, out,
-                                                                               twy));
+                                                                               twy, extra));
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -273,11 +275,11 @@ static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q,
 }
 
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
-                       bool do_drag, cudaStream_t s) {
+                       bool do_drag, cudaStream_t s, const double2* extra) {
     cudaError_t e;
     if ((e = launch_yinv<double2>(g, 3, q, psi, b.hq, b.hp, b.hu, b.twy, s)) != cudaSuccess) return e;
     if ((e = launch_xpass<double2>(g, b.hq, b.hp, b.hu, b.hpp, b.hpd, b.twx, do_drag, s)) != cudaSuccess) return e;
-    return launch_yfwd<double2>(g, b.lc, q, psi, b.hpp, b.hpd, out, b.twy, do_drag, s);
+    return launch_yfwd<double2>(g, b.lc, q, psi, b.hpp, b.hpd, out, b.twy, do_drag, s, extra);
 }
 
 // FP32 right-hand side of the mixed mode: compact FP32 q, psi in, compact FP32 RHS out; the

@@ -280,7 +280,8 @@ template <int NY, bool DRAG, class CT, int TV = 0>
 __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const LayerConst* __restrict__ lc,
                                           const CT* __restrict__ q, const CT* __restrict__ psi,
                                           const CT* __restrict__ pp, const CT* __restrict__ pd,
-                                          CT* __restrict__ out, const CT* __restrict__ twy) {
+                                          CT* __restrict__ out, const CT* __restrict__ twy,
+                                          const CT* __restrict__ extra = nullptr) {
     using C = YFwdCfg<NY, DRAG, CT, TV>;
     using RT = typename CTraits<CT>::R;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -356,6 +357,10 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
                 const CT d = out[idx];
                 r = cmk<CT>(r.x + d.x, r.y + d.y);
             }
+        }
+        if (extra) {   // an extra tendency on the kept modes (the learned closure's)
+            const CT x = extra[idx];
+            r = cmk<CT>(r.x + x.x, r.y + x.y);
         }
         if (kx == 0 && m == 0) r = cmk<CT>(0.0, 0.0);
         out[idx] = r;

@@ -1,0 +1,226 @@
+"""Learned subgrid closure on the GPU: the tensor-core network against the CPU oracle, the
+training data against the FP64 model oracle, the energy-budget fallback, and what a trained
+closure gains over QG-Leith on held-out data."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.cnn_oracle import CNNOracle, adam_step, bf16
+from oracle.qgn_oracle import Params, QGNOracle
+from qgn_fortran_b200 import QGNModule
+from qgn_fortran_b200 import closure as cl
+from qgn_fortran_b200.inputs import exponential_stratification, seeded_random_pv
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def to_dev_bf16(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(torch.bfloat16).cuda()
+
+
+def to_dev_f32(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def small_net(seed=3, H=8, W=128, layers=3, max_batch=4, nz=2):
+    net = cl.ClosureNet(nz=nz, H=H, W=W, layers=layers, max_batch=max_batch, seed=seed)
+    rng = np.random.default_rng(seed)
+    ws = []
+    for (cop, cip), (w, b) in zip(net.shapes, net.get_weights()):
+        b = 0.1 * rng.standard_normal(cop).astype(np.float32)
+        ws.append((w, b))
+    net.set_weights(ws)
+    return net, net.get_weights()
+
+
+def sample(net, batch, seed):
+    rng = np.random.default_rng(seed)
+    x = np.zeros((batch, net.H, net.W, net.cin_p), np.float32)
+    x[..., :net.cin] = rng.standard_normal((batch, net.H, net.W, net.cin))
+    t = np.zeros((batch, net.H, net.W, net.cout_p), np.float32)
+    t[..., :net.cout] = rng.standard_normal((batch, net.H, net.W, net.cout))
+    return bf16(x), t
+
+
+def test_cnn_forward_matches_oracle(cuda_ok):
+    import torch
+    net, ws = small_net()
+    x, _ = sample(net, 3, 1)
+    y = torch.zeros((3, net.H, net.W, net.cout_p), dtype=torch.float32, device="cuda")
+    net.forward(to_dev_bf16(x), y, 3)
+    torch.cuda.synchronize()
+    ref, _, _ = CNNOracle(ws, net.cout).forward(x)
+    assert rel(y.cpu().numpy(), ref) <= 1e-4
+
+
+def test_cnn_gradients_match_oracle(cuda_ok):
+    net, ws = small_net(seed=5)
+    x, t = sample(net, 2, 2)
+    loss, grads = net.gradients(to_dev_bf16(x), to_dev_f32(t), 2)
+    lref, gref = CNNOracle(ws, net.cout).loss_and_grads(x, t)
+    assert loss == pytest.approx(lref, rel=1e-5)
+    for l, ((gw, gb), (rw, rb)) in enumerate(zip(grads, gref)):
+        assert rel(gw, rw) <= 1e-3, l
+        assert rel(gb, rb) <= 1e-3, l
+
+
+def test_adam_step_matches_oracle(cuda_ok):
+    import torch
+    net, ws = small_net(seed=7)
+    x, t = sample(net, 2, 3)
+    xd, td = to_dev_bf16(x), to_dev_f32(t)
+    _, grads = net.gradients(xd, td, 2)
+    idx = torch.tensor([0, 1], dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    net.train_step(xd, td, idx, 2, 1e-3)
+    after = net.get_weights()
+    for (w0, b0), (gw, gb), (w1, b1) in zip(ws, grads, after):
+        ew, _, _ = adam_step(w0, np.zeros_like(w0), np.zeros_like(w0), gw, 1, 1e-3)
+        eb, _, _ = adam_step(b0, np.zeros_like(b0), np.zeros_like(b0), gb, 1, 1e-3)
+        assert np.allclose(w1, ew, rtol=0, atol=1e-6)
+        assert np.allclose(b1, eb, rtol=0, atol=1e-6)
+
+
+def test_training_fits_a_teacher(cuda_ok):
+    """A student network trained with the project's kernels fits a fixed teacher network."""
+    import torch
+    teacher, tw = small_net(seed=11, H=16, max_batch=64)
+    rng = np.random.default_rng(4)
+    n = 64
+    x = np.zeros((n, 16, 128, teacher.cin_p), np.float32)
+    x[..., :teacher.cin] = rng.standard_normal((n, 16, 128, teacher.cin))
+    x = bf16(x)
+    xd = to_dev_bf16(x)
+    yd = torch.zeros((n, 16, 128, teacher.cout_p), dtype=torch.float32, device="cuda")
+    teacher.forward(xd, yd, n)
+    student = cl.ClosureNet(nz=2, H=16, W=128, layers=3, max_batch=8, seed=99)
+    hist = cl.train(student, xd, yd, iters=1200, batch=8, lr=2e-3, log_every=100)
+    assert hist[-1][1] < 0.2 * hist[0][1], hist
+
+
+# ---- closure data and the coarse model ----------------------------------------------------------
+def strat(nx, nz=2, **kw):
+    p = dict(nx=nx, ny=nx, nz=nz, Lx=2.0e6, Ly=2.0e6, Htot=4000.0, f0=1.0e-4, beta=2.0e-11, A2=0.0,
+             A8=1.0e20 * (1024.0 / nx) ** 8, r0=1.0e-7, C_d=0.0, TOL=4.0e-12, is_explicit=False,
+             dt_max=math.pi / (2.0e-11 * 2.0e6))
+    p.update(kw)
+    return p
+
+
+def truncate(qf, nyc, nxc, nyf, nxf):
+    nxhc = nxc // 2 + 1
+    out = np.zeros((qf.shape[0], nyc, nxhc), dtype=np.complex128)
+    for jc in range(nyc):
+        jf = jc if jc <= nyc // 2 else jc - nyc + nyf
+        out[:, jc, :] = qf[:, jf, :nxhc]
+    return out * (nxc * nyc) / (nxf * nyf)
+
+
+def test_snapshot_matches_model_oracle(cuda_ok):
+    import torch
+    H, S, U = exponential_stratification(2)
+    pf, pc = strat(256), strat(128)
+    fine = QGNModule(pf, H, S, U)
+    coarse = QGNModule(pc, H, S, U)
+    qf = fine.initialize(seeded_random_pv(256, 256, 2, 12.0, 1.0e-6, 21), 0.0, 750.0)
+    isc = np.array([1e5, 2e5, 1e-4, 3e-4], np.float32)
+    osc = np.array([1e11, 3e11], np.float32)
+    x = torch.zeros((128, 128, 16), dtype=torch.bfloat16, device="cuda")
+    y = torch.zeros((128, 128, 16), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    cl.snapshot(fine, coarse, isc, osc, x, y, 16, 16)
+    mf, mc = QGNOracle(Params(**pf), H, S, U), QGNOracle(Params(**pc), H, S, U)
+    qc = mc.dealias(truncate(qf, 128, 128, 256, 256))
+    target = mc.dealias(truncate(mf.get_rhs(qf), 128, 128, 256, 256)) - mc.get_rhs(qc)
+    s_phys = mc.s2g_scaled(target)
+    got = y.cpu().numpy()
+    for l in range(2):
+        assert rel(got[..., l] / osc[l], s_phys[l]) <= 1e-6
+        assert rel(x.float().cpu().numpy()[..., l] / isc[l], mc.s2g_scaled(qc)[l]) <= 5e-3
+        assert rel(x.float().cpu().numpy()[..., 2 + l] / isc[2 + l], mc.s2g_scaled(mc.get_psi(qc))[l]) <= 5e-3
+    assert np.all(got[..., 2:] == 0)
+    # the coarse model now holds the coarse-grained state
+    assert rel(coarse.get_state(), qc) <= 1e-12
+
+
+def coarse_pair(nx=128, seed=31):
+    H, S, U = exponential_stratification(2)
+    p = strat(nx)
+    qp = seeded_random_pv(nx, nx, 2, 10.0, 1.0e-6, seed)
+    a = QGNModule(p, H, S, U)
+    b = QGNModule(p, H, S, U)
+    a.initialize(qp, 0.0, 3000.0)
+    b.initialize(qp, 0.0, 3000.0)
+    return a, b
+
+
+def test_failing_budget_falls_back_to_leith_exactly(cuda_ok):
+    a, b = coarse_pair()
+    net = cl.ClosureNet(nz=2, H=128, W=128, layers=6, max_batch=1, seed=1)
+    cl.attach(a, net, np.ones(4), np.ones(2), A8_background=0.0, energy_limit=-1e300)
+    a.advance_resident(6)
+    b.advance_resident(6)
+    assert np.array_equal(a.get_state(), b.get_state())
+    assert a.time() == b.time()
+    st = cl.stats(a)
+    assert st["evaluations"] == 6 and st["fallbacks"] == 6
+
+
+def test_zero_network_passes_the_budget(cuda_ok):
+    a, _ = coarse_pair()
+    net = cl.ClosureNet(nz=2, H=128, W=128, layers=6, max_batch=1, seed=1)
+    net.set_weights([(np.zeros_like(w), np.zeros_like(b)) for w, b in net.get_weights()])
+    cl.attach(a, net, np.ones(4), np.ones(2), A8_background=a.p["A8"], energy_limit=1.0)
+    a.advance_resident(5)
+    st = cl.stats(a)
+    assert st["evaluations"] == 5 and st["fallbacks"] == 0
+    assert st["dE"] == 0.0 and st["dZ"] == 0.0 and st["E"] > 0
+    assert np.all(np.isfinite(a.get_state()))
+    cl.attach(a, None)
+    a.advance_resident(1)
+
+
+def leith_tendency(m, qhat, A8L):
+    return m.s2g_scaled(-(A8L[:, None, None] * m.k8[None]) * qhat)
+
+
+def test_trained_closure_beats_leith_offline(cuda_ok):
+    """On held-out coarse-grained snapshots, the trained network predicts the subgrid PV
+    tendency far better than QG-Leith's hyperviscous tendency (even optimally rescaled)."""
+    import torch
+    H, S, U = exponential_stratification(2)
+    pf, pc = strat(256), strat(128)
+    fine = QGNModule(pf, H, S, U)
+    fine.initialize(seeded_random_pv(256, 256, 2, 8.0, 1.0e-6, 41), 0.0, 3000.0)
+    fine.advance_resident(300)
+    helper = QGNModule(pc, H, S, U)
+    net = cl.ClosureNet(nz=2, H=128, W=128, layers=6, max_batch=16, seed=2)
+    x, y, isc, osc = cl.make_dataset(fine, helper, n=112, every=3, cin_p=net.cin_p, cout_p=net.cout_p)
+    ntr = 96
+    cl.train(net, x[:ntr], y[:ntr], iters=2500, batch=8, lr=1e-3)
+    pred = torch.zeros((16, 128, 128, net.cout_p), dtype=torch.float32, device="cuda")
+    net.forward(x[ntr:], pred, 16)
+    torch.cuda.synchronize()
+    yt = y[ntr:].cpu().numpy()[..., :2]
+    yp = pred.cpu().numpy()[..., :2]
+    r2_cnn = 1.0 - np.sum((yp - yt) ** 2) / np.sum((yt - yt.mean(axis=(0, 1, 2))) ** 2)
+    # QG-Leith's tendency on the same coarse states, best-fit rescaled
+    mc = QGNOracle(Params(**pc), H, S, U)
+    xq = x[ntr:].float().cpu().numpy()[..., :2] / isc[:2]
+    lt = []
+    for i in range(16):
+        qphys = np.moveaxis(xq[i], -1, 0)
+        qhat = mc.dealias(mc.g2s(qphys))
+        lt.append(np.moveaxis(leith_tendency(mc, qhat, mc.leith_A8L(qhat)), 0, -1) * osc[:2])
+    lt = np.array(lt)
+    alpha = np.sum(lt * yt) / np.sum(lt * lt)
+    r2_leith = 1.0 - np.sum((alpha * lt - yt) ** 2) / np.sum((yt - yt.mean(axis=(0, 1, 2))) ** 2)
+    assert r2_cnn > 0.3, (r2_cnn, r2_leith)
+    assert r2_cnn > r2_leith + 0.1, (r2_cnn, r2_leith)
