@@ -192,21 +192,27 @@ def leith_tendency(m, qhat, A8L):
 
 
 def test_trained_closure_beats_leith_offline(cuda_ok):
-    """On held-out coarse-grained snapshots, the trained network predicts the subgrid PV
-    tendency far better than QG-Leith's hyperviscous tendency (even optimally rescaled)."""
+    """On held-out coarse-grained snapshots taken after the training ones, the trained network
+    predicts the subgrid PV tendency better than QG-Leith's hyperviscous tendency (even
+    optimally rescaled).  The 512^2 truth is spun up for a model year first: during the
+    decay of the initial condition the subgrid statistics drift and nothing learned on
+    earlier samples carries to later ones."""
     import torch
     H, S, U = exponential_stratification(2)
-    pf, pc = strat(256), strat(128)
+    pf, pc = strat(512), strat(128)
     fine = QGNModule(pf, H, S, U)
-    fine.initialize(seeded_random_pv(256, 256, 2, 8.0, 1.0e-6, 41), 0.0, 3000.0)
-    fine.advance_resident(300)
+    fine.initialize(seeded_random_pv(512, 512, 2, 8.0, 1.0e-6, 41), 0.0, 3000.0)
+    while fine.time()[0] < 365.0 * 86400.0:
+        fine.advance_resident(200)
     helper = QGNModule(pc, H, S, U)
     net = cl.ClosureNet(nz=2, H=128, W=128, layers=6, max_batch=16, seed=2)
-    x, y, isc, osc = cl.make_dataset(fine, helper, n=112, every=3, cin_p=net.cin_p, cout_p=net.cout_p)
-    ntr = 96
-    cl.train(net, x[:ntr], y[:ntr], iters=2500, batch=8, lr=1e-3)
-    pred = torch.zeros((16, 128, 128, net.cout_p), dtype=torch.float32, device="cuda")
-    net.forward(x[ntr:], pred, 16)
+    # samples 8 steps apart: consecutive steps are nearly the same flow
+    x, y, isc, osc = cl.make_dataset(fine, helper, n=320, every=8, cin_p=net.cin_p, cout_p=net.cout_p)
+    ntr, nte = 280, 40
+    cl.train(net, x[:ntr], y[:ntr], iters=1500, batch=8, lr=1e-3)
+    pred = torch.zeros((nte, 128, 128, net.cout_p), dtype=torch.float32, device="cuda")
+    for i in range(0, nte, 8):
+        net.forward(x[ntr + i:ntr + i + 8], pred[i:i + 8], 8)
     torch.cuda.synchronize()
     yt = y[ntr:].cpu().numpy()[..., :2]
     yp = pred.cpu().numpy()[..., :2]
@@ -215,12 +221,12 @@ def test_trained_closure_beats_leith_offline(cuda_ok):
     mc = QGNOracle(Params(**pc), H, S, U)
     xq = x[ntr:].float().cpu().numpy()[..., :2] / isc[:2]
     lt = []
-    for i in range(16):
+    for i in range(nte):
         qphys = np.moveaxis(xq[i], -1, 0)
         qhat = mc.dealias(mc.g2s(qphys))
         lt.append(np.moveaxis(leith_tendency(mc, qhat, mc.leith_A8L(qhat)), 0, -1) * osc[:2])
     lt = np.array(lt)
     alpha = np.sum(lt * yt) / np.sum(lt * lt)
     r2_leith = 1.0 - np.sum((alpha * lt - yt) ** 2) / np.sum((yt - yt.mean(axis=(0, 1, 2))) ** 2)
-    assert r2_cnn > 0.3, (r2_cnn, r2_leith)
+    assert r2_cnn > 0.15, (r2_cnn, r2_leith)
     assert r2_cnn > r2_leith + 0.1, (r2_cnn, r2_leith)
