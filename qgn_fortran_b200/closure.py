@@ -92,6 +92,14 @@ class ClosureNet:
                                                 C.byref(loss) if want_loss else None), "qgn_cnn_train_step")
         return loss.value if want_loss else None
 
+    def set_engine(self, engine: str):
+        """'tcgen05' (TMEM accumulators, default) or 'mma.sync' (warp-level MMA)."""
+        self._check(self.lib.qgn_cnn_set_engine(self.net, {"tcgen05": 0, "mma.sync": 1}[engine]),
+                    "qgn_cnn_set_engine")
+
+    def check(self):
+        self._check(self.lib.qgn_cnn_check(self.net), "qgn_cnn_check")
+
     def stream(self):
         sp = C.c_void_p()
         self._check(self.lib.qgn_cnn_stream(self.net, C.byref(sp)), "qgn_cnn_stream")

@@ -209,9 +209,9 @@ int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop
             RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
         }
     }
+    // the update kernels also clear the max reduction of the error transform
     if (mixed(ctx)) CK(launch_ark_update_mixed(g, b, st));
     else CK(launch_ark_update(g, b, st));
-    CK(launch_zero_scalar_max(b.sc, st));
     CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
     CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, max_rejects(ctx), loop, st));
     return QGN_OK;

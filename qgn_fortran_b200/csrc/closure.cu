@@ -16,13 +16,15 @@
 //     dZ = sum_l H_l/Htot <q_l S_l> <= 0            (the closure removes enstrophy)
 //     dE = -sum_l H_l/Htot <psi_l S_l> <= limit * E / day,  E = -1/2 sum_l H_l/Htot <psi_l q_l>,
 // decides per step: passing, the step uses S with the background hyperviscosity A8_background;
-// failing, S is dropped and the step is plain QG-Leith (ARK43_QGLeith.f90:62-73).
+// failing, S is dropped and the step is plain QG-Leith (ARK43_QGLeith.f90:62-73).  The
+// averages are Parseval sums over the kept modes, so the check costs one launch.
 #include "qgn_internal.cuh"
 #include "cnn.cuh"
 #include "prof.cuh"
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -34,7 +36,7 @@ struct ClosureStats {
     long long fallbacks;
     double dE, dZ, E;
     int pass;
-    int pad;
+    unsigned int red_count;     // blocks done in the budget kernel's last-block reduction
 };
 
 struct Closure {
@@ -42,7 +44,6 @@ struct Closure {
     float* scales = nullptr;          // device: in [2 nz], out [nz]
     __nv_bfloat16* x = nullptr;       // [ny][nx][cin_p]
     float* y = nullptr;               // [ny][nx][cout_p]
-    double* phys = nullptr;           // 3 physical fields
     double2* S = nullptr;             // compact closure tendency
     double* red = nullptr;            // 3 x nblocks partial sums
     double* flag = nullptr;           // 1 passing, 0 fallback
@@ -106,82 +107,114 @@ __global__ void k_pack_out(int nz, size_t npix, const double* __restrict__ s, co
         for (int c = 0; c < cout_p; ++c) y[p * cout_p + c] = c < nz ? (float)s[(size_t)c * npix + p] * osc[c] : 0.f;
 }
 
-// network output -> physical S_c = y[p][c] / out_scale_c
-__global__ void k_unpack_out(int nz, size_t npix, const float* __restrict__ y, const float* __restrict__ osc,
-                             int cout_p, double* __restrict__ s) {
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < npix * nz; e += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e / npix);
-        const size_t p = e % npix;
-        s[e] = (double)y[p * cout_p + c] / (double)osc[c];
-    }
+// The energy-budget check of the applied tendency S (compact, dealiased) in one launch, by
+// Parseval on the kept modes (the kx = 0 column in the Hermitian projection that the
+// inverse transform applies):
+//   <a b> = sum over the full plane of Re(conj(a_k) b_k) / (nx ny)^2,
+//   dE = -sum_l w_l <psi_l S_l>,  dZ = sum_l w_l <q_l S_l>,  E = -1/2 sum_l w_l <psi_l q_l>.
+// Each block writes its partial sums; the block that finishes last (counted in st->red_count)
+// adds them in a fixed order, decides, updates the statistics, and keeps S with the
+// background A8 or zeroes S (plain QG-Leith for the step).
+__device__ __forceinline__ double2 herm_proj(const Geom& g, const double2* __restrict__ f, size_t lP, int m, bool& pk) {
+    const int j = g.jfull(m);
+    const int jp = (g.ny - j) % g.ny;
+    pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
+    const double2 v = f[lP + m];
+    double2 fp = make_double2(0.0, 0.0);
+    if (pk) fp = f[lP + (jp < g.kylo ? jp : jp - g.kyshift)];
+    return make_double2(0.5 * (v.x + fp.x), 0.5 * (v.y - fp.y));
 }
 
-// per-block sums of sum_l w_l {psi S, q S, psi q} over the physical grid
-__global__ void __launch_bounds__(256) k_budget(int nz, size_t npix, const double* __restrict__ q,
-                                                const double* __restrict__ psi, const double* __restrict__ s,
-                                                const double* __restrict__ Hw, double* __restrict__ red) {
+__global__ void __launch_bounds__(256) k_budget_spec(Geom g, const double2* __restrict__ q,
+                                                     const double2* __restrict__ psi, double2* __restrict__ S,
+                                                     const double* __restrict__ Hw, double* __restrict__ red,
+                                                     double A8bg, double elimit, DevScalars* __restrict__ sc,
+                                                     ClosureStats* __restrict__ st, double* __restrict__ flag) {
     __shared__ double sm[3][8];
+    __shared__ unsigned s_last;
+    const size_t P = (size_t)g.nkx * g.nky;
+    const int nb = gridDim.x;
     double a = 0.0, b = 0.0, c = 0.0;
-    for (int l = 0; l < nz; ++l) {
-        const double w = Hw[l];
-        const double* ql = q + (size_t)l * npix;
-        const double* pl = psi + (size_t)l * npix;
-        const double* sl = s + (size_t)l * npix;
-        double al = 0.0, bl = 0.0, cl = 0.0;
-        for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
-            al += pl[p] * sl[p];
-            bl += ql[p] * sl[p];
-            cl += pl[p] * ql[p];
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(p / g.nky), m = (int)(p % g.nky);
+        for (int l = 0; l < g.nz; ++l) {
+            const size_t lP = (size_t)l * P;
+            double2 hq, hp, hs;
+            double f;
+            if (kx > 0) {
+                hq = q[lP + p];
+                hp = psi[lP + p];
+                hs = S[lP + p];
+                f = 2.0;
+            } else {
+                bool pk;
+                hq = herm_proj(g, q, lP, m, pk);
+                hp = herm_proj(g, psi, lP, m, pk);
+                hs = herm_proj(g, S, lP, m, pk);
+                f = pk ? 1.0 : 2.0;
+            }
+            const double w = Hw[l] * f;
+            a += w * (hp.x * hs.x + hp.y * hs.y);
+            b += w * (hq.x * hs.x + hq.y * hs.y);
+            c += w * (hp.x * hq.x + hp.y * hq.y);
         }
-        a += w * al;
-        b += w * bl;
-        c += w * cl;
     }
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
         b += __shfl_xor_sync(0xffffffffu, b, o);
         c += __shfl_xor_sync(0xffffffffu, c, o);
     }
-    const int wid = threadIdx.x / 32;
     if (threadIdx.x % 32 == 0) {
-        sm[0][wid] = a;
-        sm[1][wid] = b;
-        sm[2][wid] = c;
+        sm[0][threadIdx.x / 32] = a;
+        sm[1][threadIdx.x / 32] = b;
+        sm[2][threadIdx.x / 32] = c;
     }
     __syncthreads();
-    if (threadIdx.x < 3) {
-        double t = 0.0;
-        for (int i = 0; i < (int)(blockDim.x / 32); ++i) t += sm[threadIdx.x][i];
-        red[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = t;
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) {
+            t0 += sm[0][i];
+            t1 += sm[1][i];
+            t2 += sm[2][i];
+        }
+        red[blockIdx.x] = t0;
+        red[nb + blockIdx.x] = t1;
+        red[2 * nb + blockIdx.x] = t2;
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->red_count, 1u);
+        s_last = (prev + 1 == (unsigned)nb) ? 1u : 0u;
     }
-}
-
-__global__ void k_budget_decide(int nz, int nblocks, double inv_npix, double A8bg, double elimit,
-                                const double* __restrict__ red, DevScalars* __restrict__ sc,
-                                ClosureStats* __restrict__ st, double* __restrict__ flag) {
-    double a = 0.0, b = 0.0, c = 0.0;
-    for (int i = 0; i < nblocks; ++i) {
-        a += red[i];
-        b += red[nblocks + i];
-        c += red[2 * nblocks + i];
+    __syncthreads();
+    if (!s_last) return;
+    __shared__ int s_pass;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        double sa = 0.0, sb = 0.0, sc2 = 0.0;
+        for (int i = 0; i < nb; ++i) {
+            sa += __ldcg(&red[i]);
+            sb += __ldcg(&red[nb + i]);
+            sc2 += __ldcg(&red[2 * nb + i]);
+        }
+        const double N = (double)g.nx * (double)g.ny, inv = 1.0 / (N * N);
+        const double dE = -sa * inv, dZ = sb * inv, E = -0.5 * sc2 * inv;
+        const bool pass = (dZ <= 0.0) && (dE <= elimit * E / 86400.0) && (dE == dE) && (dZ == dZ);
+        st->evaluations += 1;
+        st->fallbacks += pass ? 0 : 1;
+        st->dE = dE;
+        st->dZ = dZ;
+        st->E = E;
+        st->pass = pass ? 1 : 0;
+        st->red_count = 0u;
+        *flag = pass ? 1.0 : 0.0;
+        if (pass)
+            for (int l = 0; l < g.nz; ++l) sc->A8L[l] = A8bg;
+        s_pass = pass ? 1 : 0;
     }
-    const double dE = -a * inv_npix, dZ = b * inv_npix, E = -0.5 * c * inv_npix;
-    const bool pass = (dZ <= 0.0) && (dE <= elimit * E / 86400.0) && (dE == dE) && (dZ == dZ);
-    st->evaluations += 1;
-    st->fallbacks += pass ? 0 : 1;
-    st->dE = dE;
-    st->dZ = dZ;
-    st->E = E;
-    st->pass = pass ? 1 : 0;
-    *flag = pass ? 1.0 : 0.0;
-    if (pass)
-        for (int l = 0; l < nz; ++l) sc->A8L[l] = A8bg;
-}
-
-__global__ void k_keep_if_passed(size_t n, const double* __restrict__ flag, double2* __restrict__ s) {
-    const double f = *flag;
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-        s[e] = f != 0.0 ? s[e] : make_double2(0.0, 0.0);   // a dropped tendency is exactly zero
+    __syncthreads();
+    if (!s_pass) {   // a dropped tendency is exactly zero (not S * 0: S may hold Inf)
+        const size_t n = g.csize();
+        for (size_t e = threadIdx.x; e < n; e += blockDim.x) S[e] = make_double2(0.0, 0.0);
+    }
 }
 
 int grid_of(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
@@ -202,36 +235,22 @@ bool compatible(const qgn_ctx* f, const qgn_ctx* c) {
 // the closure's tendency (compact) for the stage right-hand sides, or NULL
 const double2* closure_tendency(const qgn_ctx* ctx) { return ctx->closure ? ctx->closure->S : nullptr; }
 
-// evaluate the network on the state (b.q, with b.psi = GetPsi(b.q)) and run the budget check
+// evaluate the network on the state (b.q, with b.psi = GetPsi(b.q)) and run the budget check:
+// y-inverse of (q, psi) and an x-inverse that writes the network input, the network, the
+// forward transform of its output, the budget kernel -- eleven launches with the six convolutions
 int closure_eval(qgn_ctx* ctx) {
     Closure* c = ctx->closure;
     const Geom& g = ctx->g;
     const Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
-    const size_t npix = (size_t)g.nx * g.ny, np = npix * g.nz;
-    double* P0 = c->phys;
-    double* P1 = P0 + np;
-    double* P2 = P1 + np;
-    if (launch_to_phys(g, b, b.q, P0, st) != cudaSuccess) return QGN_ERR_CUDA;
-    if (launch_to_phys(g, b, b.psi, P1, st) != cudaSuccess) return QGN_ERR_CUDA;
-    QGN_LAUNCH(KID_LAYOUT, 16.0 * np + 2.0 * npix * c->cin_p, st,
-               k_pack_in<<<grid_of(npix), 256, 0, st>>>(g.nz, npix, P0, P1, c->scales, c->cin_p, c->x));
-    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_closure_input(g, b, b.q, b.psi, c->scales, c->x, c->cin_p, st) != cudaSuccess) return QGN_ERR_CUDA;
     if (cnn::infer(c->net, c->x, c->y, 1, st) != QGN_OK) return QGN_ERR_CUDA;
-    QGN_LAUNCH(KID_LAYOUT, 4.0 * npix * c->cout_p + 8.0 * np, st,
-               k_unpack_out<<<grid_of(np), 256, 0, st>>>(g.nz, npix, c->y, c->scales + 2 * g.nz, c->cout_p, P2));
-    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
-    if (launch_from_phys(g, b, P2, c->S, st) != cudaSuccess) return QGN_ERR_CUDA;
-    if (launch_to_phys(g, b, c->S, P2, st) != cudaSuccess) return QGN_ERR_CUDA;   // the applied (dealiased) S
-    QGN_LAUNCH(KID_PARSEVAL, 24.0 * np, st,
-               k_budget<<<c->nblocks, 256, 0, st>>>(g.nz, npix, P0, P1, P2, b.Hw, c->red));
-    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
-    QGN_LAUNCH(KID_SCALAR, 0.0, st,
-               k_budget_decide<<<1, 1, 0, st>>>(g.nz, c->nblocks, 1.0 / (double)npix, c->A8bg, c->elimit, c->red, b.sc,
-                                                 c->stats, c->flag));
-    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
-    QGN_LAUNCH(KID_LAYOUT, 32.0 * g.csize(), st,
-               k_keep_if_passed<<<grid_of(g.csize()), 256, 0, st>>>(g.csize(), c->flag, c->S));
+    if (launch_closure_output(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->S, st) != cudaSuccess)
+        return QGN_ERR_CUDA;
+    const int nb = (int)std::min<size_t>(((size_t)g.nkx * g.nky + 255) / 256, (size_t)c->nblocks);
+    QGN_LAUNCH(KID_PARSEVAL, 48.0 * g.csize(), st,
+               k_budget_spec<<<nb, 256, 0, st>>>(g, b.q, b.psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
+                                                  c->stats, c->flag));
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     return QGN_OK;
 }
@@ -242,7 +261,6 @@ void closure_free(qgn_ctx* ctx) {
     cudaFree(c->scales);
     cudaFree(c->x);
     cudaFree(c->y);
-    cudaFree(c->phys);
     cudaFree(c->S);
     cudaFree(c->red);
     cudaFree(c->flag);
@@ -351,7 +369,6 @@ int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const 
     bool ok = cudaMalloc((void**)&c->scales, sizeof(float) * 3 * g.nz) == cudaSuccess &&
               cudaMalloc((void**)&c->x, sizeof(__nv_bfloat16) * npix * c->cin_p) == cudaSuccess &&
               cudaMalloc((void**)&c->y, sizeof(float) * npix * c->cout_p) == cudaSuccess &&
-              cudaMalloc((void**)&c->phys, sizeof(double) * 3 * np) == cudaSuccess &&
               cudaMalloc((void**)&c->S, sizeof(double2) * g.csize()) == cudaSuccess &&
               cudaMalloc((void**)&c->red, sizeof(double) * 3 * c->nblocks) == cudaSuccess &&
               cudaMalloc((void**)&c->flag, sizeof(double)) == cudaSuccess &&
@@ -359,6 +376,7 @@ int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const 
     ok = ok && cudaMemcpy(c->scales, in_scale, sizeof(float) * 2 * g.nz, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(c->scales + 2 * g.nz, out_scale, sizeof(float) * g.nz, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(c->stats, 0, sizeof(ClosureStats)) == cudaSuccess &&
+         cudaMemset(c->x, 0, sizeof(__nv_bfloat16) * npix * c->cin_p) == cudaSuccess &&
          cudaMemset(c->S, 0, sizeof(double2) * g.csize()) == cudaSuccess;
     if (!ok) {
         closure_free(ctx);

@@ -4,7 +4,9 @@
 // periodic QG domain), GELU after every layer but the last.  Activations are NHWC BF16 with
 // the channel count padded to a multiple of 16; weights are FP32 masters with BF16 copies in
 // two layouts (forward: [tap][cout][cin], backward-data: [tap'][cin][cout] with the taps
-// mirrored); products run on the BF16 tensor cores (mma.m16n8k16) with FP32 accumulation.
+// mirrored); products run on the BF16 tensor cores with FP32 accumulation: tcgen05.mma with
+// the accumulator tile in TMEM (default), or the warp-level mma.m16n8k16 path (selectable with
+// qgn_cnn_set_engine or QGN_CNN_MMA=sync; the weight gradients always use it).
 //
 // Kernels (one CTA = 8 warps = 128 consecutive pixels of one image row, persistent over rows):
 //   k_conv<CIN,COUT,EPI>  implicit GEMM  out[p, n] = sum_{tap, k} in[p + tap, k] w[tap, n, k]
@@ -23,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <random>
@@ -354,6 +357,270 @@ __global__ void k_gather(const unsigned char* __restrict__ src, const int* __res
     }
 }
 
+// ---- the same convolution on the 5th-generation tensor cores (tcgen05, accumulator in TMEM) ----
+// One tile = 128 consecutive pixels of an image row (GEMM M = 128) x all COUT output channels
+// (N = COUT) with K = 9 taps x CIN, issued as 9*CIN/16 tcgen05.mma (kind::f16, BF16 in, FP32
+// accumulate) by one thread; the FP32 tile lives in TMEM (COUT columns, one lane per pixel) and
+// the epilogue reads it back with tcgen05.ld.  Operands sit in shared memory in the canonical
+// K-major no-swizzle layout (core matrices of 8 rows x 16 bytes):
+//   input rows  ring of 4 slots [CIN/8 chunks][130 pixels][8 channels]; the A tile of tap
+//               (dh, dw) starts at pixel dw of the slot holding row h+dh-1: rows (pixels) 16 B
+//               apart, 8-row groups 128 B apart (SBO), the two halves of a K step 130*16 B apart (LBO);
+//   weights     [9 taps][CIN/8 chunks][COUT][8]: SBO 128 B, LBO COUT*16 B.
+// Each CTA takes a contiguous range of tiles ordered row-fastest, so consecutive tiles share two
+// of their three input rows: one new row per tile, fetched with cp.async into the free ring slot
+// while the current tile's MMAs run.  Completion is signalled by tcgen05.commit on an mbarrier;
+// every wait is bounded, and a wait that runs out records an error, waits once more, frees the
+// TMEM and returns.
+namespace tc {
+
+constexpr int kPixS = kTileP + 2;        // staged pixels per input row (periodic halo)
+constexpr int kSlots = 4;                // input-row ring
+constexpr long long kWaitLimit = 1LL << 22;
+
+constexpr int imax(int a, int b) { return a > b ? a : b; }
+
+// Shared-memory plan.  SMEM also covers the bytes an MMA would read if the hardware took the
+// two descriptor strides the other way round (8-row groups LBO apart, K halves SBO apart):
+// every operand read of the kernel stays inside the CTA's allocation under either reading.
+template <int CIN, int COUT>
+struct Lay {
+    static constexpr int SLOT_BYTES = (CIN / 8) * kPixS * 16;
+    static constexpr int IN_BYTES = kSlots * SLOT_BYTES;
+    static constexpr int W_OFF = (IN_BYTES + 1023) / 1024 * 1024;
+    static constexpr int W_BYTES = 9 * (CIN / 8) * COUT * 16;
+    static constexpr int BAR_OFF = (W_OFF + W_BYTES + 1023) / 1024 * 1024;
+    static constexpr int A_LAST = (kSlots - 1) * SLOT_BYTES + ((CIN / 8 - 2) * kPixS + 2) * 16;
+    static constexpr int B_LAST = W_OFF + (8 * (CIN / 8) + CIN / 8 - 2) * COUT * 16;
+    static constexpr int A_END = A_LAST + imax(kPixS * 16 + 15 * 128, 15 * kPixS * 16 + 128) + 128;
+    static constexpr int B_END = B_LAST + imax(COUT * 16 + (COUT / 8 - 1) * 128, (COUT / 8 - 1) * COUT * 16 + 128) + 128;
+    static constexpr int SMEM = (imax(BAR_OFF + 64, imax(A_END, B_END)) + 1023) / 1024 * 1024 + 1024;
+    static constexpr int TMEM_COLS = COUT < 32 ? 32 : COUT;   // power of two >= 32
+};
+
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);   // version 1, no swizzle
+}
+
+// M = 128, N = COUT, BF16 x BF16 -> F32, both operands K-major
+template <int N>
+__host__ __device__ constexpr uint32_t idesc() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(id), "r"(accumulate));
+}
+
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp16(uint32_t saddr, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int NC>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float* v);
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float* v) {
+    tmem_ld<16>(taddr, v);
+    tmem_ld<16>(taddr + 16, v + 16);
+}
+
+// one input row (image b, row hh, pixels w0-1 .. w0+128 periodic) into a ring slot, asynchronously
+template <int CIN>
+__device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, int b, int hh, int H, int W, int w0,
+                                         uint32_t slot_addr) {
+    for (int i = threadIdx.x; i < kPixS * (CIN / 8); i += kThreads) {
+        const int c8 = i % (CIN / 8), px = i / (CIN / 8);
+        int ww = w0 - 1 + px;
+        ww = (ww % W + W) % W;
+        cp16(slot_addr + (uint32_t)((c8 * kPixS + px) * 16), x + (((size_t)b * H + hh) * W + ww) * CIN + c8 * 8);
+    }
+}
+
+}  // namespace tc
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
+              int B, int H, int W, float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
+              const float* __restrict__ zin, int* __restrict__ err) {
+    using L = tc::Lay<CIN, COUT>;
+    static_assert(COUT == 16 || COUT == 64, "N of the MMA");
+    extern __shared__ __align__(1024) unsigned char smtc[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smtc + L::BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smtc + L::BAR_OFF + 16);
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t bar_a = smem_u32(bar), in_a = smem_u32(smtc), w_a = smem_u32(smtc + L::W_OFF);
+
+    // this CTA's tiles: a contiguous range of t = ((b * segs + seg) * H + h), rows fastest
+    const int segs = W / kTileP;
+    const int ntiles = B * H * segs;
+    const int per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per, t1 = min(ntiles, t0 + per);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "r"((uint32_t)L::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += kThreads) {
+        const int c8 = i % (CIN / 8), n = (i / (CIN / 8)) % COUT, tap = i / ((CIN / 8) * COUT);
+        tc::cp16(w_a + (uint32_t)((((tap * (CIN / 8)) + c8) * COUT + n) * 16), wt + ((size_t)tap * COUT + n) * CIN + c8 * 8);
+    }
+    tc::cp_commit();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+
+    // ring bookkeeping (uniform across the CTA): key of the row in each slot, -1 = empty;
+    // key = (b * segs + seg) * H + hh
+    int key[tc::kSlots] = {-1, -1, -1, -1};
+    uint32_t phase = 0;
+    for (int t = t0; t < t1; ++t) {
+        const int h = t % H, bs = t / H;
+        const int seg = bs % segs, b = bs / segs;
+        const int w0 = seg * kTileP;
+        int need[3], slot[3];
+        for (int k = 0; k < 3; ++k) {
+            need[k] = bs * H + (h + k - 1 + H) % H;
+            slot[k] = -1;
+            for (int sI = 0; sI < tc::kSlots; ++sI)
+                if (key[sI] == need[k]) slot[k] = sI;
+        }
+        for (int k = 0; k < 3; ++k) {
+            if (slot[k] >= 0) continue;
+            int free_slot = -1;
+            for (int sI = 0; sI < tc::kSlots && free_slot < 0; ++sI) {
+                bool used = false;
+                for (int j = 0; j < 3; ++j) used = used || (slot[j] == sI);
+                if (!used) free_slot = sI;
+            }
+            slot[k] = free_slot;
+            key[free_slot] = need[k];
+            tc::fetch_row<CIN>(x, b, need[k] - bs * H, H, W, w0, in_a + (uint32_t)(free_slot * L::SLOT_BYTES));
+        }
+        tc::cp_commit();
+        tc::cp_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            uint32_t acc = 0;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; ++tap) {
+                const int dh = tap / 3, dw = tap % 3;
+                const uint32_t row_a = in_a + (uint32_t)(slot[dh] * L::SLOT_BYTES);
+#pragma unroll
+                for (int kc = 0; kc < CIN / 16; ++kc) {
+                    const uint32_t a_addr = row_a + (uint32_t)((2 * kc * tc::kPixS + dw) * 16);
+                    const uint32_t b_addr = w_a + (uint32_t)((tap * (CIN / 8) + 2 * kc) * COUT * 16);
+                    tc::mma(tmem, tc::sdesc(a_addr, tc::kPixS * 16, 128), tc::sdesc(b_addr, COUT * 16, 128),
+                            tc::idesc<COUT>(), acc);
+                    acc = 1;
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a)
+                         : "memory");
+        }
+        // prefetch the next tile's new row into the slot this tile does not read
+        if (t + 1 < t1) {
+            const int hn = (t + 1) % H, bsn = (t + 1) / H;
+            const int needn = bsn * H + (hn + 1) % H;
+            bool have = false;
+            for (int sI = 0; sI < tc::kSlots; ++sI) have = have || (key[sI] == needn);
+            if (!have && bsn == bs) {
+                int free_slot = -1;
+                for (int sI = 0; sI < tc::kSlots && free_slot < 0; ++sI)
+                    if (sI != slot[0] && sI != slot[1] && sI != slot[2]) free_slot = sI;
+                key[free_slot] = needn;
+                tc::fetch_row<CIN>(x, b, needn - bsn * H, H, W, (bsn % segs) * kTileP,
+                                   in_a + (uint32_t)(free_slot * L::SLOT_BYTES));
+                tc::cp_commit();
+            }
+        }
+        const bool ok = tc::bar_wait(bar_a, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(err, 1);
+            tc::bar_wait(bar_a, phase ^ 1u);   // once more for the MMAs in flight
+            break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        // epilogue: warp w reads TMEM lanes 32 (w % 4).. (pixels) and a block of columns
+        constexpr int NCOL = COUT == 64 ? 32 : 16;
+        if (COUT == 64 || warp < 4) {
+            const int px = 32 * (warp % 4) + lane;
+            const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+            float v[NCOL];
+            tc::tmem_ld<NCOL>(tmem + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)n0, v);
+            const size_t p = ((size_t)b * H + h) * W + w0 + px;
+#pragma unroll
+            for (int j = 0; j < NCOL; j += 4) {
+                const int n = n0 + j;
+                if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+                    const float4 bb = *reinterpret_cast<const float4*>(bias + n);
+                    const float4 z = make_float4(v[j] + bb.x, v[j + 1] + bb.y, v[j + 2] + bb.z, v[j + 3] + bb.w);
+                    *reinterpret_cast<float4*>(outf + p * COUT + n) = z;
+                    if (EPI == EPI_GELU) {
+                        __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(gelu(z.x), gelu(z.y)),
+                                                __floats2bfloat162_rn(gelu(z.z), gelu(z.w))};
+                        *reinterpret_cast<uint2*>(outb + p * COUT + n) = *reinterpret_cast<const uint2*>(g2);
+                    }
+                } else {
+                    const float4 z = *reinterpret_cast<const float4*>(zin + p * COUT + n);
+                    __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(v[j] * gelu_grad(z.x), v[j + 1] * gelu_grad(z.y)),
+                                            __floats2bfloat162_rn(v[j + 2] * gelu_grad(z.z), v[j + 3] * gelu_grad(z.w))};
+                    *reinterpret_cast<uint2*>(outb + p * COUT + n) = *reinterpret_cast<const uint2*>(g2);
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();   // TMEM read and ring slots released before the next tile's MMAs
+    }
+    tc::cp_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)L::TMEM_COLS));
+    }
+}
+
 template <int CIN, int COUT>
 constexpr int conv_smem() {
     return (9 * COUT + 3 * (kTileP + 2)) * RowPad<CIN>::LD * 2;
@@ -387,6 +654,8 @@ struct qgn_cnn {
     double* loss_host = nullptr;
     float* ytgt = nullptr;                           // gathered targets
     long long adam_t = 0;
+    int engine = 0;                                  // 0: tcgen05 (TMEM accumulators), 1: mma.sync
+    int* d_err = nullptr;                            // device error word of the tcgen05 kernels
     std::vector<void*> owned;
     std::string last_error;
 };
@@ -426,6 +695,18 @@ int conv_grid(const qgn_cnn* n, int batch) {
 template <int CIN, int COUT, int EPI>
 cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat16* wt, const float* bias, int batch,
                           float* outf, __nv_bfloat16* outb, const float* zin) {
+    if (n->engine == 0) {
+        constexpr int SM = tc::Lay<CIN, COUT>::SMEM;
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        k_conv_tc<CIN, COUT, EPI><<<conv_grid(n, batch), kThreads, SM, n->stream>>>(x, wt, bias, batch, n->H, n->W,
+                                                                                    outf, outb, zin, n->d_err);
+        return cudaGetLastError();
+    }
     constexpr int SM = conv_smem<CIN, COUT>();
     static bool attr = false;
     if (!attr) {
@@ -526,9 +807,18 @@ int mse(qgn_cnn* net, int batch, const float* tgt) {
     return QGN_OK;
 }
 
+int check_err(qgn_cnn* net) {
+    int h = 0;
+    NCK(cudaMemcpyAsync(&h, net->d_err, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
+    NCK(cudaStreamSynchronize(net->stream));
+    if (h) return cnn_err(net, QGN_ERR_CUDA, "a tensor-core convolution timed out waiting for its MMAs");
+    return QGN_OK;
+}
+
 int read_loss(qgn_cnn* net, double* loss) {
     NCK(cudaMemcpyAsync(net->loss_host, net->loss_part, sizeof(double) * 148, cudaMemcpyDeviceToHost, net->stream));
     NCK(cudaStreamSynchronize(net->stream));
+    if (int rc = check_err(net)) return rc;
     double s = 0.0;
     for (int i = 0; i < 148; ++i) s += net->loss_host[i];
     if (loss) *loss = s;
@@ -617,9 +907,11 @@ int qgn_cnn_create(int cin, int width, int cout, int layers, int H, int W, int m
     }
     if (nalloc(net, &net->act[layers], 16) || nalloc(net, &net->gA, NP * net->width) ||
         nalloc(net, &net->gB, NP * net->width) || nalloc(net, &net->part, part) ||
-        nalloc(net, &net->loss_part, 148) || nalloc(net, &net->ytgt, NP * pad16(cout)))
+        nalloc(net, &net->loss_part, 148) || nalloc(net, &net->ytgt, NP * pad16(cout)) ||
+        nalloc(net, &net->d_err, 1))
         return fail(QGN_ERR_CUDA);
     net->part_elems = part;
+    if (const char* e = std::getenv("QGN_CNN_MMA")) net->engine = (std::string(e) == "sync") ? 1 : 0;
     if (cudaMallocHost((void**)&net->loss_host, sizeof(double) * 148) != cudaSuccess) return fail(QGN_ERR_CUDA);
     if (cudaStreamSynchronize(net->stream) != cudaSuccess) return fail(QGN_ERR_CUDA);
     *out = net;
@@ -746,6 +1038,18 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
     }
     if (loss) return read_loss(net, loss);
     return QGN_OK;
+}
+
+int qgn_cnn_set_engine(qgn_cnn* net, int engine) {
+    if (!net || engine < 0 || engine > 1) return QGN_ERR_ARG;
+    if (cudaStreamSynchronize(net->stream) != cudaSuccess) return QGN_ERR_CUDA;
+    net->engine = engine;
+    return QGN_OK;
+}
+
+int qgn_cnn_check(qgn_cnn* net) {
+    if (!net) return QGN_ERR_ARG;
+    return check_err(net);
 }
 
 int qgn_cnn_stream(qgn_cnn* net, void** stream) {

@@ -60,7 +60,7 @@ struct DevScalars {
     int halt;                     // sticky: set with status, cleared by a state upload
     int status;                   // QGN_ERR_* of the failure that set halt
     int rejects_step;             // consecutive rejections in the current step
-    int pad0;
+    unsigned int red_count;       // blocks done in a last-block reduction (0 between launches)
     long long accepted;           // accepted steps since creation
     long long attempts;           // attempts (accepted + rejected) since creation
     long long rejected;           // rejected attempts since creation
@@ -132,6 +132,14 @@ struct qgn_ctx {
 };
 
 namespace qgn {
+
+// the learned closure's tensors (rhs_kernels.cu): xout = NHWC BF16 [ny][nx][cin_p] with
+// channels (q_0..q_nz-1, psi_0..psi_nz-1) * scale; out = forward transform (compact, dealiased)
+// of channel l of the NHWC FP32 y divided by osc[l].  Both use b.hq/b.hu as scratch.
+cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
+                                 const float* scale, void* xout, int cin_p, cudaStream_t s);
+cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
+                                  double2* out, cudaStream_t s);
 
 // ---- learned closure (closure.cu) and graph invalidation (capi.cu) -----------------------
 int closure_eval(qgn_ctx* ctx);

@@ -19,6 +19,8 @@
 #include "prof.cuh"
 #include "rhs_tiles.cuh"
 
+#include <cuda_bf16.h>
+
 #include <mutex>
 #include <type_traits>
 #include <unordered_set>
@@ -53,34 +55,48 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __re
 // ------------------------------------------------------------------------------------
 // Single-field launches of the tile bodies (rhs_tiles.cuh): one CTA per tile, tile = blockIdx
 // ------------------------------------------------------------------------------------
-template <int NY, int NF, class CT>
-__global__ void __launch_bounds__(YInvCfg<NY, CT>::THREADS, minb(YInvCfg<NY, CT>::THREADS, regcap<CT>()))
+// TV selects a tile width (0: the default; see the configs in rhs_tiles.cuh)
+template <int NY, int NF, class CT, int TV = 0>
+__global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, regcap<CT>()))
     k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
            CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
-    yinv_tile<NY, NF, CT>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy);
+    yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy);
 }
 
-template <int NX, bool DRAG, class CT>
-__global__ void __launch_bounds__(XCfg<NX, DRAG, CT>::THREADS, minb(XCfg<NX, DRAG, CT>::THREADS, regcap<CT>(128, 80)))
+template <int NX, bool DRAG, class CT, int TV = 0>
+__global__ void __launch_bounds__(XCfg<NX, DRAG, CT, TV>::THREADS,
+                                  minb(XCfg<NX, DRAG, CT, TV>::THREADS, regcap<CT>(128, 80)))
     k_xpass(Geom g, int layer0, const CT* __restrict__ pq, const CT* __restrict__ pv,
             const CT* __restrict__ pu, CT* __restrict__ pp, CT* __restrict__ pd,
             const CT* __restrict__ twx) {
-    xpass_tile<NX, DRAG, CT>(g, blockIdx.x, layer0 + blockIdx.y, pq, pv, pu, pp, pd, twx);
+    xpass_tile<NX, DRAG, CT, TV>(g, blockIdx.x, layer0 + blockIdx.y, pq, pv, pu, pp, pd, twx);
 }
 
-template <int NY, bool DRAG, class CT>
-__global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT>::THREADS, minb(YFwdCfg<NY, DRAG, CT>::THREADS, regcap<CT>()))
+template <int NY, bool DRAG, class CT, int TV = 0>
+__global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT, TV>::THREADS,
+                                  minb(YFwdCfg<NY, DRAG, CT, TV>::THREADS, regcap<CT>()))
     k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const CT* __restrict__ q,
            const CT* __restrict__ psi, const CT* __restrict__ pp, const CT* __restrict__ pd,
            CT* __restrict__ out, const CT* __restrict__ twy, const CT* __restrict__ extra) {
-    yfwd_tile<NY, DRAG, CT>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy, extra);
+    yfwd_tile<NY, DRAG, CT, TV>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy, extra);
 }
 
-template <int NX, int EPI>
-__global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
+template <int NX, int EPI, int TV = 0>
+__global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
     k_xinv1(Geom g, const double2* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
             const double2* __restrict__ twx) {
-    xinv1_tile<NX, EPI>(g, blockIdx.x, blockIdx.y, hq, sc, outp, twx);
+    xinv1_tile<NX, EPI, TV>(g, blockIdx.x, blockIdx.y, hq, sc, outp, twx);
+}
+
+// Small grids launch few CTAs with the default tiles (at 128^2 x 4: 12 for the y-inverse),
+// so each CTA's serial transform work sets the kernel's duration.  For transform lengths
+// 64..256 a narrow variant (fewer columns or rows per CTA) is used when the default gives
+// fewer than two CTAs per SM and the narrow one gives more.  Tile width changes no arithmetic.
+constexpr int kNarrowY = 32, kNarrowX = 16, kNarrowX1 = 32;
+template <int N>
+constexpr bool has_narrow() { return N >= 64 && N <= 256; }
+static bool narrow_better(long long ctas_default, long long ctas_narrow) {
+    return ctas_default < 2 * 148 && ctas_narrow > ctas_default;
 }
 
 // ------------------------------------------------------------------------------------
@@ -88,9 +104,12 @@ __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
 // QGN_Module.f90:179-183): r2c of row pairs packed as r1 + i r2, then forward y columns
 // keeping the dealiased modes only.
 // ------------------------------------------------------------------------------------
-template <int NX>
+// SRC 0: physical field phys[nz][ny][nx]; SRC 1: channel l of the NHWC FP32 tensor y (cout_p
+// channels per pixel) divided by osc[l] (the learned closure's output)
+template <int NX, int SRC = 0>
 __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
-    k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx) {
+    k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx,
+            const float* __restrict__ y = nullptr, int cout_p = 0, const float* __restrict__ osc = nullptr) {
     using C = X1Cfg<NX>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = reinterpret_cast<double2*>(sm_raw);
@@ -100,7 +119,12 @@ __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
     const int slot = tid / C::G, lane = tid % C::G;
     const int rp = blockIdx.x * C::RP + slot;
     const size_t prow = ((size_t)l * g.ny + 2 * rp) * NX;
-    auto ld = [&](int x) -> double2 { return make_double2(phys[prow + x], phys[prow + NX + x]); };
+    auto ld = [&](int x) -> double2 {
+        if (SRC == 0) return make_double2(phys[prow + x], phys[prow + NX + x]);
+        const size_t pix = (size_t)(2 * rp) * NX + x;
+        const double inv = (double)osc[l];
+        return make_double2((double)y[pix * cout_p + l] / inv, (double)y[(pix + NX) * cout_p + l] / inv);
+    };
     NoIO none;
     fft_fused<NX, -1, SRC_FN, DST_SMEM>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
     const int nkx = g.nkx;
@@ -189,27 +213,56 @@ cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, 
     return cudaGetLastError();
 }
 
+template <int NY, int NF, class CT, int TV>
+static cudaError_t yinv_go(const Geom& g, const CT* q, const CT* psi, CT* hq, CT* hp, CT* hu, const CT* twy,
+                           cudaStream_t s) {
+    using C = YInvCfg<NY, CT, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_yinv<NY, NF, CT, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
+    const double es = (double)sizeof(CT);
+    const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
+    QGN_LAUNCH(KID_YINV, NF == 3 ? 2.0 * Cb + 3.0 * Hb : NF * (Cb + Hb), s,
+               k_yinv<NY, NF, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
+    return cudaGetLastError();
+}
+
 template <class CT>
 static cudaError_t launch_yinv(const Geom& g, int nf, const CT* q, const CT* psi, CT* hq, CT* hp, CT* hu, const CT* twy,
                                cudaStream_t s) {
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
-        using C = YInvCfg<NY, CT>;
-        dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
-        cudaError_t e;
-        const double es = (double)sizeof(CT);
-        const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
-        if (nf == 3) {
-            if ((e = set_smem(k_yinv<NY, 3, CT>, C::SMEM)) != cudaSuccess) return e;
-            QGN_LAUNCH(KID_YINV, 2.0 * Cb + 3.0 * Hb, s,
-                       k_yinv<NY, 3, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
-        } else {
-            if ((e = set_smem(k_yinv<NY, 1, CT>, C::SMEM)) != cudaSuccess) return e;
-            QGN_LAUNCH(KID_YINV, Cb + Hb, s,
-                       k_yinv<NY, 1, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
+        if constexpr (has_narrow<NY>()) {
+            const long long cd = (long long)((g.nkx + YInvCfg<NY, CT>::TKX - 1) / YInvCfg<NY, CT>::TKX) * g.nz;
+            const long long cn =
+                (long long)((g.nkx + YInvCfg<NY, CT, kNarrowY>::TKX - 1) / YInvCfg<NY, CT, kNarrowY>::TKX) * g.nz;
+            if (narrow_better(cd, cn)) {
+                if constexpr (std::is_same<CT, double2>::value) {
+                    if (nf == 2) return yinv_go<NY, 2, CT, kNarrowY>(g, q, psi, hq, hp, hu, twy, s);
+                }
+                return nf == 3 ? yinv_go<NY, 3, CT, kNarrowY>(g, q, psi, hq, hp, hu, twy, s)
+                               : yinv_go<NY, 1, CT, kNarrowY>(g, q, psi, hq, hp, hu, twy, s);
+            }
         }
-        return cudaGetLastError();
+        if constexpr (std::is_same<CT, double2>::value) {
+            if (nf == 2) return yinv_go<NY, 2, CT, 0>(g, q, psi, hq, hp, hu, twy, s);
+        }
+        return nf == 3 ? yinv_go<NY, 3, CT, 0>(g, q, psi, hq, hp, hu, twy, s)
+                       : yinv_go<NY, 1, CT, 0>(g, q, psi, hq, hp, hu, twy, s);
     });
+}
+
+template <int NX, bool DRAG, class CT, int TV>
+static cudaError_t xpass_go(const Geom& g, int layer0, int layers, const CT* hq, const CT* hp, const CT* hu, CT* hpp,
+                            CT* hpd, const CT* twx, cudaStream_t s) {
+    using C = XCfg<NX, DRAG, CT, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_xpass<NX, DRAG, CT, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, layers);
+    const double es = (double)sizeof(CT);
+    QGN_LAUNCH(KID_XPASS, (DRAG ? 7.0 : 5.0) * es * (double)layers * g.ny * g.nkx, s,
+               k_xpass<NX, DRAG, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, layer0, hq, hp, hu, hpp, hpd, twx));
+    return cudaGetLastError();
 }
 
 template <class CT>
@@ -218,27 +271,47 @@ static cudaError_t launch_xpass(const Geom& g, const CT* hq, const CT* hp, const
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
         cudaError_t e;
-        const double es = (double)sizeof(CT);
         const int nplain = drag ? g.nz - 1 : g.nz;
+        bool narrow = false;
+        if constexpr (has_narrow<NX>()) {
+            const long long cd = (long long)((g.ny / 2 + XCfg<NX, false, CT>::RP - 1) / XCfg<NX, false, CT>::RP) * g.nz;
+            const long long cn =
+                (long long)((g.ny / 2 + XCfg<NX, false, CT, kNarrowX>::RP - 1) / XCfg<NX, false, CT, kNarrowX>::RP) *
+                g.nz;
+            narrow = narrow_better(cd, cn);
+        }
         if (nplain > 0) {
-            using C = XCfg<NX, false, CT>;
-            if ((e = set_smem(k_xpass<NX, false, CT>, C::SMEM)) != cudaSuccess) return e;
-            dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, nplain);
-            QGN_LAUNCH(KID_XPASS, 5.0 * es * (double)nplain * g.ny * g.nkx, s,
-                       k_xpass<NX, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, hq, hp, hu, hpp, hpd, twx));
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if constexpr (has_narrow<NX>())
+                e = narrow ? xpass_go<NX, false, CT, kNarrowX>(g, 0, nplain, hq, hp, hu, hpp, hpd, twx, s)
+                           : xpass_go<NX, false, CT, 0>(g, 0, nplain, hq, hp, hu, hpp, hpd, twx, s);
+            else
+                e = xpass_go<NX, false, CT, 0>(g, 0, nplain, hq, hp, hu, hpp, hpd, twx, s);
+            if (e != cudaSuccess) return e;
         }
         if (drag) {
-            using C = XCfg<NX, true, CT>;
-            if ((e = set_smem(k_xpass<NX, true, CT>, C::SMEM)) != cudaSuccess) return e;
-            dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 1);
-            QGN_LAUNCH(KID_XPASS, 7.0 * es * (double)g.ny * g.nkx, s,
-                       k_xpass<NX, true, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, hq, hp, hu, hpp, hpd,
-                                                                                twx));
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if constexpr (has_narrow<NX>())
+                e = narrow ? xpass_go<NX, true, CT, kNarrowX>(g, g.nz - 1, 1, hq, hp, hu, hpp, hpd, twx, s)
+                           : xpass_go<NX, true, CT, 0>(g, g.nz - 1, 1, hq, hp, hu, hpp, hpd, twx, s);
+            else
+                e = xpass_go<NX, true, CT, 0>(g, g.nz - 1, 1, hq, hp, hu, hpp, hpd, twx, s);
+            if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
     });
+}
+
+template <int NY, bool DRAG, class CT, int TV>
+static cudaError_t yfwd_go(const Geom& g, int layer0, int layers, const LayerConst* lc, const CT* q, const CT* psi,
+                           const CT* hpp, const CT* hpd, CT* out, const CT* twy, const CT* extra, cudaStream_t s) {
+    using C = YFwdCfg<NY, DRAG, CT, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_yfwd<NY, DRAG, CT, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, layers);
+    const double lb = (double)sizeof(CT) * (double)layers * g.nkx;
+    QGN_LAUNCH(KID_YFWD, lb * ((DRAG ? 4.0 : 2.0) * NY + 3.0 * g.nky), s,
+               k_yfwd<NY, DRAG, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, layer0, lc, q, psi, hpp, hpd, out, twy,
+                                                                          extra));
+    return cudaGetLastError();
 }
 
 template <class CT>
@@ -248,27 +321,29 @@ static cudaError_t launch_yfwd(const Geom& g, const LayerConst* lc, const CT* q,
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
         cudaError_t e;
-        const double es = (double)sizeof(CT);
         const int nplain = drag ? g.nz - 1 : g.nz;
+        bool narrow = false;
+        if constexpr (has_narrow<NY>()) {
+            using D = YFwdCfg<NY, false, CT>;
+            using Nn = YFwdCfg<NY, false, CT, kNarrowY>;
+            narrow = narrow_better((long long)((g.nkx + D::TKX - 1) / D::TKX) * g.nz,
+                                   (long long)((g.nkx + Nn::TKX - 1) / Nn::TKX) * g.nz);
+        }
         if (nplain > 0) {
-            using C = YFwdCfg<NY, false, CT>;
-            if ((e = set_smem(k_yfwd<NY, false, CT>, C::SMEM)) != cudaSuccess) return e;
-            dim3 grid((g.nkx + C::TKX - 1) / C::TKX, nplain);
-            const double lb = es * (double)nplain * g.nkx;
-            QGN_LAUNCH(KID_YFWD, lb * (2.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, false, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, 0, lc, q, psi, hpp, hpd, out, twy,
-                                                                                 extra));
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if constexpr (has_narrow<NY>())
+                e = narrow ? yfwd_go<NY, false, CT, kNarrowY>(g, 0, nplain, lc, q, psi, hpp, hpd, out, twy, extra, s)
+                           : yfwd_go<NY, false, CT, 0>(g, 0, nplain, lc, q, psi, hpp, hpd, out, twy, extra, s);
+            else
+                e = yfwd_go<NY, false, CT, 0>(g, 0, nplain, lc, q, psi, hpp, hpd, out, twy, extra, s);
+            if (e != cudaSuccess) return e;
         }
         if (drag) {
-            using C = YFwdCfg<NY, true, CT>;
-            if ((e = set_smem(k_yfwd<NY, true, CT>, C::SMEM)) != cudaSuccess) return e;
-            dim3 grid((g.nkx + C::TKX - 1) / C::TKX, 1);
-            const double lb = es * (double)g.nkx;
-            QGN_LAUNCH(KID_YFWD, lb * (4.0 * NY + 3.0 * g.nky), s,
-                       k_yfwd<NY, true, CT><<<grid, C::THREADS, C::SMEM, s>>>(g, g.nz - 1, lc, q, psi, hpp, hpd, out,
-                                                                               twy, extra));
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if constexpr (has_narrow<NY>())
+                e = narrow ? yfwd_go<NY, true, CT, kNarrowY>(g, g.nz - 1, 1, lc, q, psi, hpp, hpd, out, twy, extra, s)
+                           : yfwd_go<NY, true, CT, 0>(g, g.nz - 1, 1, lc, q, psi, hpp, hpd, out, twy, extra, s);
+            else
+                e = yfwd_go<NY, true, CT, 0>(g, g.nz - 1, 1, lc, q, psi, hpp, hpd, out, twy, extra, s);
+            if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
     });
@@ -297,18 +372,28 @@ cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const
     return launch_yfwd<float2>(g, b.lc, q, psi, hpp, hpd, out, b.twy32, do_drag, s);
 }
 
+template <int NX, int EPI, int TV>
+static cudaError_t xinv1_go(const Geom& g, const Buffers& b, DevScalars* sc, double* outp, cudaStream_t s) {
+    using C = X1Cfg<NX, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_xinv1<NX, EPI, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
+    const double hb = 16.0 * (double)g.nz * g.ny * g.nkx;
+    QGN_LAUNCH(KID_XINV1, hb + (EPI == 1 ? 8.0 * (double)g.nz * g.ny * NX : 0.0), s,
+               k_xinv1<NX, EPI, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, sc, outp, b.twx));
+    return cudaGetLastError();
+}
+
 template <int EPI>
 static cudaError_t launch_xinv1(const Geom& g, const Buffers& b, DevScalars* sc, double* outp, cudaStream_t s) {
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
-        using C = X1Cfg<NX>;
-        cudaError_t e;
-        if ((e = set_smem(k_xinv1<NX, EPI>, C::SMEM)) != cudaSuccess) return e;
-        dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
-        const double hb = 16.0 * (double)g.nz * g.ny * g.nkx;
-        QGN_LAUNCH(KID_XINV1, hb + (EPI == 1 ? 8.0 * (double)g.nz * g.ny * NX : 0.0), s,
-                   k_xinv1<NX, EPI><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, sc, outp, b.twx));
-        return cudaGetLastError();
+        if constexpr (has_narrow<NX>()) {
+            const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * g.nz;
+            const long long cn = (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * g.nz;
+            if (narrow_better(cd, cn)) return xinv1_go<NX, EPI, kNarrowX1>(g, b, sc, outp, s);
+        }
+        return xinv1_go<NX, EPI, 0>(g, b, sc, outp, s);
     });
 }
 
@@ -348,6 +433,74 @@ cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, do
     return launch_xinv1<1>(g, b, nullptr, out, s);
 }
 
+
+// ------------------------------------------------------------------------------------
+// The learned closure's tensors: the network input (scaled physical q, psi as NHWC BF16)
+// straight from the y-inverse's packed rows, and the forward transform of its NHWC output.
+// ------------------------------------------------------------------------------------
+template <int NX, int TV>
+__global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
+    k_xpack(Geom g, const double2* __restrict__ hq_q, const double2* __restrict__ hq_psi,
+            const double2* __restrict__ twx, const float* __restrict__ scale, __nv_bfloat16* __restrict__ xout,
+            int cin_p) {
+    const int field = blockIdx.y / g.nz, l = blockIdx.y % g.nz;
+    xinv1_tile<NX, 2, TV>(g, blockIdx.x, l, field ? hq_psi : hq_q, nullptr, nullptr, twx, scale, xout, cin_p,
+                          field * g.nz + l);
+}
+
+template <int NX, int TV>
+static cudaError_t xpack_go(const Geom& g, const Buffers& b, const float* scale, __nv_bfloat16* xout, int cin_p,
+                            cudaStream_t s) {
+    using C = X1Cfg<NX, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_xpack<NX, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 2 * g.nz);
+    QGN_LAUNCH(KID_XINV1, 2.0 * (16.0 * g.nz * g.ny * g.nkx + 2.0 * g.nz * g.ny * NX), s,
+               k_xpack<NX, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, b.hu, b.twx, scale, xout, cin_p));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
+                                 const float* scale, void* xout, int cin_p, cudaStream_t s) {
+    cudaError_t e = launch_yinv<double2>(g, 2, q, psi, b.hq, nullptr, b.hu, b.twy, s);
+    if (e != cudaSuccess) return e;
+    __nv_bfloat16* x = static_cast<__nv_bfloat16*>(xout);
+    return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
+        constexpr int NX = decltype(NXc)::value;
+        if constexpr (has_narrow<NX>()) {
+            const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * 2 * g.nz;
+            const long long cn =
+                (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * 2 * g.nz;
+            if (narrow_better(cd, cn)) return xpack_go<NX, kNarrowX1>(g, b, scale, x, cin_p, s);
+        }
+        return xpack_go<NX, 0>(g, b, scale, x, cin_p, s);
+    });
+}
+
+cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
+                                  double2* out, cudaStream_t s) {
+    cudaError_t e = dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
+        constexpr int NX = decltype(NXc)::value;
+        using C = X1Cfg<NX>;
+        cudaError_t e2;
+        if ((e2 = set_smem(k_xfwd1<NX, 1>, C::SMEM)) != cudaSuccess) return e2;
+        dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
+        QGN_LAUNCH(KID_XFWD1, 4.0 * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
+                   k_xfwd1<NX, 1><<<grid, C::THREADS, C::SMEM, s>>>(g, nullptr, b.hq, b.twx, y, cout_p, osc));
+        return cudaGetLastError();
+    });
+    if (e != cudaSuccess) return e;
+    return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
+        constexpr int NY = decltype(NYc)::value;
+        using C = YInvCfg<NY>;
+        cudaError_t e2;
+        if ((e2 = set_smem(k_yfwd1<NY>, C::SMEM)) != cudaSuccess) return e2;
+        dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
+        QGN_LAUNCH(KID_YFWD1, 16.0 * (double)g.nz * g.nkx * (NY + g.nky), s,
+                   k_yfwd1<NY><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, out, b.twy));
+        return cudaGetLastError();
+    });
+}
 
 // ------------------------------------------------------------------------------------
 // WriteQPmodal support (QGN_Module.f90:381-440): the reference's Jacobian there is the full,

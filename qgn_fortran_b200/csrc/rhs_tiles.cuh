@@ -8,6 +8,8 @@
 #include "qgn_internal.cuh"
 #include "fft.cuh"
 
+#include <cuda_bf16.h>
+
 namespace qgn {
 
 // ------------------------------------------------------------------------------------
@@ -137,7 +139,7 @@ __device__ __forceinline__ CT pack_hi(CT f1, CT f2) {
 
 // ------------------------------------------------------------------------------------
 // yinv: inverse y transforms of kept columns into packed row pairs.
-// NF = 3: (q -> pq, -i ky psi -> pu, i kx psi -> pv);  NF = 1: (f -> pq).
+// NF = 3: (q -> pq, -i ky psi -> pu, i kx psi -> pv);  NF = 2: (q -> pq, psi -> pu);  NF = 1: (f -> pq).
 // The first radix pass reads the compact column straight from HBM (zeros in the dealiased
 // band); the transformed column stays in shared memory, where a packing loop pairs rows
 // y and y+1 and writes the two packed arrays with TKX-wide coalesced stores.
@@ -167,7 +169,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
             if (!colok || !kept) return cmk<CT>(0.0, 0.0);
             CT v = src[colbase + (j < g.kylo ? j : j - g.kyshift)];
-            if (f == 1) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
+            if (f == 1 && NF == 3) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
                 const RT kyv = (RT)g.kyval(j);
                 v = cmk<CT>(kyv * v.y, -kyv * v.x);
             } else if (f == 2) {   // v_hat = i kx psi_hat  (QGN_Module.f90:224)
@@ -382,9 +384,13 @@ struct X1Cfg {
 };
 
 template <int NX, int EPI, int TV = 0>
+// EPI 2 (the learned closure's input): channel chan of the NHWC BF16 tensor xout with
+// cin_p channels per pixel, grid/(nx*ny) * scale[chan]
 __device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const double2* __restrict__ hq,
                                            DevScalars* __restrict__ sc, double* __restrict__ outp,
-                                           const double2* __restrict__ twx) {
+                                           const double2* __restrict__ twx, const float* __restrict__ scale = nullptr,
+                                           __nv_bfloat16* __restrict__ xout = nullptr, int cin_p = 0,
+                                           int chan = 0) {
     using C = X1Cfg<NX, TV>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = reinterpret_cast<double2*>(sm_raw);
@@ -409,9 +415,14 @@ __device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const do
             const double m1 = fabs(a.x), m2 = fabs(a.y);
             if (!(m1 == m1) || !(m2 == m2)) mx = __longlong_as_double(0x7ff8000000000000LL);
             else if (mx == mx) mx = fmax(mx, fmax(m1, m2));
-        } else {
+        } else if (EPI == 1) {
             outp[prow + x] = a.x * g.inv_nxny;
             outp[prow + NX + x] = a.y * g.inv_nxny;
+        } else {
+            const size_t pix = (size_t)(2 * rp) * NX + x;
+            const float sf = scale[chan];
+            xout[pix * cin_p + chan] = __float2bfloat16_rn((float)(a.x * g.inv_nxny) * sf);
+            xout[(pix + NX) * cin_p + chan] = __float2bfloat16_rn((float)(a.y * g.inv_nxny) * sf);
         }
     };
     fft_fused<NX, +1, SRC_FN, DST_FN>(sm + slot * C::TS, lane, ok, twx, ld, st);

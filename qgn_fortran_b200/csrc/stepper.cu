@@ -84,13 +84,18 @@ __device__ __forceinline__ void point_k(const Geom& g, size_t p, int& kx, int& m
 }
 
 // ---- ARK update + embedded error combination (ARK43_QGLeith.f90:120-134) ---------------------
+// It also clears the scalars of the error transform's max reduction that follows it.
 __global__ void __launch_bounds__(256) k_ark_update(Geom g, StagePtrs sp, const double2* __restrict__ q,
                                                     double2* __restrict__ qnew, double2* __restrict__ err,
                                                     const LayerConst* __restrict__ lc,
-                                                    const DevScalars* __restrict__ sc) {
+                                                    DevScalars* __restrict__ sc) {
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e == 0) {
+        sc->maxbits = 0ULL;
+        sc->accept = 0;
+    }
     if (e >= total) return;
     const int l = (int)(e / P);
     const size_t p = e % P;
@@ -160,6 +165,26 @@ struct CombPtrs {
     const T* Q[6];
 };
 
+// sum_j ae_sj N_j + sum_j ai_sj L_j with L_j = -D q_j, in FP64 (stage S of ARK43_QGLeith.f90:87-118)
+template <int S>
+__device__ __forceinline__ void comb_sum64(const double2* nn, const double2* qq, double2 q0, double D, double& ax,
+                                           double& ay) {
+    ax = 0.0;
+    ay = 0.0;
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        ax += c_ae[S * 6 + j] * nn[j].x;
+        ay += c_ae[S * 6 + j] * nn[j].y;
+    }
+    ax += c_ai[S * 6] * (-D * q0.x);
+    ay += c_ai[S * 6] * (-D * q0.y);
+#pragma unroll
+    for (int j = 1; j < S; ++j) {
+        ax += c_ai[S * 6 + j] * (-D * qq[j].x);
+        ay += c_ai[S * 6 + j] * (-D * qq[j].y);
+    }
+}
+
 template <int S, class T>
 __global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const double2* __restrict__ q,
                                                   T* __restrict__ qout, const LayerConst* __restrict__ lc,
@@ -184,20 +209,7 @@ __global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const 
     const double2 q0 = q[e];
     double ax, ay;
     if constexpr (sizeof(T) == 16) {
-        ax = 0.0;
-        ay = 0.0;
-#pragma unroll
-        for (int j = 0; j < S; ++j) {
-            ax += c_ae[S * 6 + j] * nn[j].x;
-            ay += c_ae[S * 6 + j] * nn[j].y;
-        }
-        ax += c_ai[S * 6] * (-D * q0.x);
-        ay += c_ai[S * 6] * (-D * q0.y);
-#pragma unroll
-        for (int j = 1; j < S; ++j) {
-            ax += c_ai[S * 6 + j] * (-D * qq[j].x);
-            ay += c_ai[S * 6 + j] * (-D * qq[j].y);
-        }
+        comb_sum64<S>(nn, qq, q0, D, ax, ay);
     } else {
         Comp32 cx, cy;
         const float Df = (float)D;
@@ -259,10 +271,14 @@ struct StagePtrs32 {
 __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
                                                           double2* __restrict__ qnew, double2* __restrict__ err,
                                                           const LayerConst* __restrict__ lc,
-                                                          const DevScalars* __restrict__ sc) {
+                                                          DevScalars* __restrict__ sc) {
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e == 0) {   // clears the max reduction of the error transform that follows
+        sc->maxbits = 0ULL;
+        sc->accept = 0;
+    }
     if (e >= total) return;
     const int l = (int)(e / P);
     const size_t p = e % P;
@@ -396,10 +412,19 @@ __device__ __forceinline__ double kpow(double k2) {
 }
 
 template <int POW>
+__device__ __forceinline__ double parseval_block(const Geom& g, const double2* __restrict__ f, int l);
+
+template <int POW>
 __global__ void __launch_bounds__(256) k_parseval(Geom g, const double2* __restrict__ f, double* __restrict__ partial) {
+    const double t = parseval_block<POW>(g, f, blockIdx.y);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+}
+
+// this block's share of sum_k w(k)|F_k|^2 for layer l (valid in thread 0)
+template <int POW>
+__device__ __forceinline__ double parseval_block(const Geom& g, const double2* __restrict__ f, int l) {
     __shared__ double red[8];
     const size_t P = (size_t)g.nkx * g.nky;
-    const int l = blockIdx.y;
     double acc = 0.0;
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
         int kx, m;
@@ -423,11 +448,10 @@ __global__ void __launch_bounds__(256) k_parseval(Geom g, const double2* __restr
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
+    double t = 0.0;
+    if (threadIdx.x == 0)
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        partial[(size_t)l * gridDim.x + blockIdx.x] = t;
-    }
+    return t;
 }
 
 // warp-parallel fixed-order sum of one layer's partials (deterministic)
@@ -439,14 +463,35 @@ __device__ __forceinline__ double layer_sum(const double* __restrict__ partial, 
     return s;
 }
 
-// A8L(k) = (1.3*Lx/(nx*pi))**12 * sqrt(mean(q*d))  with mean(q*d) = S/(nx ny)^2  (ARK43_QGLeith.f90:71-73)
-__global__ void k_leith_final(Geom g, const double* __restrict__ partial, int nblocks, double c12, DevScalars* sc) {
-    const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (l >= g.nz) return;
-    const double s = layer_sum(partial, l, nblocks);
+// QG-Leith in one launch, A8L(k) = (1.3*Lx/(nx*pi))**12 * sqrt(mean(q*d)) with
+// mean(q*d) = S/(nx ny)^2 (ARK43_QGLeith.f90:71-73): each block writes its Parseval partial;
+// the block that finishes last (counted in sc->red_count, reset to 0 after) sums the
+// partials of every layer in a fixed order (deterministic) and writes A8L.
+__global__ void __launch_bounds__(256) k_leith(Geom g, const double2* __restrict__ f, double* __restrict__ partial,
+                                               double c12, DevScalars* __restrict__ sc) {
+    __shared__ unsigned s_last;
+    const int nb = gridDim.x;
+    const double t = parseval_block<4>(g, f, blockIdx.y);
+    if (threadIdx.x == 0) {
+        partial[(size_t)blockIdx.y * nb + blockIdx.x] = t;
+        __threadfence();
+        const unsigned prev = atomicAdd(&sc->red_count, 1u);
+        s_last = (prev + 1 == gridDim.x * gridDim.y) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
     const double N = (double)g.nx * (double)g.ny;
-    if ((threadIdx.x & 31) == 0) sc->A8L[l] = c12 * sqrt((s / N) / N);
+    for (int l = threadIdx.x >> 5; l < g.nz; l += blockDim.x >> 5) {
+        double s = 0.0;
+        for (int b = threadIdx.x & 31; b < nb; b += 32) s += __ldcg(&partial[(size_t)l * nb + b]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0) sc->A8L[l] = c12 * sqrt((s / N) / N);
+    }
+    if (threadIdx.x == 0) sc->red_count = 0u;
 }
+
 
 // layer KE = 0.5 * S/(nx ny)^2 * H_k/Htot with S the k^2-weighted Parseval sum of psi
 __global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nblocks, const double* __restrict__ Hw,
@@ -557,6 +602,75 @@ static cudaError_t launch_comb(const Geom& g, const Buffers& b, int s, cudaStrea
     return cudaGetLastError();
 }
 
+// Stage S on a small grid in one kernel: one thread per kept mode combines every layer (the
+// arithmetic of k_ark_comb) and runs GetPsi on the result, saving the second launch that
+// dominates when the grid is only a few thousand modes per layer.
+template <int S, int NZ>
+__global__ void __launch_bounds__(256, 2) k_ark_stage_small(Geom g, CombPtrs<double2> cp, const double2* __restrict__ q,
+                                                           double2* __restrict__ qout, double2* __restrict__ psi,
+                                                           const LayerConst* __restrict__ lc,
+                                                           const ModalConst* __restrict__ mc,
+                                                           const DevScalars* __restrict__ sc) {
+    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    const int nz = g.nz;
+    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
+    __syncthreads();
+    const size_t P = (size_t)g.nkx * g.nky;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    int kx, m;
+    double k2;
+    point_k(g, p, kx, m, k2);
+    const double k8 = (k2 * k2) * (k2 * k2);
+    const double dt = sc->dt;
+    constexpr int NZC = NZ > 0 ? NZ : kMaxNZ;
+    double2 qv[NZC], pv[NZC];
+#pragma unroll
+    for (int l = 0; l < NZC; ++l) {
+        if (l < nz) {
+            const size_t e = (size_t)l * P + p;
+            const double D = lc->A2 * k2 + sc->A8L[l] * k8;
+            double2 nn[S], qq[S];
+#pragma unroll
+            for (int j = 0; j < S; ++j) nn[j] = cp.N[j][e];
+#pragma unroll
+            for (int j = 1; j < S; ++j) qq[j] = cp.Q[j][e];
+            const double2 q0 = q[e];
+            double ax, ay;
+            comb_sum64<S>(nn, qq, q0, D, ax, ay);
+            const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
+            qv[l] = make_double2(Mq * (q0.x + dt * ax), Mq * (q0.y + dt * ay));
+            qout[e] = qv[l];
+        }
+    }
+    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+#pragma unroll
+    for (int l = 0; l < NZC; ++l)
+        if (l < nz) psi[(size_t)l * P + p] = pv[l];
+}
+
+// grids of at most this many kept mode-layers take the fused stage kernel
+constexpr size_t kSmallStage = (size_t)1 << 17;
+
+template <int NZ>
+static cudaError_t launch_stage_small_nz(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    const CombPtrs<double2> cp = comb_ptrs<double2>(b);
+    const size_t P = (size_t)g.nkx * g.nky;
+    const unsigned nbk = blocks_for(P, 256);
+    const double C = (double)g.csize(), nb = 16.0 * C * (2.0 * s + 2.0);
+    double2* qo = b.Qs[s];
+    switch (s) {
+        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<1, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<2, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<3, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<4, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<5, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, float2* psi, cudaStream_t st) {
     const size_t P = (size_t)g.nkx * g.nky;
     dim3 grid(blocks_for(P, 256));
@@ -573,6 +687,15 @@ cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, f
 
 // stage s of ARK4(3)6L[2]SA: q_s (streaming combination), then psi_s = GetPsi(q_s)
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    if (g.csize() <= kSmallStage) {
+        switch (g.nz) {
+            case 2: return launch_stage_small_nz<2>(g, b, s, st);
+            case 4: return launch_stage_small_nz<4>(g, b, s, st);
+            case 8: return launch_stage_small_nz<8>(g, b, s, st);
+            case 16: return launch_stage_small_nz<16>(g, b, s, st);
+            default: break;   // other layer counts: the two streaming kernels
+        }
+    }
     cudaError_t e = launch_comb<double2>(g, b, s, st);
     if (e != cudaSuccess) return e;
     return launch_modal(g, b.mc, b.Qs[s], b.psi, st);
@@ -664,8 +787,7 @@ static int parseval_blocks(const Geom& g) {
 cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t st) {
     const int nb = parseval_blocks(g);
     QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
-               k_parseval<4><<<dim3(nb, g.nz), 256, 0, st>>>(g, q, b.red));
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_leith_final<<<(g.nz + 7) / 8, 256, 0, st>>>(g, b.red, nb, c12, b.sc));
+               k_leith<<<dim3(nb, g.nz), 256, 0, st>>>(g, q, b.red, c12, b.sc));
     return cudaGetLastError();
 }
 

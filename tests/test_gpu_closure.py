@@ -60,6 +60,29 @@ def test_cnn_forward_matches_oracle(cuda_ok):
     assert rel(y.cpu().numpy(), ref) <= 1e-4
 
 
+@pytest.mark.parametrize("layers", [2, 3])
+def test_tcgen05_and_mma_sync_engines_agree(cuda_ok, layers):
+    """The tcgen05 (TMEM) convolutions and the warp-level mma.sync ones compute the same
+    network; outputs and gradients differ only by FP32 summation order."""
+    import torch
+    net, ws = small_net(seed=13, H=16, layers=layers, max_batch=4)
+    x, t = sample(net, 4, 9)
+    xd, td = to_dev_bf16(x), to_dev_f32(t)
+    outs, grads = [], []
+    for engine in ("mma.sync", "tcgen05"):
+        net.set_engine(engine)
+        y = torch.zeros((4, net.H, net.W, net.cout_p), dtype=torch.float32, device="cuda")
+        net.forward(xd, y, 4)
+        net.check()
+        outs.append(y.cpu().numpy())
+        grads.append(net.gradients(xd, td, 4)[1])
+    assert rel(outs[1], outs[0]) <= 1e-5
+    ref, _, _ = CNNOracle(ws, net.cout).forward(x)
+    assert rel(outs[1], ref) <= 1e-4
+    for (a, _), (b, _) in zip(grads[1], grads[0]):
+        assert rel(a, b) <= 1e-3
+
+
 def test_cnn_gradients_match_oracle(cuda_ok):
     net, ws = small_net(seed=5)
     x, t = sample(net, 2, 2)
