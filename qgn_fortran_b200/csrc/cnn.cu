@@ -375,7 +375,7 @@ __global__ void k_gather(const unsigned char* __restrict__ src, const int* __res
 namespace tc {
 
 constexpr int kPixS = kTileP + 2;        // staged pixels per input row (periodic halo)
-constexpr int kSlots = 4;                // input-row ring
+constexpr int kSlots = 6;                // input-row ring: rows of the tile in flight and the next
 constexpr long long kWaitLimit = 1LL << 22;
 
 constexpr int imax(int a, int b) { return a > b ? a : b; }
@@ -394,8 +394,11 @@ struct Lay {
     static constexpr int B_LAST = W_OFF + (8 * (CIN / 8) + CIN / 8 - 2) * COUT * 16;
     static constexpr int A_END = A_LAST + imax(kPixS * 16 + 15 * 128, 15 * kPixS * 16 + 128) + 128;
     static constexpr int B_END = B_LAST + imax(COUT * 16 + (COUT / 8 - 1) * 128, (COUT / 8 - 1) * COUT * 16 + 128) + 128;
-    static constexpr int SMEM = (imax(BAR_OFF + 64, imax(A_END, B_END)) + 1023) / 1024 * 1024 + 1024;
-    static constexpr int TMEM_COLS = COUT < 32 ? 32 : COUT;   // power of two >= 32
+    static constexpr int OPS_END = (imax(BAR_OFF + 64, imax(A_END, B_END)) + 1023) / 1024 * 1024;
+    static constexpr int STF_OFF = OPS_END;                         // FP32 output staging [128][COUT]
+    static constexpr int STB_OFF = STF_OFF + kTileP * COUT * 4;     // BF16 output staging [128][COUT]
+    static constexpr int SMEM = STB_OFF + kTileP * COUT * 2;
+    static constexpr int TMEM_COLS = COUT < 32 ? 64 : 2 * COUT;   // two accumulator tiles, power of two
 };
 
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -469,6 +472,74 @@ __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, i
 
 }  // namespace tc
 
+// Epilogue of one tile: warp w reads TMEM lanes 32 (w % 4).. (one pixel per thread) and a block
+// of columns, applies bias + GELU (or GELU' for the backward pass), and writes the tile through
+// XOR-swizzled shared-memory staging so that the global stores are contiguous 16-byte pieces.
+// The tile's outputs are contiguous in global memory: pixels p0 .. p0+127, COUT channels each.
+template <int CIN, int COUT, int EPI>
+__device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const float* breg,
+                                                 float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
+                                                 const float* __restrict__ zin, unsigned char* stf, unsigned char* stb) {
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    constexpr int NCOL = COUT == 64 ? 32 : 16;
+    constexpr int CF = COUT / 4;        // 16-byte pieces per staged FP32 row
+    constexpr int CB = COUT / 8;        // 16-byte pieces per staged BF16 row
+    const bool reads = COUT == 64 || warp < 4;
+    const int px = 32 * (warp % 4) + lane;
+    const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+    if (EPI == EPI_GELU_GRAD) {   // the tile's pre-activations, read contiguously
+        for (int i = threadIdx.x; i < kTileP * CF; i += kThreads) {
+            const int r = i / CF, c = i % CF;
+            *reinterpret_cast<float4*>(stf + (r * CF + (c ^ (r % CF))) * 16) =
+                *reinterpret_cast<const float4*>(zin + (p0 + r) * COUT + c * 4);
+        }
+        __syncthreads();
+    }
+    if (reads) {
+        float v[NCOL];
+        tc::tmem_ld<NCOL>(tacc + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)n0, v);
+#pragma unroll
+        for (int j = 0; j < NCOL; j += 4) {
+            const int c = (n0 + j) / 4;
+            float4* fz = reinterpret_cast<float4*>(stf + (px * CF + (c ^ (px % CF))) * 16);
+            uint2* fb = reinterpret_cast<uint2*>(stb + (px * CB + (((n0 + j) / 8) ^ (px % CB))) * 16 + ((n0 + j) % 8) * 2);
+            if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+                const float4 z = make_float4(v[j] + breg[j], v[j + 1] + breg[j + 1], v[j + 2] + breg[j + 2],
+                                             v[j + 3] + breg[j + 3]);
+                *fz = z;
+                if (EPI == EPI_GELU) {
+                    __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(gelu(z.x), gelu(z.y)),
+                                            __floats2bfloat162_rn(gelu(z.z), gelu(z.w))};
+                    *fb = *reinterpret_cast<const uint2*>(g2);
+                }
+            } else {
+                const float4 z = *fz;
+                __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(v[j] * gelu_grad(z.x), v[j + 1] * gelu_grad(z.y)),
+                                        __floats2bfloat162_rn(v[j + 2] * gelu_grad(z.z), v[j + 3] * gelu_grad(z.w))};
+                *fb = *reinterpret_cast<const uint2*>(g2);
+            }
+        }
+    }
+    __syncthreads();
+    if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+        for (int i = threadIdx.x; i < kTileP * CF; i += kThreads) {
+            const int r = i / CF, c = i % CF;
+            *reinterpret_cast<float4*>(outf + (p0 + r) * COUT + c * 4) =
+                *reinterpret_cast<const float4*>(stf + (r * CF + (c ^ (r % CF))) * 16);
+        }
+    }
+    if (EPI == EPI_GELU || EPI == EPI_GELU_GRAD) {
+        for (int i = threadIdx.x; i < kTileP * CB; i += kThreads) {
+            const int r = i / CB, c = i % CB;
+            *reinterpret_cast<uint4*>(outb + (p0 + r) * COUT + c * 8) =
+                *reinterpret_cast<const uint4*>(stb + (r * CB + (c ^ (r % CB))) * 16);
+        }
+    }
+}
+
+// Pipelined over the CTA's tiles: the MMAs of tile t run into TMEM buffer t&1 while the
+// epilogue drains tile t-1 from the other buffer, and the next tile's new input row is fetched
+// meanwhile.  Input rows live in a 6-slot ring.
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kThreads, 1)
     k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
@@ -476,10 +547,11 @@ __global__ void __launch_bounds__(kThreads, 1)
               const float* __restrict__ zin, int* __restrict__ err) {
     using L = tc::Lay<CIN, COUT>;
     static_assert(COUT == 16 || COUT == 64, "N of the MMA");
+    constexpr int NACC = COUT < 32 ? 32 : COUT;           // TMEM columns per accumulator tile
     extern __shared__ __align__(1024) unsigned char smtc[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smtc + L::BAR_OFF);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(smtc + L::BAR_OFF + 16);
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smtc + L::BAR_OFF);   // bar[0], bar[1]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smtc + L::BAR_OFF + 32);
+    const int warp = threadIdx.x / 32;
     const uint32_t bar_a = smem_u32(bar), in_a = smem_u32(smtc), w_a = smem_u32(smtc + L::W_OFF);
 
     // this CTA's tiles: a contiguous range of t = ((b * segs + seg) * H + h), rows fastest
@@ -495,6 +567,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a + 8));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += kThreads) {
@@ -506,111 +579,126 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *tslot;
+    unsigned char* stf = smtc + L::STF_OFF;
+    unsigned char* stb = smtc + L::STB_OFF;
+    // this thread's bias values (its columns are the same in every tile)
+    float breg[COUT == 64 ? 32 : 16];
+    {
+        constexpr int NCOL = COUT == 64 ? 32 : 16;
+        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+#pragma unroll
+        for (int j = 0; j < NCOL; ++j) breg[j] = (EPI == EPI_GELU_GRAD) ? 0.f : bias[n0 + j];
+    }
+    // descriptors without their start address; per MMA the address is added in
+    const uint64_t da0 = tc::sdesc(0u, tc::kPixS * 16, 128), db0 = tc::sdesc(0u, COUT * 16, 128);
 
-    // ring bookkeeping (uniform across the CTA): key of the row in each slot, -1 = empty;
-    // key = (b * segs + seg) * H + hh
-    int key[tc::kSlots] = {-1, -1, -1, -1};
-    uint32_t phase = 0;
-    for (int t = t0; t < t1; ++t) {
+    // Ring slots are handed out round-robin, so the last six rows fetched sit in distinct slots.
+    // A tile that continues the previous one (same image and segment, next row) reuses two of
+    // its rows and needs one new row, usually prefetched during the previous tile; otherwise
+    // all three rows are fetched.  Live rows (previous tile, this tile, the prefetch) are at
+    // most the last five fetched, so no slot that an MMA in flight reads is overwritten.
+    int next_slot = 0;
+    int sl[3] = {0, 0, 0};                  // this tile's slots (rows h-1, h, h+1)
+    int pre_slot = -1;                      // slot of the row prefetched for this tile, or -1
+    int pbs = -1;
+    uint32_t phase[2] = {0u, 0u};
+    int pb = 0, ph = 0, pw0 = 0;            // coordinates of the previous tile
+    bool failed = false;
+    for (int t = t0; t < t1 && !failed; ++t) {
         const int h = t % H, bs = t / H;
         const int seg = bs % segs, b = bs / segs;
         const int w0 = seg * kTileP;
-        int need[3], slot[3];
-        for (int k = 0; k < 3; ++k) {
-            need[k] = bs * H + (h + k - 1 + H) % H;
-            slot[k] = -1;
-            for (int sI = 0; sI < tc::kSlots; ++sI)
-                if (key[sI] == need[k]) slot[k] = sI;
-        }
-        for (int k = 0; k < 3; ++k) {
-            if (slot[k] >= 0) continue;
-            int free_slot = -1;
-            for (int sI = 0; sI < tc::kSlots && free_slot < 0; ++sI) {
-                bool used = false;
-                for (int j = 0; j < 3; ++j) used = used || (slot[j] == sI);
-                if (!used) free_slot = sI;
+        const bool cont = t > t0 && bs == pbs && h == ph + 1 && H >= 3;
+        if (cont) {
+            sl[0] = sl[1];
+            sl[1] = sl[2];
+            if (pre_slot >= 0) {
+                sl[2] = pre_slot;
+            } else {
+                sl[2] = next_slot;
+                next_slot = (next_slot + 1) % tc::kSlots;
+                tc::fetch_row<CIN>(x, b, (h + 1) % H, H, W, w0, in_a + (uint32_t)(sl[2] * L::SLOT_BYTES));
             }
-            slot[k] = free_slot;
-            key[free_slot] = need[k];
-            tc::fetch_row<CIN>(x, b, need[k] - bs * H, H, W, w0, in_a + (uint32_t)(free_slot * L::SLOT_BYTES));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sl[k] = next_slot;
+                next_slot = (next_slot + 1) % tc::kSlots;
+                tc::fetch_row<CIN>(x, b, (h + k - 1 + H) % H, H, W, w0, in_a + (uint32_t)(sl[k] * L::SLOT_BYTES));
+            }
         }
+        pre_slot = -1;
         tc::cp_commit();
         tc::cp_wait_all();
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
+        const int buf = (t - t0) & 1;
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            uint32_t acc = 0;
-#pragma unroll 1
+            const uint32_t dacc = tmem + (uint32_t)(buf * NACC);
+            const uint32_t ra[3] = {in_a + (uint32_t)(sl[0] * L::SLOT_BYTES), in_a + (uint32_t)(sl[1] * L::SLOT_BYTES),
+                                    in_a + (uint32_t)(sl[2] * L::SLOT_BYTES)};
+#pragma unroll
             for (int tap = 0; tap < 9; ++tap) {
-                const int dh = tap / 3, dw = tap % 3;
-                const uint32_t row_a = in_a + (uint32_t)(slot[dh] * L::SLOT_BYTES);
 #pragma unroll
                 for (int kc = 0; kc < CIN / 16; ++kc) {
-                    const uint32_t a_addr = row_a + (uint32_t)((2 * kc * tc::kPixS + dw) * 16);
+                    const uint32_t a_addr = ra[tap / 3] + (uint32_t)((2 * kc * tc::kPixS + tap % 3) * 16);
                     const uint32_t b_addr = w_a + (uint32_t)((tap * (CIN / 8) + 2 * kc) * COUT * 16);
-                    tc::mma(tmem, tc::sdesc(a_addr, tc::kPixS * 16, 128), tc::sdesc(b_addr, COUT * 16, 128),
-                            tc::idesc<COUT>(), acc);
-                    acc = 1;
+                    tc::mma(dacc, da0 | (uint64_t)((a_addr >> 4) & 0x3FFFu), db0 | (uint64_t)((b_addr >> 4) & 0x3FFFu),
+                            tc::idesc<COUT>(), (tap | kc) ? 1u : 0u);
                 }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_a)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             bar_a + 8u * (uint32_t)buf)
                          : "memory");
         }
-        // prefetch the next tile's new row into the slot this tile does not read
-        if (t + 1 < t1) {
-            const int hn = (t + 1) % H, bsn = (t + 1) / H;
-            const int needn = bsn * H + (hn + 1) % H;
-            bool have = false;
-            for (int sI = 0; sI < tc::kSlots; ++sI) have = have || (key[sI] == needn);
-            if (!have && bsn == bs) {
-                int free_slot = -1;
-                for (int sI = 0; sI < tc::kSlots && free_slot < 0; ++sI)
-                    if (sI != slot[0] && sI != slot[1] && sI != slot[2]) free_slot = sI;
-                key[free_slot] = needn;
-                tc::fetch_row<CIN>(x, b, needn - bsn * H, H, W, (bsn % segs) * kTileP,
-                                   in_a + (uint32_t)(free_slot * L::SLOT_BYTES));
-                tc::cp_commit();
-            }
+        // the next tile's new row, if it continues this one.  Only when this tile continued the
+        // previous one (or is the first): after a fresh three-row fetch the six slots hold the
+        // previous tile's rows, whose MMAs may still be running, and this tile's.
+        if ((cont || t == t0) && t + 1 < t1 && (t + 1) / H == bs && h + 1 < H && H >= 3) {
+            pre_slot = next_slot;
+            next_slot = (next_slot + 1) % tc::kSlots;
+            tc::fetch_row<CIN>(x, b, (h + 2) % H, H, W, w0, in_a + (uint32_t)(pre_slot * L::SLOT_BYTES));
+            tc::cp_commit();
         }
-        const bool ok = tc::bar_wait(bar_a, phase);
-        phase ^= 1u;
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(err, 1);
-            tc::bar_wait(bar_a, phase ^ 1u);   // once more for the MMAs in flight
-            break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        // epilogue: warp w reads TMEM lanes 32 (w % 4).. (pixels) and a block of columns
-        constexpr int NCOL = COUT == 64 ? 32 : 16;
-        if (COUT == 64 || warp < 4) {
-            const int px = 32 * (warp % 4) + lane;
-            const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
-            float v[NCOL];
-            tc::tmem_ld<NCOL>(tmem + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)n0, v);
-            const size_t p = ((size_t)b * H + h) * W + w0 + px;
-#pragma unroll
-            for (int j = 0; j < NCOL; j += 4) {
-                const int n = n0 + j;
-                if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
-                    const float4 bb = *reinterpret_cast<const float4*>(bias + n);
-                    const float4 z = make_float4(v[j] + bb.x, v[j + 1] + bb.y, v[j + 2] + bb.z, v[j + 3] + bb.w);
-                    *reinterpret_cast<float4*>(outf + p * COUT + n) = z;
-                    if (EPI == EPI_GELU) {
-                        __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(gelu(z.x), gelu(z.y)),
-                                                __floats2bfloat162_rn(gelu(z.z), gelu(z.w))};
-                        *reinterpret_cast<uint2*>(outb + p * COUT + n) = *reinterpret_cast<const uint2*>(g2);
-                    }
-                } else {
-                    const float4 z = *reinterpret_cast<const float4*>(zin + p * COUT + n);
-                    __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(v[j] * gelu_grad(z.x), v[j + 1] * gelu_grad(z.y)),
-                                            __floats2bfloat162_rn(v[j + 2] * gelu_grad(z.z), v[j + 3] * gelu_grad(z.w))};
-                    *reinterpret_cast<uint2*>(outb + p * COUT + n) = *reinterpret_cast<const uint2*>(g2);
-                }
+        // drain the previous tile while this one's MMAs run
+        if (t > t0) {
+            const int pbuf = buf ^ 1;
+            const bool ok = tc::bar_wait(bar_a + 8u * (uint32_t)pbuf, phase[pbuf]);
+            phase[pbuf] ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicOr(err, 1);
+                failed = true;
+            } else {
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(pbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
+                                                 outf, outb, zin, stf, stb);
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();   // TMEM read and ring slots released before the next tile's MMAs
+        __syncthreads();   // the drained buffer and the previous tile's slots are free again
+        pbs = bs;
+        pb = b;
+        ph = h;
+        pw0 = w0;
+    }
+    // the last tile
+    if (t1 > t0 && !failed) {
+        const int lbuf = (t1 - 1 - t0) & 1;
+        const bool ok = tc::bar_wait(bar_a + 8u * (uint32_t)lbuf, phase[lbuf]);
+        phase[lbuf] ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(err, 1);
+            failed = true;
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(lbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
+                                             outf, outb, zin, stf, stb);
+        }
+    }
+    if (failed) {   // once more, bounded, for MMAs still in flight, before the TMEM is freed
+        tc::bar_wait(bar_a, phase[0]);
+        tc::bar_wait(bar_a + 8u, phase[1]);
     }
     tc::cp_wait_all();
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
