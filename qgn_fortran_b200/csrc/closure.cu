@@ -43,7 +43,7 @@ struct Closure {
     qgn_cnn* net = nullptr;
     float* scales = nullptr;          // device: in [2 nz], out [nz]
     __nv_bfloat16* x = nullptr;       // [ny][nx][cin_p]
-    float* y = nullptr;               // [ny][nx][cout_p]
+    float* y = nullptr;               // [cout_p][ny*nx] (planar network output)
     double2* S = nullptr;             // compact closure tendency
     double* red = nullptr;            // 3 x nblocks partial sums
     double* flag = nullptr;           // 1 passing, 0 fallback
@@ -244,7 +244,7 @@ int closure_eval(qgn_ctx* ctx) {
     const Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
     if (launch_closure_input(g, b, b.q, b.psi, c->scales, c->x, c->cin_p, st) != cudaSuccess) return QGN_ERR_CUDA;
-    if (cnn::infer(c->net, c->x, c->y, 1, st) != QGN_OK) return QGN_ERR_CUDA;
+    if (cnn::infer(c->net, c->x, c->y, 1, st, true) != QGN_OK) return QGN_ERR_CUDA;   // planar output
     if (launch_closure_output(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->S, st) != cudaSuccess)
         return QGN_ERR_CUDA;
     const int nb = (int)std::min<size_t>(((size_t)g.nkx * g.nky + 255) / 256, (size_t)c->nblocks);

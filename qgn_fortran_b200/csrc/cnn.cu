@@ -40,7 +40,9 @@ constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kWChunkRows = 16;      // image rows per weight-gradient partial
 
-enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELU_GRAD = 2 };
+// EPI_PLANAR: as EPI_LINEAR but the FP32 output is planar, out[n][pixel] (the closure's input
+// to its forward transform)
+enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELU_GRAD = 2, EPI_PLANAR = 3 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -160,7 +162,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int half = 0; half < 2; ++half) {
                 const size_t p = prow0 + g + 8 * half;
                 float v0 = acc[j][2 * half], v1 = acc[j][2 * half + 1];
-                if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+                if (EPI == EPI_PLANAR) {
+                    const size_t np = (size_t)B * H * W;
+                    outf[(size_t)n * np + p] = v0 + bias[n];
+                    outf[(size_t)(n + 1) * np + p] = v1 + bias[n + 1];
+                } else if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
                     v0 += bias[n];
                     v1 += bias[n + 1];
                     *reinterpret_cast<float2*>(outf + p * COUT + n) = make_float2(v0, v1);
@@ -479,7 +485,8 @@ __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, i
 template <int CIN, int COUT, int EPI>
 __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const float* breg,
                                                  float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
-                                                 const float* __restrict__ zin, unsigned char* stf, unsigned char* stb) {
+                                                 const float* __restrict__ zin, unsigned char* stf, unsigned char* stb,
+                                                 size_t npix) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     constexpr int NCOL = COUT == 64 ? 32 : 16;
     constexpr int CF = COUT / 4;        // 16-byte pieces per staged FP32 row
@@ -503,7 +510,7 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
             const int c = (n0 + j) / 4;
             float4* fz = reinterpret_cast<float4*>(stf + (px * CF + (c ^ (px % CF))) * 16);
             uint2* fb = reinterpret_cast<uint2*>(stb + (px * CB + (((n0 + j) / 8) ^ (px % CB))) * 16 + ((n0 + j) % 8) * 2);
-            if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
+            if (EPI == EPI_GELU || EPI == EPI_LINEAR || EPI == EPI_PLANAR) {
                 const float4 z = make_float4(v[j] + breg[j], v[j + 1] + breg[j + 1], v[j + 2] + breg[j + 2],
                                              v[j + 3] + breg[j + 3]);
                 *fz = z;
@@ -526,6 +533,14 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
             const int r = i / CF, c = i % CF;
             *reinterpret_cast<float4*>(outf + (p0 + r) * COUT + c * 4) =
                 *reinterpret_cast<const float4*>(stf + (r * CF + (c ^ (r % CF))) * 16);
+        }
+    }
+    if (EPI == EPI_PLANAR) {   // out[n][p0 + r]: each channel's 128 pixels are contiguous
+        for (int i = threadIdx.x; i < COUT * kTileP; i += kThreads) {
+            const int n = i / kTileP, r = i % kTileP;
+            const int c = n / 4;
+            outf[(size_t)n * npix + p0 + r] =
+                reinterpret_cast<const float*>(stf + (r * CF + (c ^ (r % CF))) * 16)[n % 4];
         }
     }
     if (EPI == EPI_GELU || EPI == EPI_GELU_GRAD) {
@@ -672,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             } else {
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(pbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
-                                                 outf, outb, zin, stf, stb);
+                                                 outf, outb, zin, stf, stb, (size_t)B * H * W);
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -693,7 +708,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(lbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
-                                             outf, outb, zin, stf, stb);
+                                             outf, outb, zin, stf, stb, (size_t)B * H * W);
         }
     }
     if (failed) {   // once more, bounded, for MMAs still in flight, before the TMEM is freed
@@ -844,12 +859,15 @@ cudaError_t launch_wgrad(qgn_cnn* n, int cin, int cout, const __nv_bfloat16* x, 
 
 // forward of a batch: layer 0 reads x0 (default act[0]); the last layer's FP32 output goes
 // to ylast (default z[L-1])
-int forward(qgn_cnn* net, int batch, const __nv_bfloat16* x0 = nullptr, float* ylast = nullptr) {
+int forward(qgn_cnn* net, int batch, const __nv_bfloat16* x0 = nullptr, float* ylast = nullptr, bool planar = false) {
     const int L = net->layers;
     for (int l = 0; l < L; ++l) {
         const bool last = l == L - 1;
         const __nv_bfloat16* in = (l == 0 && x0) ? x0 : net->act[l];
-        cudaError_t e = last ? launch_conv<EPI_LINEAR>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l],
+        cudaError_t e = (last && planar)
+                            ? launch_conv<EPI_PLANAR>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l], batch,
+                                                      ylast ? ylast : net->z[l], nullptr, nullptr)
+                        : last ? launch_conv<EPI_LINEAR>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l],
                                                        batch, ylast ? ylast : net->z[l], nullptr, nullptr)
                              : launch_conv<EPI_GELU>(net, net->ci[l], net->co[l], in, net->wf[l], net->bias[l],
                                                      batch, net->z[l], net->act[l + 1], nullptr);
@@ -922,11 +940,11 @@ int padded_out(const qgn_cnn* net) { return net->co[net->layers - 1]; }
 int height(const qgn_cnn* net) { return net->H; }
 int width(const qgn_cnn* net) { return net->W; }
 int real_out(const qgn_cnn* net) { return net->cout; }
-int infer(qgn_cnn* net, const void* x, float* y, int batch, cudaStream_t stream) {
+int infer(qgn_cnn* net, const void* x, float* y, int batch, cudaStream_t stream, bool planar) {
     if (batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
     cudaStream_t own = net->stream;
     net->stream = stream;
-    const int rc = forward(net, batch, static_cast<const __nv_bfloat16*>(x), y);
+    const int rc = forward(net, batch, static_cast<const __nv_bfloat16*>(x), y, planar);
     net->stream = own;
     return rc;
 }
@@ -1065,7 +1083,7 @@ int qgn_cnn_set_weights(qgn_cnn* net, const float* host) {
 // Runs on `stream` (NULL: the network's own stream), ordered after the caller's work there.
 int qgn_cnn_forward(qgn_cnn* net, const void* x, float* y, int batch, void* stream) {
     if (!net || !x || !y || batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
-    return qgn::cnn::infer(net, x, y, batch, stream ? static_cast<cudaStream_t>(stream) : net->stream);
+    return qgn::cnn::infer(net, x, y, batch, stream ? static_cast<cudaStream_t>(stream) : net->stream, false);
 }
 
 // gradients of the MSE loss at the current weights for x (BF16 [batch][H][W][cin_p]) and

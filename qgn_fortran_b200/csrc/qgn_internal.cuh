@@ -135,7 +135,7 @@ namespace qgn {
 
 // the learned closure's tensors (rhs_kernels.cu): xout = NHWC BF16 [ny][nx][cin_p] with
 // channels (q_0..q_nz-1, psi_0..psi_nz-1) * scale; out = forward transform (compact, dealiased)
-// of channel l of the NHWC FP32 y divided by osc[l].  Both use b.hq/b.hu as scratch.
+// of channel l of the planar FP32 y[channel][ny*nx] divided by osc[l].  Both use b.hq/b.hu as scratch.
 cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
                                  const float* scale, void* xout, int cin_p, cudaStream_t s);
 cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,

@@ -56,11 +56,15 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __re
 // Single-field launches of the tile bodies (rhs_tiles.cuh): one CTA per tile, tile = blockIdx
 // ------------------------------------------------------------------------------------
 // TV selects a tile width (0: the default; see the configs in rhs_tiles.cuh)
+// with more than one field, the narrow variants spread the fields over CTAs (blockIdx.z)
 template <int NY, int NF, class CT, int TV = 0>
 __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, regcap<CT>()))
     k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
            CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
-    yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy);
+    if (TV != 0 && NF > 1)
+        yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy, blockIdx.z, blockIdx.z + 1);
+    else
+        yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy);
 }
 
 template <int NX, bool DRAG, class CT, int TV = 0>
@@ -104,13 +108,13 @@ static bool narrow_better(long long ctas_default, long long ctas_narrow) {
 // QGN_Module.f90:179-183): r2c of row pairs packed as r1 + i r2, then forward y columns
 // keeping the dealiased modes only.
 // ------------------------------------------------------------------------------------
-// SRC 0: physical field phys[nz][ny][nx]; SRC 1: channel l of the NHWC FP32 tensor y (cout_p
-// channels per pixel) divided by osc[l] (the learned closure's output)
-template <int NX, int SRC = 0>
-__global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
+// SRC 0: physical field phys[nz][ny][nx]; SRC 1: channel l of the planar FP32 tensor
+// y[channel][ny*nx] divided by osc[l] (the learned closure's output)
+template <int NX, int SRC = 0, int TV = 0>
+__global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
     k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx,
             const float* __restrict__ y = nullptr, int cout_p = 0, const float* __restrict__ osc = nullptr) {
-    using C = X1Cfg<NX>;
+    using C = X1Cfg<NX, TV>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = reinterpret_cast<double2*>(sm_raw);
     const int tid = threadIdx.x;
@@ -122,8 +126,9 @@ __global__ void __launch_bounds__(X1Cfg<NX>::THREADS, minb(X1Cfg<NX>::THREADS))
     auto ld = [&](int x) -> double2 {
         if (SRC == 0) return make_double2(phys[prow + x], phys[prow + NX + x]);
         const size_t pix = (size_t)(2 * rp) * NX + x;
+        const float* yl = y + (size_t)l * g.ny * NX;
         const double inv = (double)osc[l];
-        return make_double2((double)y[pix * cout_p + l] / inv, (double)y[(pix + NX) * cout_p + l] / inv);
+        return make_double2((double)yl[pix] / inv, (double)yl[pix + NX] / inv);
     };
     NoIO none;
     fft_fused<NX, -1, SRC_FN, DST_SMEM>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
@@ -219,7 +224,7 @@ static cudaError_t yinv_go(const Geom& g, const CT* q, const CT* psi, CT* hq, CT
     using C = YInvCfg<NY, CT, TV>;
     cudaError_t e;
     if ((e = set_smem(k_yinv<NY, NF, CT, TV>, C::SMEM)) != cudaSuccess) return e;
-    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
+    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz, (TV != 0 && NF > 1) ? NF : 1);
     const double es = (double)sizeof(CT);
     const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
     QGN_LAUNCH(KID_YINV, NF == 3 ? 2.0 * Cb + 3.0 * Hb : NF * (Cb + Hb), s,
@@ -403,17 +408,35 @@ cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f
     return launch_xinv1<0>(g, b, sc, nullptr, s);
 }
 
-cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys, double2* out, cudaStream_t s) {
-    cudaError_t e = dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
+template <int NX, int SRC, int TV>
+static cudaError_t xfwd1_go(const Geom& g, const Buffers& b, const double* phys, const float* y, int cout_p,
+                            const float* osc, cudaStream_t s) {
+    using C = X1Cfg<NX, TV>;
+    cudaError_t e;
+    if ((e = set_smem(k_xfwd1<NX, SRC, TV>, C::SMEM)) != cudaSuccess) return e;
+    dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
+    QGN_LAUNCH(KID_XFWD1, (SRC ? 4.0 : 8.0) * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
+               k_xfwd1<NX, SRC, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, phys, b.hq, b.twx, y, cout_p, osc));
+    return cudaGetLastError();
+}
+
+// forward x transform of a physical field (SRC 0) or of the closure's NHWC output (SRC 1)
+template <int SRC>
+static cudaError_t launch_xfwd1(const Geom& g, const Buffers& b, const double* phys, const float* y, int cout_p,
+                                const float* osc, cudaStream_t s) {
+    return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
-        using C = X1Cfg<NX>;
-        cudaError_t e2;
-        if ((e2 = set_smem(k_xfwd1<NX>, C::SMEM)) != cudaSuccess) return e2;
-        dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
-        QGN_LAUNCH(KID_XFWD1, 8.0 * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
-                   k_xfwd1<NX><<<grid, C::THREADS, C::SMEM, s>>>(g, phys, b.hq, b.twx));
-        return cudaGetLastError();
+        if constexpr (has_narrow<NX>()) {
+            const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * g.nz;
+            const long long cn = (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * g.nz;
+            if (narrow_better(cd, cn)) return xfwd1_go<NX, SRC, kNarrowX1>(g, b, phys, y, cout_p, osc, s);
+        }
+        return xfwd1_go<NX, SRC, 0>(g, b, phys, y, cout_p, osc, s);
     });
+}
+
+cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys, double2* out, cudaStream_t s) {
+    cudaError_t e = launch_xfwd1<0>(g, b, phys, nullptr, 0, nullptr, s);
     if (e != cudaSuccess) return e;
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
@@ -479,16 +502,7 @@ cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2*
 
 cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
                                   double2* out, cudaStream_t s) {
-    cudaError_t e = dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
-        constexpr int NX = decltype(NXc)::value;
-        using C = X1Cfg<NX>;
-        cudaError_t e2;
-        if ((e2 = set_smem(k_xfwd1<NX, 1>, C::SMEM)) != cudaSuccess) return e2;
-        dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
-        QGN_LAUNCH(KID_XFWD1, 4.0 * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
-                   k_xfwd1<NX, 1><<<grid, C::THREADS, C::SMEM, s>>>(g, nullptr, b.hq, b.twx, y, cout_p, osc));
-        return cudaGetLastError();
-    });
+    cudaError_t e = launch_xfwd1<1>(g, b, nullptr, y, cout_p, osc, s);
     if (e != cudaSuccess) return e;
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;

@@ -145,9 +145,12 @@ __device__ __forceinline__ CT pack_hi(CT f1, CT f2) {
 // y and y+1 and writes the two packed arrays with TKX-wide coalesced stores.
 // ------------------------------------------------------------------------------------
 template <int NY, int NF, class CT, int TV = 0>
+// f_begin/f_end: the fields this CTA transforms (all NF by default; one each when a launch
+// spreads the fields over CTAs)
 __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT* __restrict__ q,
                                           const CT* __restrict__ psi, CT* __restrict__ pq, CT* __restrict__ pv,
-                                          CT* __restrict__ pu, const CT* __restrict__ twy) {
+                                          CT* __restrict__ pu, const CT* __restrict__ twy, int f_begin = 0,
+                                          int f_end = NF) {
     using C = YInvCfg<NY, CT, TV>;
     using RT = typename CTraits<CT>::R;
     extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -162,7 +165,9 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
     CT* xs = sm + slot * C::TS;
     NoIOT<CT> none;
 #pragma unroll
+#pragma unroll
     for (int f = 0; f < NF; ++f) {
+        if (f < f_begin || f >= f_end) continue;
         const CT* src = (f == 0) ? q : psi;
         CT* dst = (f == 0) ? pq : (f == 1 ? pu : pv);
         auto ld = [&](int j) -> CT {
@@ -191,7 +196,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             row[k] = ok ? pack_lo(f1, f2, k == 0 || 2 * k == g.nx) : cmk<CT>(0.0, 0.0);
             row[g.nkxp + k] = (ok && k > 0) ? pack_hi(f1, f2) : cmk<CT>(0.0, 0.0);
         }
-        if (f + 1 < NF) __syncthreads();   // the next field's first pass reuses the slots
+        if (f + 1 < f_end) __syncthreads();   // the next field's first pass reuses the slots
     }
 }
 
