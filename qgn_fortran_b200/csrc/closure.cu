@@ -59,6 +59,7 @@ constexpr int kBudgetBlocks = 148;
 // sharp spectral cutoff: coarse compact <- fine compact on the coarse grid's kept modes,
 // rescaled for the unnormalised transforms
 __global__ void k_truncate(Geom gf, Geom gc, const double2* __restrict__ src, double2* __restrict__ dst, double scale) {
+    QGN_PDL_ENTRY();
     const size_t n = gc.csize();
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int m = (int)(e % gc.nky);
@@ -74,6 +75,7 @@ __global__ void k_truncate(Geom gf, Geom gc, const double2* __restrict__ src, do
 }
 
 __global__ void k_copy_time(const DevScalars* __restrict__ a, DevScalars* __restrict__ b) {
+    QGN_PDL_ENTRY();
     b->t = a->t;
     b->dt = a->dt;
     b->halt = 0;
@@ -82,6 +84,7 @@ __global__ void k_copy_time(const DevScalars* __restrict__ a, DevScalars* __rest
 }
 
 __global__ void k_sub(size_t n, const double2* __restrict__ a, const double2* __restrict__ b, double2* __restrict__ o) {
+    QGN_PDL_ENTRY();
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
         o[e] = make_double2(a[e].x - b[e].x, a[e].y - b[e].y);
 }
@@ -89,6 +92,7 @@ __global__ void k_sub(size_t n, const double2* __restrict__ a, const double2* __
 // network input x[p][c]: c < nz -> q_c, nz <= c < 2 nz -> psi_{c-nz}, scaled; zeros beyond
 __global__ void k_pack_in(int nz, size_t npix, const double* __restrict__ q, const double* __restrict__ psi,
                           const float* __restrict__ sc, int cin_p, __nv_bfloat16* __restrict__ x) {
+    QGN_PDL_ENTRY();
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
         __nv_bfloat16* xp = x + p * cin_p;
         for (int c = 0; c < cin_p; ++c) {
@@ -103,6 +107,7 @@ __global__ void k_pack_in(int nz, size_t npix, const double* __restrict__ q, con
 // training target y[p][c] = S_c * out_scale_c (c < nz), zeros beyond
 __global__ void k_pack_out(int nz, size_t npix, const double* __restrict__ s, const float* __restrict__ osc, int cout_p,
                            float* __restrict__ y) {
+    QGN_PDL_ENTRY();
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x)
         for (int c = 0; c < cout_p; ++c) y[p * cout_p + c] = c < nz ? (float)s[(size_t)c * npix + p] * osc[c] : 0.f;
 }
@@ -130,6 +135,7 @@ __global__ void __launch_bounds__(256) k_budget_spec(Geom g, const double2* __re
                                                      const double* __restrict__ Hw, double* __restrict__ red,
                                                      double A8bg, double elimit, DevScalars* __restrict__ sc,
                                                      ClosureStats* __restrict__ st, double* __restrict__ flag) {
+    QGN_PDL_ENTRY();
     __shared__ double sm[3][8];
     __shared__ unsigned s_last;
     const size_t P = (size_t)g.nkx * g.nky;
@@ -222,7 +228,7 @@ int grid_of(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); 
 cudaError_t coarse_grain_on(const qgn_ctx* fine, qgn_ctx* coarse, const double2* src, double2* dst, cudaStream_t s) {
     const double scale = ((double)coarse->g.nx * coarse->g.ny) / ((double)fine->g.nx * fine->g.ny);
     QGN_LAUNCH(KID_LAYOUT, 32.0 * (double)coarse->g.csize(), s,
-               k_truncate<<<grid_of(coarse->g.csize()), 256, 0, s>>>(fine->g, coarse->g, src, dst, scale));
+               ::qgn::launch(k_truncate, grid_of(coarse->g.csize()), 256, 0, s, fine->g, coarse->g, src, dst, scale));
     return cudaGetLastError();
 }
 
@@ -249,7 +255,7 @@ int closure_eval(qgn_ctx* ctx) {
         return QGN_ERR_CUDA;
     const int nb = (int)std::min<size_t>(((size_t)g.nkx * g.nky + 255) / 256, (size_t)c->nblocks);
     QGN_LAUNCH(KID_PARSEVAL, 48.0 * g.csize(), st,
-               k_budget_spec<<<nb, 256, 0, st>>>(g, b.q, b.psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
+               ::qgn::launch(k_budget_spec, nb, 256, 0, st, g, b.q, b.psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
                                                   c->stats, c->flag));
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     return QGN_OK;
@@ -295,7 +301,7 @@ int qgn_coarse_grain(qgn_ctx* fine, qgn_ctx* coarse) {
     if (cudaStreamSynchronize(coarse->stream) != cudaSuccess) return QGN_ERR_CUDA;
     cudaStream_t s = fine->stream;
     if (coarse_grain_on(fine, coarse, fine->b.q, coarse->b.q, s) != cudaSuccess) return QGN_ERR_CUDA;
-    k_copy_time<<<1, 1, 0, s>>>(fine->b.sc, coarse->b.sc);
+    ::qgn::launch(k_copy_time, 1, 1, 0, s, fine->b.sc, coarse->b.sc);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return QGN_ERR_CUDA;
     coarse->b.Qs[0] = coarse->b.q;
     coarse->halted = false;
@@ -331,13 +337,13 @@ int qgn_closure_snapshot(qgn_ctx* fine, qgn_ctx* coarse, const float* in_scale, 
     // coarse GetRHS of the coarse-grained state
     if (launch_modal(gc, bc.mc, bc.q, bc.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_rhs(gc, bc, bc.q, bc.psi, bc.N[5], coarse->p.C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
-    k_sub<<<grid_of(gc.csize()), 256, 0, s>>>(gc.csize(), bc.N[4], bc.N[5], bc.err);
+    ::qgn::launch(k_sub, grid_of(gc.csize()), 256, 0, s, gc.csize(), bc.N[4], bc.N[5], bc.err);
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_to_phys(gc, bc, bc.q, P0, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_to_phys(gc, bc, bc.psi, P1, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_to_phys(gc, bc, bc.err, P2, s) != cudaSuccess) return QGN_ERR_CUDA;
-    k_pack_in<<<grid_of(npix), 256, 0, s>>>(nz, npix, P0, P1, sc, cin_p, static_cast<__nv_bfloat16*>(x_dev));
-    k_pack_out<<<grid_of(npix), 256, 0, s>>>(nz, npix, P2, sc + 2 * nz, cout_p, y_dev);
+    ::qgn::launch(k_pack_in, grid_of(npix), 256, 0, s, nz, npix, P0, P1, sc, cin_p, static_cast<__nv_bfloat16*>(x_dev));
+    ::qgn::launch(k_pack_out, grid_of(npix), 256, 0, s, nz, npix, P2, sc + 2 * nz, cout_p, y_dev);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return QGN_ERR_CUDA;
     return QGN_OK;
 }

@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_conv(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
            int B, int H, int W, float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
            const float* __restrict__ zin) {
+    QGN_PDL_ENTRY();
     static_assert(CIN % 16 == 0 && COUT % 16 == 0, "channel counts are padded to 16");
     constexpr int LDI = RowPad<CIN>::LD;
     constexpr int NT = COUT / 8;       // n-tiles of 8 output channels per warp
@@ -188,6 +189,7 @@ template <int CIN, int COUT>
 __global__ void __launch_bounds__(kThreads, 1)
     k_wgrad(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ gr, int B, int H, int W,
             float* __restrict__ part) {
+    QGN_PDL_ENTRY();
     constexpr int LDI = RowPad<CIN>::LD, LDG = RowPad<COUT>::LD;
     constexpr int MT = CIN / 16, NT = COUT / 8;
     constexpr int TILES = MT * NT;                  // 16x8 output tiles of dW[tap]
@@ -261,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 __global__ void k_reduce_wgrad(const float* __restrict__ part, int nchunks, int n, float* __restrict__ dw) {
+    QGN_PDL_ENTRY();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float s = 0.f;
         for (int c = 0; c < nchunks; ++c) s += part[(size_t)c * n + i];
@@ -271,6 +274,7 @@ __global__ void k_reduce_wgrad(const float* __restrict__ part, int nchunks, int 
 // bias gradient: per-block column sums of G, then a chunk reduction
 __global__ void k_bias_part(const __nv_bfloat16* __restrict__ gr, long long npix, int C, int pix_per_block,
                             float* __restrict__ part) {
+    QGN_PDL_ENTRY();
     const long long p0 = (long long)blockIdx.x * pix_per_block;
     const long long p1 = min(npix, p0 + pix_per_block);
     for (int c = threadIdx.x; c < C; c += blockDim.x) {
@@ -283,6 +287,7 @@ __global__ void k_bias_part(const __nv_bfloat16* __restrict__ gr, long long npix
 // MSE over the real output channels; G = bf16(2 (Y - T) / count), zero in padded channels
 __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tgt, long long npix, int C, int creal,
                       double inv_count, __nv_bfloat16* __restrict__ g, double* __restrict__ loss_part) {
+    QGN_PDL_ENTRY();
     __shared__ double red[kThreads / 32];
     double s = 0.0;
     const long long n = npix * C;
@@ -311,6 +316,7 @@ __global__ void k_mse(const float* __restrict__ y, const float* __restrict__ tgt
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ g, int n, int cout, int cin, float lr, float b1, float b2, float eps,
                        float c1, float c2, __nv_bfloat16* __restrict__ wf, __nv_bfloat16* __restrict__ wb) {
+    QGN_PDL_ENTRY();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float gi = g[i];
         const float mi = b1 * m[i] + (1.f - b1) * gi;
@@ -332,6 +338,7 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
 __global__ void k_adam_bias(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                             const float* __restrict__ g, int n, float lr, float b1, float b2, float eps, float c1,
                             float c2) {
+    QGN_PDL_ENTRY();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gi = g[i];
@@ -344,6 +351,7 @@ __global__ void k_adam_bias(float* __restrict__ w, float* __restrict__ m, float*
 
 __global__ void k_weights_bf16(const float* __restrict__ w, int n, int cout, int cin, __nv_bfloat16* __restrict__ wf,
                                __nv_bfloat16* __restrict__ wb) {
+    QGN_PDL_ENTRY();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int tap = i / (cout * cin), r = i % (cout * cin);
         const int co = r / cin, ci = r % cin;
@@ -356,6 +364,7 @@ __global__ void k_weights_bf16(const float* __restrict__ w, int n, int cout, int
 // gather batch samples: dst[b] = src[idx[b]] (rows of `bytes` bytes, 16-byte multiples)
 __global__ void k_gather(const unsigned char* __restrict__ src, const int* __restrict__ idx, int nb, size_t bytes,
                          unsigned char* __restrict__ dst) {
+    QGN_PDL_ENTRY();
     const size_t vec = bytes / 16;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vec * nb; i += (size_t)gridDim.x * blockDim.x) {
         const size_t b = i / vec, o = i % vec;
@@ -560,6 +569,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
               int B, int H, int W, float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
               const float* __restrict__ zin, int* __restrict__ err) {
+    QGN_PDL_ENTRY();
     using L = tc::Lay<CIN, COUT>;
     static_assert(COUT == 16 || COUT == 64, "N of the MMA");
     constexpr int NACC = COUT < 32 ? 32 : COUT;           // TMEM columns per accumulator tile
@@ -806,7 +816,7 @@ cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat1
             if (e != cudaSuccess) return e;
             attr = true;
         }
-        k_conv_tc<CIN, COUT, EPI><<<conv_grid(n, batch), kThreads, SM, n->stream>>>(x, wt, bias, batch, n->H, n->W,
+        ::qgn::launch(k_conv_tc<CIN, COUT, EPI>, conv_grid(n, batch), kThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W,
                                                                                     outf, outb, zin, n->d_err);
         return cudaGetLastError();
     }
@@ -817,7 +827,7 @@ cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat1
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    k_conv<CIN, COUT, EPI><<<conv_grid(n, batch), kThreads, SM, n->stream>>>(x, wt, bias, batch, n->H, n->W, outf,
+    ::qgn::launch(k_conv<CIN, COUT, EPI>, conv_grid(n, batch), kThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W, outf,
                                                                              outb, zin);
     return cudaGetLastError();
 }
@@ -844,7 +854,7 @@ cudaError_t launch_wgrad_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat
     }
     const int chunks = (batch * n->H + kWChunkRows - 1) / kWChunkRows;
     *nchunks = chunks;
-    k_wgrad<CIN, COUT><<<dim3(chunks, 9), kThreads, SM, n->stream>>>(x, g, batch, n->H, n->W, part);
+    ::qgn::launch(k_wgrad<CIN, COUT>, dim3(chunks, 9), kThreads, SM, n->stream, x, g, batch, n->H, n->W, part);
     return cudaGetLastError();
 }
 
@@ -886,13 +896,13 @@ int backward(qgn_cnn* net, int batch) {
         int chunks = 0;
         NCK(launch_wgrad(net, net->ci[l], net->co[l], net->act[l], gcur, batch, net->part, &chunks));
         const int nw = 9 * net->co[l] * net->ci[l];
-        k_reduce_wgrad<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->part, chunks, nw, net->gw[l]);
+        ::qgn::launch(k_reduce_wgrad, (nw + 255) / 256, 256, 0, net->stream, net->part, chunks, nw, net->gw[l]);
         NCK(cudaGetLastError());
         const int ppb = 1024;
         const int nbp = (int)((np + ppb - 1) / ppb);
-        k_bias_part<<<nbp, 64, 0, net->stream>>>(gcur, np, net->co[l], ppb, net->part);
+        ::qgn::launch(k_bias_part, nbp, 64, 0, net->stream, gcur, np, net->co[l], ppb, net->part);
         NCK(cudaGetLastError());
-        k_reduce_wgrad<<<1, 64, 0, net->stream>>>(net->part, nbp, net->co[l], net->gb[l]);
+        ::qgn::launch(k_reduce_wgrad, 1, 64, 0, net->stream, net->part, nbp, net->co[l], net->gb[l]);
         NCK(cudaGetLastError());
         if (l > 0) {
             NCK(launch_conv<EPI_GELU_GRAD>(net, net->co[l], net->ci[l], gcur, net->wb[l], nullptr, batch, nullptr,
@@ -908,7 +918,7 @@ int mse(qgn_cnn* net, int batch, const float* tgt) {
     const long long np = (long long)npix(net, batch);
     const int C = net->co[L - 1];
     const double inv = 1.0 / ((double)np * net->cout);
-    k_mse<<<148, kThreads, 0, net->stream>>>(net->z[L - 1], tgt, np, C, net->cout, inv, net->gA, net->loss_part);
+    ::qgn::launch(k_mse, 148, kThreads, 0, net->stream, net->z[L - 1], tgt, np, C, net->cout, inv, net->gA, net->loss_part);
     NCK(cudaGetLastError());
     return QGN_OK;
 }
@@ -1005,7 +1015,7 @@ int qgn_cnn_create(int cin, int width, int cout, int layers, int H, int W, int m
             cudaSuccess)
             return fail(QGN_ERR_CUDA);
         cudaStreamSynchronize(net->stream);
-        k_weights_bf16<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
+        ::qgn::launch(k_weights_bf16, (nw + 255) / 256, 256, 0, net->stream, net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
                                                                   net->wb[l]);
         const size_t chunks = (size_t)((max_batch * H + kWChunkRows - 1) / kWChunkRows);
         part = std::max(part, chunks * nw);
@@ -1062,7 +1072,7 @@ int qgn_cnn_set_weights(qgn_cnn* net, const float* host) {
         off += nw;
         NCK(cudaMemcpyAsync(net->bias[l], host + off, sizeof(float) * net->co[l], cudaMemcpyHostToDevice, net->stream));
         off += net->co[l];
-        k_weights_bf16<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
+        ::qgn::launch(k_weights_bf16, (nw + 255) / 256, 256, 0, net->stream, net->w[l], nw, net->co[l], net->ci[l], net->wf[l],
                                                                   net->wb[l]);
         NCK(cudaGetLastError());
     }
@@ -1120,10 +1130,10 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
     const int L = net->layers;
     const size_t xs = (size_t)net->H * net->W * net->ci[0] * sizeof(__nv_bfloat16);
     const size_t ys = (size_t)net->H * net->W * net->co[L - 1] * sizeof(float);
-    k_gather<<<148 * 4, 256, 0, net->stream>>>(static_cast<const unsigned char*>(x_all), idx, batch, xs,
+    ::qgn::launch(k_gather, 148 * 4, 256, 0, net->stream, static_cast<const unsigned char*>(x_all), idx, batch, xs,
                                               reinterpret_cast<unsigned char*>(net->act[0]));
     NCK(cudaGetLastError());
-    k_gather<<<148 * 4, 256, 0, net->stream>>>(reinterpret_cast<const unsigned char*>(y_all), idx, batch, ys,
+    ::qgn::launch(k_gather, 148 * 4, 256, 0, net->stream, reinterpret_cast<const unsigned char*>(y_all), idx, batch, ys,
                                               reinterpret_cast<unsigned char*>(net->ytgt));
     NCK(cudaGetLastError());
     int rc = forward(net, batch);
@@ -1135,10 +1145,10 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
     const float c1 = 1.f - std::pow(b1, (float)net->adam_t), c2 = 1.f - std::pow(b2, (float)net->adam_t);
     for (int l = 0; l < L; ++l) {
         const int nw = 9 * net->co[l] * net->ci[l];
-        k_adam<<<(nw + 255) / 256, 256, 0, net->stream>>>(net->w[l], net->mw[l], net->vw[l], net->gw[l], nw, net->co[l],
+        ::qgn::launch(k_adam, (nw + 255) / 256, 256, 0, net->stream, net->w[l], net->mw[l], net->vw[l], net->gw[l], nw, net->co[l],
                                                           net->ci[l], lr, b1, b2, eps, c1, c2, net->wf[l], net->wb[l]);
         NCK(cudaGetLastError());
-        k_adam_bias<<<1, 64, 0, net->stream>>>(net->bias[l], net->mb[l], net->vb[l], net->gb[l], net->co[l], lr, b1, b2,
+        ::qgn::launch(k_adam_bias, 1, 64, 0, net->stream, net->bias[l], net->mb[l], net->vb[l], net->gb[l], net->co[l], lr, b1, b2,
                                                eps, c1, c2);
         NCK(cudaGetLastError());
     }

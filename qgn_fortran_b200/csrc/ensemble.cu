@@ -156,6 +156,7 @@ __device__ __noinline__ void ens_stage_point(const EnsMember& M, const Geom& g, 
 template <class CT>
 __global__ void __launch_bounds__(256, 2) k_ens_stage(const EnsMember* __restrict__ mem, const int* __restrict__ start,
                                                    int nm, int s) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
@@ -201,6 +202,7 @@ __device__ __noinline__ void ens_yinv_one(const EnsMember& M, const Geom& g, int
 template <class CT, int TV>
 __global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
     k_ens_yinv(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -231,6 +233,7 @@ __device__ __noinline__ void ens_xpass_one(const EnsMember& M, const Geom& g, in
 template <class CT, int TV>
 __global__ void __launch_bounds__(3 * TV, minb(3 * TV, regcap<CT>(128, 96)))
     k_ens_xpass(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -262,6 +265,7 @@ __device__ __noinline__ void ens_yfwd_one(const EnsMember& M, const Geom& g, int
 template <class CT, int TV>
 __global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
     k_ens_yfwd(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -282,6 +286,7 @@ __global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
 // ---- embedded error (BSRK3.f90:30-34), FP64 -------------------------------------------------
 template <class CT>
 __global__ void __launch_bounds__(256) k_ens_err(EnsMember* __restrict__ mem, const int* __restrict__ start, int nm) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -315,6 +320,7 @@ __device__ __noinline__ void ens_yinv1_one(const EnsMember& M, const Geom& g, in
 
 __global__ void __launch_bounds__(128, minb(128)) k_ens_yinv1(const EnsMember* __restrict__ mem,
                                                               const int* __restrict__ start, int nm) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -342,6 +348,7 @@ __device__ __noinline__ void ens_xinv1_one(const EnsMember& M, const Geom& g, in
 
 __global__ void __launch_bounds__(128, minb(128)) k_ens_xinv1(const EnsMember* __restrict__ mem,
                                                               const int* __restrict__ start, int nm) {
+    QGN_PDL_ENTRY();
     const int total = start[nm];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int mi = ens_find(start, nm, t);
@@ -365,6 +372,7 @@ __global__ void __launch_bounds__(128, minb(128)) k_ens_xinv1(const EnsMember* _
 // condition of the graph (and *any) says whether a member is still active.
 __global__ void __launch_bounds__(256) k_ens_ctrl(EnsMember* __restrict__ mem, int nm,
                                                   cudaGraphConditionalHandle loop, int has_loop, int* __restrict__ any) {
+    QGN_PDL_ENTRY();
     int act = 0;
     for (int i = threadIdx.x; i < nm; i += blockDim.x) {
         EnsMember& M = mem[i];
@@ -394,6 +402,7 @@ __global__ void __launch_bounds__(256) k_ens_ctrl(EnsMember* __restrict__ mem, i
 }
 
 __global__ void k_ens_arm(EnsMember* __restrict__ mem, int nm, int nsteps) {
+    QGN_PDL_ENTRY();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x) {
         EnsMember& M = mem[i];
         const bool go = nsteps > 0 && M.sc->halt == 0;
@@ -404,6 +413,7 @@ __global__ void k_ens_arm(EnsMember* __restrict__ mem, int nm, int nsteps) {
 }
 
 __global__ void k_ens_fsal_done(EnsMember* __restrict__ mem, int nm) {
+    QGN_PDL_ENTRY();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x)
         if (mem[i].active) mem[i].need_fsal = 0;
 }
@@ -588,7 +598,7 @@ int launch_stage(qgn_ens* e, int s) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += (double)c->g.csize() * (16.0 + 2.0 * sizeof(CT) + (s == 3 ? 3 : (s ? 1 : 0)) * sizeof(CT));
     QGN_LAUNCH(KID_STAGE, bytes, e->stream,
-               k_ens_stage<CT><<<grid_for(e, EP_POINT, -1), kPointTile, 0, e->stream>>>(e->d_mem, start_of(e, EP_POINT),
+               ::qgn::launch(k_ens_stage<CT>, grid_for(e, EP_POINT, -1), kPointTile, 0, e->stream, e->d_mem, start_of(e, EP_POINT),
                                                                                         (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
@@ -601,7 +611,7 @@ int launch_yinv_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += sizeof(CT) * (2.0 * c->g.csize() + 3.0 * c->g.nz * c->g.ny * c->g.nkx);
     QGN_LAUNCH(KID_YINV, bytes, e->stream,
-               k_ens_yinv<CT, TV><<<grid, TV, SM, e->stream>>>(e->d_mem, start_of(e, EP_YINV), (int)e->mem.size(), s));
+               ::qgn::launch(k_ens_yinv<CT, TV>, grid, TV, SM, e->stream, e->d_mem, start_of(e, EP_YINV), (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
 }
@@ -613,7 +623,7 @@ int launch_xpass_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += 5.0 * sizeof(CT) * c->g.nz * c->g.ny * c->g.nkx;
     QGN_LAUNCH(KID_XPASS, bytes, e->stream,
-               k_ens_xpass<CT, TV><<<grid, 3 * TV, SM, e->stream>>>(e->d_mem, start_of(e, EP_XPASS),
+               ::qgn::launch(k_ens_xpass<CT, TV>, grid, 3 * TV, SM, e->stream, e->d_mem, start_of(e, EP_XPASS),
                                                                    (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
@@ -626,7 +636,7 @@ int launch_yfwd_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += sizeof(CT) * c->g.nz * c->g.nkx * (2.0 * c->g.ny + 3.0 * c->g.nky);
     QGN_LAUNCH(KID_YFWD, bytes, e->stream,
-               k_ens_yfwd<CT, TV><<<grid, TV, SM, e->stream>>>(e->d_mem, start_of(e, EP_YFWD), (int)e->mem.size(), s));
+               ::qgn::launch(k_ens_yfwd<CT, TV>, grid, TV, SM, e->stream, e->d_mem, start_of(e, EP_YFWD), (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
 }
@@ -666,7 +676,7 @@ int launch_fsal(qgn_ens* e) {
     int r = launch_stage<CT>(e, 0);
     if (r == QGN_OK) r = launch_rhs_all<CT>(e, 0);
     if (r != QGN_OK) return r;
-    QGN_LAUNCH(KID_SCALAR, 0.0, e->stream, k_ens_fsal_done<<<1, 256, 0, e->stream>>>(e->d_mem, (int)e->mem.size()));
+    QGN_LAUNCH(KID_SCALAR, 0.0, e->stream, ::qgn::launch(k_ens_fsal_done, 1, 256, 0, e->stream, e->d_mem, (int)e->mem.size()));
     ECK(cudaGetLastError());
     return QGN_OK;
 }
@@ -686,20 +696,20 @@ int launch_attempt(qgn_ens* e, const cudaGraphConditionalHandle* loop) {
     }
     const int nm = (int)e->mem.size();
     QGN_LAUNCH(KID_LINCOMB, eb, e->stream,
-               k_ens_err<CT><<<grid_for(e, EP_ELEM, -1), kPointTile, 0, e->stream>>>(e->d_mem, start_of(e, EP_ELEM), nm));
+               ::qgn::launch(k_ens_err<CT>, grid_for(e, EP_ELEM, -1), kPointTile, 0, e->stream, e->d_mem, start_of(e, EP_ELEM), nm));
     ECK(cudaGetLastError());
     ECK(smem_attr(k_ens_yinv1, yinv1_smem()));
     QGN_LAUNCH(KID_YINV, yb, e->stream,
-               k_ens_yinv1<<<grid_for(e, EP_YINV1, -1), 128, yinv1_smem(), e->stream>>>(e->d_mem, start_of(e, EP_YINV1),
+               ::qgn::launch(k_ens_yinv1, grid_for(e, EP_YINV1, -1), 128, yinv1_smem(), e->stream, e->d_mem, start_of(e, EP_YINV1),
                                                                                       nm));
     ECK(cudaGetLastError());
     ECK(smem_attr(k_ens_xinv1, xinv1_smem()));
     QGN_LAUNCH(KID_XINV1, xb, e->stream,
-               k_ens_xinv1<<<grid_for(e, EP_XINV1, -1), 128, xinv1_smem(), e->stream>>>(e->d_mem, start_of(e, EP_XINV1),
+               ::qgn::launch(k_ens_xinv1, grid_for(e, EP_XINV1, -1), 128, xinv1_smem(), e->stream, e->d_mem, start_of(e, EP_XINV1),
                                                                                       nm));
     ECK(cudaGetLastError());
     QGN_LAUNCH(KID_SCALAR, 0.0, e->stream,
-               k_ens_ctrl<<<1, 256, 0, e->stream>>>(e->d_mem, nm, loop ? *loop : 0, loop ? 1 : 0, e->d_any));
+               ::qgn::launch(k_ens_ctrl, 1, 256, 0, e->stream, e->d_mem, nm, loop ? *loop : 0, loop ? 1 : 0, e->d_any));
     ECK(cudaGetLastError());
     return QGN_OK;
 }
@@ -886,7 +896,7 @@ int qgn_ens_advance(qgn_ens* e, int nsteps) {
     ECK(cudaMemcpyAsync(e->d_mem, e->h_mem.data(), sizeof(EnsMember) * nm, cudaMemcpyHostToDevice, e->stream));
     int rc = upload_tables(e);
     if (rc != QGN_OK) return rc;
-    QGN_LAUNCH(KID_SCALAR, 0.0, e->stream, k_ens_arm<<<(nm + 255) / 256, 256, 0, e->stream>>>(e->d_mem, nm, nsteps));
+    QGN_LAUNCH(KID_SCALAR, 0.0, e->stream, ::qgn::launch(k_ens_arm, (nm + 255) / 256, 256, 0, e->stream, e->d_mem, nm, nsteps));
     ECK(cudaGetLastError());
     std::vector<DevScalars> s0, s1;
     if (!e->tuned && nsteps > 0) {

@@ -16,6 +16,7 @@
 #include <vector>
 #include "../../include/qgn_gpu.h"
 #include "prof.cuh"
+#include "launch.cuh"
 
 namespace qgn {
 

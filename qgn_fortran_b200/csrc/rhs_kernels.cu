@@ -30,6 +30,7 @@ namespace qgn {
 template <int NZ>
 __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __restrict__ mc,
                                                const double2* __restrict__ q, double2* __restrict__ psi) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
@@ -61,6 +62,7 @@ template <int NY, int NF, class CT, int TV = 0>
 __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, regcap<CT>()))
     k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
            CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
+    QGN_PDL_ENTRY();
     if (TV != 0 && NF > 1)
         yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy, blockIdx.z, blockIdx.z + 1);
     else
@@ -69,10 +71,11 @@ __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY,
 
 template <int NX, bool DRAG, class CT, int TV = 0>
 __global__ void __launch_bounds__(XCfg<NX, DRAG, CT, TV>::THREADS,
-                                  minb(XCfg<NX, DRAG, CT, TV>::THREADS, regcap<CT>(128, 80)))
+                                  minb(XCfg<NX, DRAG, CT, TV>::THREADS, regcap<CT>(NX >= 1024 ? 112 : 128, 80)))
     k_xpass(Geom g, int layer0, const CT* __restrict__ pq, const CT* __restrict__ pv,
             const CT* __restrict__ pu, CT* __restrict__ pp, CT* __restrict__ pd,
             const CT* __restrict__ twx) {
+    QGN_PDL_ENTRY();
     xpass_tile<NX, DRAG, CT, TV>(g, blockIdx.x, layer0 + blockIdx.y, pq, pv, pu, pp, pd, twx);
 }
 
@@ -82,6 +85,7 @@ __global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT, TV>::THREADS,
     k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const CT* __restrict__ q,
            const CT* __restrict__ psi, const CT* __restrict__ pp, const CT* __restrict__ pd,
            CT* __restrict__ out, const CT* __restrict__ twy, const CT* __restrict__ extra) {
+    QGN_PDL_ENTRY();
     yfwd_tile<NY, DRAG, CT, TV>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy, extra);
 }
 
@@ -89,6 +93,7 @@ template <int NX, int EPI, int TV = 0>
 __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
     k_xinv1(Geom g, const double2* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
             const double2* __restrict__ twx) {
+    QGN_PDL_ENTRY();
     xinv1_tile<NX, EPI, TV>(g, blockIdx.x, blockIdx.y, hq, sc, outp, twx);
 }
 
@@ -114,6 +119,7 @@ template <int NX, int SRC = 0, int TV = 0>
 __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
     k_xfwd1(Geom g, const double* __restrict__ phys, double2* __restrict__ hq, const double2* __restrict__ twx,
             const float* __restrict__ y = nullptr, int cout_p = 0, const float* __restrict__ osc = nullptr) {
+    QGN_PDL_ENTRY();
     using C = X1Cfg<NX, TV>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = reinterpret_cast<double2*>(sm_raw);
@@ -123,12 +129,12 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
     const int slot = tid / C::G, lane = tid % C::G;
     const int rp = blockIdx.x * C::RP + slot;
     const size_t prow = ((size_t)l * g.ny + 2 * rp) * NX;
+    const double rsc = SRC == 0 ? 1.0 : 1.0 / (double)osc[l];   // one division per thread
     auto ld = [&](int x) -> double2 {
-        if (SRC == 0) return make_double2(phys[prow + x], phys[prow + NX + x]);
+        if constexpr (SRC == 0) return make_double2(phys[prow + x], phys[prow + NX + x]);
         const size_t pix = (size_t)(2 * rp) * NX + x;
         const float* yl = y + (size_t)l * g.ny * NX;
-        const double inv = (double)osc[l];
-        return make_double2((double)yl[pix] / inv, (double)yl[pix + NX] / inv);
+        return make_double2((double)yl[pix] * rsc, (double)yl[pix + NX] * rsc);
     };
     NoIO none;
     fft_fused<NX, -1, SRC_FN, DST_SMEM>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
@@ -148,6 +154,7 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
 template <int NY>
 __global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREADS))
     k_yfwd1(Geom g, const double2* __restrict__ hq, double2* __restrict__ out, const double2* __restrict__ twy) {
+    QGN_PDL_ENTRY();
     using C = YInvCfg<NY>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     double2* sm = reinterpret_cast<double2*>(sm_raw);
@@ -209,11 +216,11 @@ cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, 
     dim3 grid((unsigned)((P + 255) / 256));
     const double nb = 2.0 * 16.0 * (double)g.csize();
     switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, s, k_modal<2><<<grid, 256, 0, s>>>(g, mc, q, psi)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, s, k_modal<4><<<grid, 256, 0, s>>>(g, mc, q, psi)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, s, k_modal<8><<<grid, 256, 0, s>>>(g, mc, q, psi)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, s, k_modal<16><<<grid, 256, 0, s>>>(g, mc, q, psi)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, s, k_modal<0><<<grid, 256, 0, s>>>(g, mc, q, psi)); break;
+        case 2: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<2>, grid, 256, 0, s, g, mc, q, psi)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<4>, grid, 256, 0, s, g, mc, q, psi)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<8>, grid, 256, 0, s, g, mc, q, psi)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<16>, grid, 256, 0, s, g, mc, q, psi)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<0>, grid, 256, 0, s, g, mc, q, psi)); break;
     }
     return cudaGetLastError();
 }
@@ -228,7 +235,7 @@ static cudaError_t yinv_go(const Geom& g, const CT* q, const CT* psi, CT* hq, CT
     const double es = (double)sizeof(CT);
     const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
     QGN_LAUNCH(KID_YINV, NF == 3 ? 2.0 * Cb + 3.0 * Hb : NF * (Cb + Hb), s,
-               k_yinv<NY, NF, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, q, psi, hq, hp, hu, twy));
+               ::qgn::launch(k_yinv<NY, NF, CT, TV>, grid, C::THREADS, C::SMEM, s, g, q, psi, hq, hp, hu, twy));
     return cudaGetLastError();
 }
 
@@ -266,7 +273,7 @@ static cudaError_t xpass_go(const Geom& g, int layer0, int layers, const CT* hq,
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, layers);
     const double es = (double)sizeof(CT);
     QGN_LAUNCH(KID_XPASS, (DRAG ? 7.0 : 5.0) * es * (double)layers * g.ny * g.nkx, s,
-               k_xpass<NX, DRAG, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, layer0, hq, hp, hu, hpp, hpd, twx));
+               ::qgn::launch(k_xpass<NX, DRAG, CT, TV>, grid, C::THREADS, C::SMEM, s, g, layer0, hq, hp, hu, hpp, hpd, twx));
     return cudaGetLastError();
 }
 
@@ -314,7 +321,7 @@ static cudaError_t yfwd_go(const Geom& g, int layer0, int layers, const LayerCon
     dim3 grid((g.nkx + C::TKX - 1) / C::TKX, layers);
     const double lb = (double)sizeof(CT) * (double)layers * g.nkx;
     QGN_LAUNCH(KID_YFWD, lb * ((DRAG ? 4.0 : 2.0) * NY + 3.0 * g.nky), s,
-               k_yfwd<NY, DRAG, CT, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, layer0, lc, q, psi, hpp, hpd, out, twy,
+               ::qgn::launch(k_yfwd<NY, DRAG, CT, TV>, grid, C::THREADS, C::SMEM, s, g, layer0, lc, q, psi, hpp, hpd, out, twy,
                                                                           extra));
     return cudaGetLastError();
 }
@@ -385,7 +392,7 @@ static cudaError_t xinv1_go(const Geom& g, const Buffers& b, DevScalars* sc, dou
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
     const double hb = 16.0 * (double)g.nz * g.ny * g.nkx;
     QGN_LAUNCH(KID_XINV1, hb + (EPI == 1 ? 8.0 * (double)g.nz * g.ny * NX : 0.0), s,
-               k_xinv1<NX, EPI, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, sc, outp, b.twx));
+               ::qgn::launch(k_xinv1<NX, EPI, TV>, grid, C::THREADS, C::SMEM, s, g, b.hq, sc, outp, b.twx));
     return cudaGetLastError();
 }
 
@@ -416,7 +423,7 @@ static cudaError_t xfwd1_go(const Geom& g, const Buffers& b, const double* phys,
     if ((e = set_smem(k_xfwd1<NX, SRC, TV>, C::SMEM)) != cudaSuccess) return e;
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
     QGN_LAUNCH(KID_XFWD1, (SRC ? 4.0 : 8.0) * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
-               k_xfwd1<NX, SRC, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, phys, b.hq, b.twx, y, cout_p, osc));
+               ::qgn::launch(k_xfwd1<NX, SRC, TV>, grid, C::THREADS, C::SMEM, s, g, phys, b.hq, b.twx, y, cout_p, osc));
     return cudaGetLastError();
 }
 
@@ -445,7 +452,7 @@ cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys
         if ((e2 = set_smem(k_yfwd1<NY>, C::SMEM)) != cudaSuccess) return e2;
         dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
         QGN_LAUNCH(KID_YFWD1, 16.0 * (double)g.nz * g.nkx * (NY + g.nky), s,
-                   k_yfwd1<NY><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, out, b.twy));
+                   ::qgn::launch(k_yfwd1<NY>, grid, C::THREADS, C::SMEM, s, g, b.hq, out, b.twy));
         return cudaGetLastError();
     });
 }
@@ -466,6 +473,7 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
     k_xpack(Geom g, const double2* __restrict__ hq_q, const double2* __restrict__ hq_psi,
             const double2* __restrict__ twx, const float* __restrict__ scale, __nv_bfloat16* __restrict__ xout,
             int cin_p) {
+    QGN_PDL_ENTRY();
     const int field = blockIdx.y / g.nz, l = blockIdx.y % g.nz;
     xinv1_tile<NX, 2, TV>(g, blockIdx.x, l, field ? hq_psi : hq_q, nullptr, nullptr, twx, scale, xout, cin_p,
                           field * g.nz + l);
@@ -479,7 +487,7 @@ static cudaError_t xpack_go(const Geom& g, const Buffers& b, const float* scale,
     if ((e = set_smem(k_xpack<NX, TV>, C::SMEM)) != cudaSuccess) return e;
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 2 * g.nz);
     QGN_LAUNCH(KID_XINV1, 2.0 * (16.0 * g.nz * g.ny * g.nkx + 2.0 * g.nz * g.ny * NX), s,
-               k_xpack<NX, TV><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, b.hu, b.twx, scale, xout, cin_p));
+               ::qgn::launch(k_xpack<NX, TV>, grid, C::THREADS, C::SMEM, s, g, b.hq, b.hu, b.twx, scale, xout, cin_p));
     return cudaGetLastError();
 }
 
@@ -511,7 +519,7 @@ cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* 
         if ((e2 = set_smem(k_yfwd1<NY>, C::SMEM)) != cudaSuccess) return e2;
         dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
         QGN_LAUNCH(KID_YFWD1, 16.0 * (double)g.nz * g.nkx * (NY + g.nky), s,
-                   k_yfwd1<NY><<<grid, C::THREADS, C::SMEM, s>>>(g, b.hq, out, b.twy));
+                   ::qgn::launch(k_yfwd1<NY>, grid, C::THREADS, C::SMEM, s, g, b.hq, out, b.twy));
         return cudaGetLastError();
     });
 }
@@ -532,6 +540,7 @@ Geom full_geom(const Geom& g) {
 }
 
 __global__ void k_uv_hat(Geom g, const double2* __restrict__ psi, double2* __restrict__ uh, double2* __restrict__ vh) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
@@ -545,6 +554,7 @@ __global__ void k_uv_hat(Geom g, const double2* __restrict__ psi, double2* __res
 }
 
 __global__ void k_products(size_t n, const double* __restrict__ q, double* __restrict__ u, double* __restrict__ v) {
+    QGN_PDL_ENTRY();
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const double qq = q[e];
         u[e] = u[e] * qq;     // u_phys*q_phys
@@ -554,6 +564,7 @@ __global__ void k_products(size_t n, const double* __restrict__ q, double* __res
 
 // jaco_hat = i kx uq_hat + i ky vq_hat on the full spectrum (QGN_Module.f90:244-247), in place into uq
 __global__ void k_jac_full(Geom gf, double2* __restrict__ uq, const double2* __restrict__ vq) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)gf.nkx * gf.nky;
     const size_t total = P * gf.nz;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
@@ -569,6 +580,7 @@ __global__ void k_jac_full(Geom gf, double2* __restrict__ uq, const double2* __r
 // optionally psi_mode = q_mode / (-k^2 + EVals(k)) with psi_mode(1,1) = 0 (QGN_Module.f90:399-400)
 __global__ void k_modal_proj(Geom g, const ModalConst* __restrict__ mc, const double2* __restrict__ x,
                              double2* __restrict__ xm, double2* __restrict__ pm) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const int nz = g.nz;
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
@@ -606,12 +618,12 @@ cudaError_t launch_modal_fields(const Geom& g, const Buffers& b, const double2* 
     double* Pv = phys3 + 2 * np;
     // GetPsi, u_hat, v_hat and the physical fields of the Jacobian (QGN_Module.f90:218-234)
     if ((e = launch_modal(g, b.mc, q, b.psi, s)) != cudaSuccess) return e;
-    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)g.csize(), s, k_uv_hat<<<blocks, 256, 0, s>>>(g, b.psi, fa, fb));
+    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)g.csize(), s, ::qgn::launch(k_uv_hat, blocks, 256, 0, s, g, b.psi, fa, fb));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_to_phys(g, b, q, Pq, s)) != cudaSuccess) return e;
     if ((e = launch_to_phys(g, b, fa, Pu, s)) != cudaSuccess) return e;
     if ((e = launch_to_phys(g, b, fb, Pv, s)) != cudaSuccess) return e;
-    QGN_LAUNCH(KID_LAYOUT, 40.0 * (double)np, s, k_products<<<blocks, 256, 0, s>>>(np, Pq, Pu, Pv));
+    QGN_LAUNCH(KID_LAYOUT, 40.0 * (double)np, s, ::qgn::launch(k_products, blocks, 256, 0, s, np, Pq, Pu, Pv));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // full-spectrum r2c of u*q and v*q and the undealiased Jacobian (QGN_Module.f90:235-247)
     const Geom gf = full_geom(g);
@@ -619,13 +631,13 @@ cudaError_t launch_modal_fields(const Geom& g, const Buffers& b, const double2* 
     bf.hq = full_half;
     if ((e = launch_from_phys(gf, bf, Pu, fa, s)) != cudaSuccess) return e;
     if ((e = launch_from_phys(gf, bf, Pv, fb, s)) != cudaSuccess) return e;
-    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)gf.csize(), s, k_jac_full<<<blocks, 256, 0, s>>>(gf, fa, fb));
+    QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)gf.csize(), s, ::qgn::launch(k_jac_full, blocks, 256, 0, s, gf, fa, fb));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // modal projections and their physical fields (QGN_Module.f90:390-415)
-    QGN_LAUNCH(KID_MODAL, 32.0 * (double)gf.csize(), s, k_modal_proj<<<blocks, 256, 0, s>>>(gf, b.mc, fa, fb, nullptr));
+    QGN_LAUNCH(KID_MODAL, 32.0 * (double)gf.csize(), s, ::qgn::launch(k_modal_proj, blocks, 256, 0, s, gf, b.mc, fa, fb, nullptr));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_to_phys(gf, bf, fb, out_j, s)) != cudaSuccess) return e;
-    QGN_LAUNCH(KID_MODAL, 48.0 * (double)g.csize(), s, k_modal_proj<<<blocks, 256, 0, s>>>(g, b.mc, q, fa, fb));
+    QGN_LAUNCH(KID_MODAL, 48.0 * (double)g.csize(), s, ::qgn::launch(k_modal_proj, blocks, 256, 0, s, g, b.mc, q, fa, fb));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_to_phys(g, b, fa, out_q, s)) != cudaSuccess) return e;
     return launch_to_phys(g, b, fb, out_p, s);

@@ -49,6 +49,7 @@ cudaError_t scratch_address(unsigned char** out) {
 
 // the reference's q_hat(nx/2+1,ny,nz) in device memory -> compact kept modes, (0,0) zeroed
 __global__ void k_full_to_compact_dev(Geom g, const double2* __restrict__ full, double2* __restrict__ c) {
+    QGN_PDL_ENTRY();
     const size_t n = g.csize();
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         const int m = (int)(e % g.nky);
@@ -64,6 +65,7 @@ __global__ void k_full_to_compact_dev(Geom g, const double2* __restrict__ full, 
 
 // compact -> the reference's layout with zeros in the dealiased band
 __global__ void k_compact_to_full_dev(Geom g, const double2* __restrict__ c, double2* __restrict__ full) {
+    QGN_PDL_ENTRY();
     const size_t total = (size_t)g.nz * g.ny * g.nxh;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(e % g.nxh);
@@ -79,6 +81,7 @@ __global__ void k_compact_to_full_dev(Geom g, const double2* __restrict__ c, dou
 
 // exp(-2 pi i m/n) for m in [0,n)
 __global__ void k_twiddle_table(int n, double2* __restrict__ tw) {
+    QGN_PDL_ENTRY();
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n) return;
     double s, c;
@@ -174,14 +177,14 @@ extern "C" int qgn_rhs_static(const qgn_params* p, const double* H, const double
     if (cudaMemcpyAsync(b.lc, &lc, sizeof(lc), cudaMemcpyHostToDevice, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (cudaMemcpyAsync(b.mc, &mc, sizeof(mc), cudaMemcpyHostToDevice, s) != cudaSuccess) return QGN_ERR_CUDA;
 
-    k_twiddle_table<<<(g.nx + 255) / 256, 256, 0, s>>>(g.nx, b.twx);
-    k_twiddle_table<<<(g.ny + 255) / 256, 256, 0, s>>>(g.ny, b.twy);
+    ::qgn::launch(k_twiddle_table, (g.nx + 255) / 256, 256, 0, s, g.nx, b.twx);
+    ::qgn::launch(k_twiddle_table, (g.ny + 255) / 256, 256, 0, s, g.ny, b.twy);
     const int blocks = 148 * 8;
-    k_full_to_compact_dev<<<blocks, 256, 0, s>>>(g, reinterpret_cast<const double2*>(q_hat_dev), qc);
+    ::qgn::launch(k_full_to_compact_dev, blocks, 256, 0, s, g, reinterpret_cast<const double2*>(q_hat_dev), qc);
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_modal(g, b.mc, qc, pc, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_rhs(g, b, qc, pc, oc, p->C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
-    k_compact_to_full_dev<<<blocks, 256, 0, s>>>(g, oc, reinterpret_cast<double2*>(rhs_dev));
+    ::qgn::launch(k_compact_to_full_dev, blocks, 256, 0, s, g, oc, reinterpret_cast<double2*>(rhs_dev));
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     return QGN_OK;
 }

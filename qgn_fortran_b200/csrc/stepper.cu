@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(256) k_ark_update(Geom g, StagePtrs sp, const 
                                                     double2* __restrict__ qnew, double2* __restrict__ err,
                                                     const LayerConst* __restrict__ lc,
                                                     DevScalars* __restrict__ sc) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -189,6 +190,7 @@ template <int S, class T>
 __global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const double2* __restrict__ q,
                                                   T* __restrict__ qout, const LayerConst* __restrict__ lc,
                                                   const DevScalars* __restrict__ sc) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,6 +238,7 @@ __global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const 
 template <int NZ>
 __global__ void __launch_bounds__(256, 2) k_modal_f32(Geom g, const ModalConst* __restrict__ mc,
                                                       const float2* __restrict__ q, float2* __restrict__ psi) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
@@ -272,6 +275,7 @@ __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp
                                                           double2* __restrict__ qnew, double2* __restrict__ err,
                                                           const LayerConst* __restrict__ lc,
                                                           DevScalars* __restrict__ sc) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,6 +316,7 @@ template <int NZ>
 __global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const ModalConst* __restrict__ mc,
                                                      const double2* __restrict__ q, float2* __restrict__ q32,
                                                      float2* __restrict__ psi32) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
@@ -339,6 +344,7 @@ __global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const ModalConst
 }
 
 __global__ void k_f2d(size_t n, const float2* __restrict__ a, double2* __restrict__ b) {
+    QGN_PDL_ENTRY();
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e < n) b[e] = make_double2(a[e].x, a[e].y);
 }
@@ -349,6 +355,7 @@ __global__ void __launch_bounds__(256, 2) k_combo(Geom g, Combo cb, const double
                                                double2* __restrict__ out, double2* __restrict__ psi,
                                                const ModalConst* __restrict__ mc,
                                                const DevScalars* __restrict__ sc, int want_psi) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
@@ -389,6 +396,7 @@ __global__ void __launch_bounds__(256, 2) k_combo(Geom g, Combo cb, const double
 
 // ---- linear combination without q: out = sum_j a_j R_j (error spectra) --------------------
 __global__ void k_lincomb(size_t n, Combo cb, double2* __restrict__ out) {
+    QGN_PDL_ENTRY();
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     double2 v = make_double2(0.0, 0.0);
@@ -416,6 +424,7 @@ __device__ __forceinline__ double parseval_block(const Geom& g, const double2* _
 
 template <int POW>
 __global__ void __launch_bounds__(256) k_parseval(Geom g, const double2* __restrict__ f, double* __restrict__ partial) {
+    QGN_PDL_ENTRY();
     const double t = parseval_block<POW>(g, f, blockIdx.y);
     if (threadIdx.x == 0) partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
 }
@@ -469,6 +478,7 @@ __device__ __forceinline__ double layer_sum(const double* __restrict__ partial, 
 // partials of every layer in a fixed order (deterministic) and writes A8L.
 __global__ void __launch_bounds__(256) k_leith(Geom g, const double2* __restrict__ f, double* __restrict__ partial,
                                                double c12, DevScalars* __restrict__ sc) {
+    QGN_PDL_ENTRY();
     __shared__ unsigned s_last;
     const int nb = gridDim.x;
     const double t = parseval_block<4>(g, f, blockIdx.y);
@@ -496,6 +506,7 @@ __global__ void __launch_bounds__(256) k_leith(Geom g, const double2* __restrict
 // layer KE = 0.5 * S/(nx ny)^2 * H_k/Htot with S the k^2-weighted Parseval sum of psi
 __global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nblocks, const double* __restrict__ Hw,
                            double* __restrict__ ke) {
+    QGN_PDL_ENTRY();
     const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (l >= g.nz) return;
     const double s = layer_sum(partial, l, nblocks);
@@ -506,6 +517,7 @@ __global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nbloc
 // isotropic KE spectrum per layer in integer shells round(sqrt(i^2 + jj^2))
 __global__ void k_ke_spectrum(Geom g, const double2* __restrict__ psi, const double* __restrict__ Hw, int nbins,
                               double* __restrict__ spec) {
+    QGN_PDL_ENTRY();
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t total = P * g.nz;
     const double N = (double)g.nx * (double)g.ny;
@@ -539,6 +551,7 @@ __global__ void k_ke_spectrum(Geom g, const double2* __restrict__ psi, const dou
 // the graph's retry loop ---------------------------------------------------------------------
 __global__ void k_controller(int kind, double inv_n, double TOL, double dt_max, int max_rejects,
                              cudaGraphConditionalHandle loop, int has_loop, DevScalars* sc) {
+    QGN_PDL_ENTRY();
     const unsigned again = ctrl_decide(kind, inv_n, TOL, dt_max, max_rejects, sc);
     if (has_loop) cudaGraphSetConditional(loop, again);
 }
@@ -546,21 +559,26 @@ __global__ void k_controller(int kind, double inv_n, double TOL, double dt_max, 
 // start of a step: clears the per-step reject count; with a gate handle it also opens the
 // graph's step body only while the run is not halted
 __global__ void k_step_gate(DevScalars* sc, cudaGraphConditionalHandle gate, int has_gate) {
+    QGN_PDL_ENTRY();
     sc->rejects_step = 0;
     if (has_gate) cudaGraphSetConditional(gate, sc->halt == 0 ? 1u : 0u);
 }
 
-__global__ void k_set_cond(cudaGraphConditionalHandle h, unsigned int v) { cudaGraphSetConditional(h, v); }
+__global__ void k_set_cond(cudaGraphConditionalHandle h, unsigned int v) {
+    QGN_PDL_ENTRY(); cudaGraphSetConditional(h, v); }
 
 __global__ void k_zero_max(DevScalars* sc) {
+    QGN_PDL_ENTRY();
     sc->maxbits = 0ULL;
     sc->accept = 0;
 }
 
-__global__ void k_advance_time(DevScalars* sc) { sc->t = sc->t + sc->dt; }
+__global__ void k_advance_time(DevScalars* sc) {
+    QGN_PDL_ENTRY(); sc->t = sc->t + sc->dt; }
 
 // a new state from the host: set t and dt and clear a previous failure
 __global__ void k_set_time(DevScalars* sc, double t, double dt) {
+    QGN_PDL_ENTRY();
     sc->t = t;
     sc->dt = dt;
     sc->nonfinite = 0;
@@ -592,11 +610,11 @@ static cudaError_t launch_comb(const Geom& g, const Buffers& b, int s, cudaStrea
     const double nb = 16.0 * C + es * C * (2.0 * s - 1.0 + 1.0);
     const unsigned nbk = blocks_for(g.csize(), 256);
     switch (s) {
-        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<1, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<2, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
-        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<3, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<4, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
-        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_comb<5, T><<<nbk, 256, 0, st>>>(g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_comb<1, T>, nbk, 256, 0, st, g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_comb<2, T>, nbk, 256, 0, st, g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_comb<3, T>, nbk, 256, 0, st, g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_comb<4, T>, nbk, 256, 0, st, g, cp, b.q, qout, b.lc, b.sc))); break;
+        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_comb<5, T>, nbk, 256, 0, st, g, cp, b.q, qout, b.lc, b.sc))); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -611,6 +629,7 @@ __global__ void __launch_bounds__(256, 2) k_ark_stage_small(Geom g, CombPtrs<dou
                                                            const LayerConst* __restrict__ lc,
                                                            const ModalConst* __restrict__ mc,
                                                            const DevScalars* __restrict__ sc) {
+    QGN_PDL_ENTRY();
     __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
     const int nz = g.nz;
     for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
@@ -661,11 +680,11 @@ static cudaError_t launch_stage_small_nz(const Geom& g, const Buffers& b, int s,
     const double C = (double)g.csize(), nb = 16.0 * C * (2.0 * s + 2.0);
     double2* qo = b.Qs[s];
     switch (s) {
-        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<1, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<2, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<3, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<4, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (k_ark_stage_small<5, NZ><<<nbk, 256, 0, st>>>(g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<1, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<2, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<3, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<4, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<5, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -676,11 +695,11 @@ cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, f
     dim3 grid(blocks_for(P, 256));
     const double nb = 16.0 * (double)g.csize();
     switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<2><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<4><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<8><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<16><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_f32<0><<<grid, 256, 0, st>>>(g, b.mc, q, psi)); break;
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<2>, grid, 256, 0, st, g, b.mc, q, psi)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<4>, grid, 256, 0, st, g, b.mc, q, psi)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<8>, grid, 256, 0, st, g, b.mc, q, psi)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<16>, grid, 256, 0, st, g, b.mc, q, psi)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<0>, grid, 256, 0, st, g, b.mc, q, psi)); break;
     }
     return cudaGetLastError();
 }
@@ -720,7 +739,7 @@ cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_
     const StagePtrs32 sp = stage_ptrs32(b);
     const double C = (double)g.csize();
     QGN_LAUNCH(KID_UPDATE, 16.0 * C * 3.0 + 8.0 * C * 9.0, st,
-               k_ark_update_mixed<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
+               ::qgn::launch(k_ark_update_mixed, blocks_for(g.csize(), 256), 256, 0, st, g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
     return cudaGetLastError();
 }
 
@@ -730,17 +749,17 @@ cudaError_t launch_modal_mixed(const Geom& g, const Buffers& b, const double2* q
     dim3 grid(blocks_for(P, 256));
     const double nb = 32.0 * (double)g.csize();
     switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<2><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<4><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<8><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<16><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, st, k_modal_mixed<0><<<grid, 256, 0, st>>>(g, b.mc, q, q32, psi32)); break;
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<2>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<4>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<8>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<16>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<0>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_f2d(size_t n, const float2* a, double2* b, cudaStream_t st) {
-    QGN_LAUNCH(KID_LAYOUT, 24.0 * (double)n, st, k_f2d<<<blocks_for(n, 256), 256, 0, st>>>(n, a, b));
+    QGN_LAUNCH(KID_LAYOUT, 24.0 * (double)n, st, ::qgn::launch(k_f2d, blocks_for(n, 256), 256, 0, st, n, a, b));
     return cudaGetLastError();
 }
 
@@ -748,7 +767,7 @@ cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t st) 
     StagePtrs sp{};
     for (int j = 0; j < 6; ++j) { sp.N[j] = b.N[j]; sp.Qs[j] = b.Qs[j]; }
     QGN_LAUNCH(KID_UPDATE, 12.0 * 16.0 * (double)g.csize(), st,
-               k_ark_update<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
+               ::qgn::launch(k_ark_update, blocks_for(g.csize(), 256), 256, 0, st, g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
     return cudaGetLastError();
 }
 
@@ -759,18 +778,18 @@ cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const
     const int wp = want_psi ? 1 : 0;
     const double nb = 16.0 * (double)g.csize() * (1.0 + cb.n + 1.0 + wp);
     switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<2><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 4: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<4><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 8: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<8><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 16: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<16><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        default: QGN_LAUNCH(KID_COMBO, nb, st, k_combo<0><<<grid, 256, 0, st>>>(g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 2: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<2>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 4: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<4>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 8: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<8>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        case 16: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<16>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+        default: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<0>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStream_t st) {
     QGN_LAUNCH(KID_LINCOMB, 16.0 * (double)g.csize() * (cb.n + 1.0), st,
-               k_lincomb<<<blocks_for(g.csize(), 256), 256, 0, st>>>(g.csize(), cb, out));
+               ::qgn::launch(k_lincomb, blocks_for(g.csize(), 256), 256, 0, st, g.csize(), cb, out));
     return cudaGetLastError();
 }
 
@@ -787,15 +806,15 @@ static int parseval_blocks(const Geom& g) {
 cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t st) {
     const int nb = parseval_blocks(g);
     QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
-               k_leith<<<dim3(nb, g.nz), 256, 0, st>>>(g, q, b.red, c12, b.sc));
+               ::qgn::launch(k_leith, dim3(nb, g.nz), 256, 0, st, g, q, b.red, c12, b.sc));
     return cudaGetLastError();
 }
 
 cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t st) {
     const int nb = parseval_blocks(g);
     QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
-               k_parseval<1><<<dim3(nb, g.nz), 256, 0, st>>>(g, psi, b.red));
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_ke_final<<<(g.nz + 7) / 8, 256, 0, st>>>(g, b.red, nb, Hw, ke));
+               ::qgn::launch(k_parseval<1>, dim3(nb, g.nz), 256, 0, st, g, psi, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_ke_final, (g.nz + 7) / 8, 256, 0, st, g, b.red, nb, Hw, ke));
     return cudaGetLastError();
 }
 
@@ -804,40 +823,40 @@ cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* 
     cudaError_t e = cudaMemsetAsync(spec, 0, sizeof(double) * (size_t)nbins * g.nz, st);
     if (e != cudaSuccess) return e;
     QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
-               k_ke_spectrum<<<148 * 8, 256, 0, st>>>(g, psi, Hw, nbins, spec));
+               ::qgn::launch(k_ke_spectrum, 148 * 8, 256, 0, st, g, psi, Hw, nbins, spec));
     return cudaGetLastError();
 }
 
 cudaError_t launch_controller(const Geom& g, const Buffers& b, int kind, double TOL, double dt_max, int max_rejects,
                               const cudaGraphConditionalHandle* loop, cudaStream_t st) {
     QGN_LAUNCH(KID_SCALAR, 0.0, st,
-               k_controller<<<1, 1, 0, st>>>(kind, g.inv_nxny, TOL, dt_max, max_rejects, loop ? *loop : 0,
+               ::qgn::launch(k_controller, 1, 1, 0, st, kind, g.inv_nxny, TOL, dt_max, max_rejects, loop ? *loop : 0,
                                              loop ? 1 : 0, b.sc));
     return cudaGetLastError();
 }
 
 cudaError_t launch_step_gate(DevScalars* sc, const cudaGraphConditionalHandle* gate, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_step_gate<<<1, 1, 0, st>>>(sc, gate ? *gate : 0, gate ? 1 : 0));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_step_gate, 1, 1, 0, st, sc, gate ? *gate : 0, gate ? 1 : 0));
     return cudaGetLastError();
 }
 
 cudaError_t launch_set_cond(cudaGraphConditionalHandle h, unsigned int v, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_set_cond<<<1, 1, 0, st>>>(h, v));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_set_cond, 1, 1, 0, st, h, v));
     return cudaGetLastError();
 }
 
 cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_zero_max<<<1, 1, 0, st>>>(sc));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_zero_max, 1, 1, 0, st, sc));
     return cudaGetLastError();
 }
 
 cudaError_t launch_set_time(DevScalars* sc, double t, double dt, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_set_time<<<1, 1, 0, st>>>(sc, t, dt));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_set_time, 1, 1, 0, st, sc, t, dt));
     return cudaGetLastError();
 }
 
 cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t st) {
-    QGN_LAUNCH(KID_SCALAR, 0.0, st, k_advance_time<<<1, 1, 0, st>>>(sc));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_advance_time, 1, 1, 0, st, sc));
     return cudaGetLastError();
 }
 
