@@ -255,8 +255,10 @@ int qgn_cnn_gradients(qgn_cnn* net, const void* x, const float* y, int batch, fl
  * dataset x_all [n][H][W][cin_p] BF16, y_all [n][H][W][cout_p] FP32; loss before the update */
 int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, const int* idx, int batch,
                        float lr, double* loss);
-/* tensor-core path of the convolutions: 0 = tcgen05 with TMEM accumulators (default),
- * 1 = warp-level mma.sync; both give the same result up to FP32 summation order */
+/* tensor-core path of the convolutions: 0 = tcgen05 with TMEM accumulators (default; an
+ * inference whose image rows fit one CTA each runs all layers in one cooperative launch),
+ * 1 = warp-level mma.sync, 2 = tcgen05 with one launch per layer; 0 and 2 give identical
+ * results, 1 the same up to FP32 summation order */
 int qgn_cnn_set_engine(qgn_cnn* net, int engine);
 /* waits for the network's stream; QGN_ERR_CUDA if a tensor-core kernel reported a timeout */
 int qgn_cnn_check(qgn_cnn* net);

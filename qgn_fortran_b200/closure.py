@@ -93,8 +93,9 @@ class ClosureNet:
         return loss.value if want_loss else None
 
     def set_engine(self, engine: str):
-        """'tcgen05' (TMEM accumulators, default) or 'mma.sync' (warp-level MMA)."""
-        self._check(self.lib.qgn_cnn_set_engine(self.net, {"tcgen05": 0, "mma.sync": 1}[engine]),
+        """'tcgen05' (TMEM accumulators, default; a small-batch inference runs all layers in one
+        launch), 'mma.sync' (warp-level MMA) or 'tcgen05-layers' (one tcgen05 launch per layer)."""
+        self._check(self.lib.qgn_cnn_set_engine(self.net, {"tcgen05": 0, "mma.sync": 1, "tcgen05-layers": 2}[engine]),
                     "qgn_cnn_set_engine")
 
     def check(self):

@@ -6,7 +6,9 @@
 // two layouts (forward: [tap][cout][cin], backward-data: [tap'][cin][cout] with the taps
 // mirrored); products run on the BF16 tensor cores with FP32 accumulation: tcgen05.mma with
 // the accumulator tile in TMEM (default), or the warp-level mma.m16n8k16 path (selectable with
-// qgn_cnn_set_engine or QGN_CNN_MMA=sync; the weight gradients always use it).
+// qgn_cnn_set_engine or QGN_CNN_MMA=sync; the weight gradients always use it).  An inference
+// whose tiles fit one CTA each runs all layers in one cooperative launch (k_cnn_fused);
+// QGN_CNN_MMA=layers keeps one tcgen05 launch per layer.
 //
 // Kernels (one CTA = 8 warps = 128 consecutive pixels of one image row, persistent over rows):
 //   k_conv<CIN,COUT,EPI>  implicit GEMM  out[p, n] = sum_{tap, k} in[p + tap, k] w[tap, n, k]
@@ -17,6 +19,8 @@
 //   k_reduce_*            deterministic chunk sums of dW and the bias gradient
 //   k_mse                 loss and dL/dY = 2 (Y - T)/count, as BF16 G of the last layer
 //   k_adam                Adam on the FP32 masters, refreshing both BF16 layouts
+//   k_conv_tc<CIN,COUT,EPI>  the implicit GEMM on tcgen05 (TMEM accumulators)
+//   k_cnn_fused           every layer of a small-batch inference, rows exchanged through L2
 #include "qgn_internal.cuh"
 #include "cnn.cuh"
 
@@ -42,7 +46,9 @@ constexpr int kWChunkRows = 16;      // image rows per weight-gradient partial
 
 // EPI_PLANAR: as EPI_LINEAR but the FP32 output is planar, out[n][pixel] (the closure's input
 // to its forward transform)
-enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELU_GRAD = 2, EPI_PLANAR = 3 };
+// EPI_GELU_ACT: as EPI_GELU without the FP32 pre-activation (inference: only the BF16
+// activation feeds the next layer)
+enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELU_GRAD = 2, EPI_PLANAR = 3, EPI_GELU_ACT = 4 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -473,6 +479,36 @@ __device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, float* v) {
     tmem_ld<16>(taddr + 16, v + 16);
 }
 
+// The 9*CIN/16 MMAs of one tile into the accumulator at TMEM address dacc, then a commit that
+// arrives on the mbarrier at bar when they have completed.  ra: shared addresses of the ring
+// slots holding input rows h-1, h, h+1; w: the layer's weights.  One thread issues.
+template <int CIN, int COUT>
+__device__ __forceinline__ void issue_tile(uint32_t dacc, const uint32_t* ra, uint32_t w, uint32_t bar) {
+    // descriptors without their start address; per MMA the address is added in
+    const uint64_t da0 = sdesc(0u, kPixS * 16, 128), db0 = sdesc(0u, COUT * 16, 128);
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; ++kc) {
+            const uint32_t a_addr = ra[tap / 3] + (uint32_t)((2 * kc * kPixS + tap % 3) * 16);
+            const uint32_t b_addr = w + (uint32_t)((tap * (CIN / 8) + 2 * kc) * COUT * 16);
+            mma(dacc, da0 | (uint64_t)((a_addr >> 4) & 0x3FFFu), db0 | (uint64_t)((b_addr >> 4) & 0x3FFFu),
+                idesc<COUT>(), (tap | kc) ? 1u : 0u);
+        }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+
+// a layer's weights [9][COUT][CIN] (BF16) into the K-major operand layout [9][CIN/8][COUT][8]
+__device__ __forceinline__ void fetch_weights(const __nv_bfloat16* __restrict__ wt, int cin, int cout, uint32_t w) {
+    const int c8n = cin / 8;
+    for (int i = threadIdx.x; i < 9 * cout * c8n; i += kThreads) {
+        const int c8 = i % c8n, n = (i / c8n) % cout, tap = i / (c8n * cout);
+        cp16(w + (uint32_t)(((tap * c8n + c8) * cout + n) * 16), wt + ((size_t)tap * cout + n) * cin + c8 * 8);
+    }
+}
+
 // one input row (image b, row hh, pixels w0-1 .. w0+128 periodic) into a ring slot, asynchronously
 template <int CIN>
 __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, int b, int hh, int H, int W, int w0,
@@ -519,11 +555,11 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
             const int c = (n0 + j) / 4;
             float4* fz = reinterpret_cast<float4*>(stf + (px * CF + (c ^ (px % CF))) * 16);
             uint2* fb = reinterpret_cast<uint2*>(stb + (px * CB + (((n0 + j) / 8) ^ (px % CB))) * 16 + ((n0 + j) % 8) * 2);
-            if (EPI == EPI_GELU || EPI == EPI_LINEAR || EPI == EPI_PLANAR) {
+            if (EPI == EPI_GELU || EPI == EPI_LINEAR || EPI == EPI_PLANAR || EPI == EPI_GELU_ACT) {
                 const float4 z = make_float4(v[j] + breg[j], v[j + 1] + breg[j + 1], v[j + 2] + breg[j + 2],
                                              v[j + 3] + breg[j + 3]);
-                *fz = z;
-                if (EPI == EPI_GELU) {
+                if (EPI != EPI_GELU_ACT) *fz = z;
+                if (EPI == EPI_GELU || EPI == EPI_GELU_ACT) {
                     __nv_bfloat162 g2[2] = {__floats2bfloat162_rn(gelu(z.x), gelu(z.y)),
                                             __floats2bfloat162_rn(gelu(z.z), gelu(z.w))};
                     *fb = *reinterpret_cast<const uint2*>(g2);
@@ -552,7 +588,7 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
                 reinterpret_cast<const float*>(stf + (r * CF + (c ^ (r % CF))) * 16)[n % 4];
         }
     }
-    if (EPI == EPI_GELU || EPI == EPI_GELU_GRAD) {
+    if (EPI == EPI_GELU || EPI == EPI_GELU_GRAD || EPI == EPI_GELU_ACT) {
         for (int i = threadIdx.x; i < kTileP * CB; i += kThreads) {
             const int r = i / CB, c = i % CB;
             *reinterpret_cast<uint4*>(outb + (p0 + r) * COUT + c * 8) =
@@ -595,10 +631,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a + 8));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += kThreads) {
-        const int c8 = i % (CIN / 8), n = (i / (CIN / 8)) % COUT, tap = i / ((CIN / 8) * COUT);
-        tc::cp16(w_a + (uint32_t)((((tap * (CIN / 8)) + c8) * COUT + n) * 16), wt + ((size_t)tap * COUT + n) * CIN + c8 * 8);
-    }
+    tc::fetch_weights(wt, CIN, COUT, w_a);
     tc::cp_commit();
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -614,9 +647,6 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int j = 0; j < NCOL; ++j) breg[j] = (EPI == EPI_GELU_GRAD) ? 0.f : bias[n0 + j];
     }
-    // descriptors without their start address; per MMA the address is added in
-    const uint64_t da0 = tc::sdesc(0u, tc::kPixS * 16, 128), db0 = tc::sdesc(0u, COUT * 16, 128);
-
     // Ring slots are handed out round-robin, so the last six rows fetched sit in distinct slots.
     // A tile that continues the previous one (same image and segment, next row) reuses two of
     // its rows and needs one new row, usually prefetched during the previous tile; otherwise
@@ -660,22 +690,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int buf = (t - t0) & 1;
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t dacc = tmem + (uint32_t)(buf * NACC);
             const uint32_t ra[3] = {in_a + (uint32_t)(sl[0] * L::SLOT_BYTES), in_a + (uint32_t)(sl[1] * L::SLOT_BYTES),
                                     in_a + (uint32_t)(sl[2] * L::SLOT_BYTES)};
-#pragma unroll
-            for (int tap = 0; tap < 9; ++tap) {
-#pragma unroll
-                for (int kc = 0; kc < CIN / 16; ++kc) {
-                    const uint32_t a_addr = ra[tap / 3] + (uint32_t)((2 * kc * tc::kPixS + tap % 3) * 16);
-                    const uint32_t b_addr = w_a + (uint32_t)((tap * (CIN / 8) + 2 * kc) * COUT * 16);
-                    tc::mma(dacc, da0 | (uint64_t)((a_addr >> 4) & 0x3FFFu), db0 | (uint64_t)((b_addr >> 4) & 0x3FFFu),
-                            tc::idesc<COUT>(), (tap | kc) ? 1u : 0u);
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                             bar_a + 8u * (uint32_t)buf)
-                         : "memory");
+            tc::issue_tile<CIN, COUT>(tmem + (uint32_t)(buf * NACC), ra, w_a, bar_a + 8u * (uint32_t)buf);
         }
         // the next tile's new row, if it continues this one.  Only when this tile continued the
         // previous one (or is the first): after a fresh three-row fetch the six slots hold the
@@ -734,6 +751,200 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// ---- all layers of an inference in one launch (small batches) --------------------------------
+// When every tile (one image row segment) of a batch has a CTA of its own, the network runs as a
+// single cooperative launch: CTA t computes tile t of every layer in turn.  Layer l of tile
+// (b, h) needs layer l-1 of rows h-1, h, h+1: its own row is its own previous output, the other
+// two come from the CTAs of the neighbouring rows, which publish each finished layer by
+// incrementing their flag (release after a device-scope fence; the reader polls with an acquire
+// load, bounded).  Flags count up across launches: a CTA reads its own flag at entry (every flag
+// holds the same value between launches, since each launch adds L-1 to each) and waits for its
+// neighbours' flags to reach that base + l.  Each layer writes its own activation buffer, so no
+// row is overwritten while a neighbour may still read it.  The next layer's weights are fetched
+// while the epilogue drains the accumulator.  A wait that runs out sets bit 2 of the error word
+// and the CTA skips its remaining layers; its neighbours then run out too, so the launch ends.
+constexpr int kMaxFusedLayers = 8;
+constexpr long long kFlagLimit = 1LL << 21;
+
+struct FusedArgs {
+    const __nv_bfloat16* x;                       // input [B][H][W][ci[0]]
+    __nv_bfloat16* act[kMaxFusedLayers];          // act[l]: input of layer l (l >= 1), [B][H][W][ci[l]]
+    const __nv_bfloat16* wt[kMaxFusedLayers];     // [9][co][ci] BF16
+    const float* bias[kMaxFusedLayers];
+    int ci[kMaxFusedLayers], co[kMaxFusedLayers];
+    int L, B, H, W, planar;
+    float* y;                                     // last layer: planar [co][B*H*W] or [B][H][W][co]
+    unsigned int* flags;                          // one per tile
+    int* err;
+};
+
+namespace tc {
+// shared-memory plan of the fused kernel: three row slots (rows h-1, h, h+1) of up to 64
+// channels, one weight block, the accumulator barrier, FP32 and BF16 output staging; the
+// operand region also covers reads under the swapped reading of the descriptor strides
+struct FusedLay {
+    static constexpr int SLOT_BYTES = 8 * kPixS * 16;
+    static constexpr int IN_BYTES = 3 * SLOT_BYTES;
+    static constexpr int W_OFF = (IN_BYTES + 1023) / 1024 * 1024;
+    static constexpr int W_BYTES = 9 * 8 * 64 * 16;
+    static constexpr int BAR_OFF = (W_OFF + W_BYTES + 1023) / 1024 * 1024;
+    static constexpr int A_LAST = 2 * SLOT_BYTES + (6 * kPixS + 2) * 16;
+    static constexpr int B_LAST = W_OFF + (8 * 8 + 8 - 2) * 64 * 16;
+    static constexpr int A_END = A_LAST + imax(kPixS * 16 + 15 * 128, 15 * kPixS * 16 + 128) + 128;
+    static constexpr int B_END = B_LAST + imax(64 * 16 + 7 * 128, 7 * 64 * 16 + 128) + 128;
+    static constexpr int OPS_END = (imax(BAR_OFF + 64, imax(A_END, B_END)) + 1023) / 1024 * 1024;
+    static constexpr int STF_OFF = OPS_END;
+    static constexpr int STB_OFF = STF_OFF + kTileP * 64 * 4;
+    static constexpr int SMEM = STB_OFF + kTileP * 64 * 2;
+    static constexpr int TMEM_COLS = 64;
+};
+
+__device__ __forceinline__ bool wait_flag(const unsigned int* f, unsigned int target) {
+    for (long long i = 0; i < kFlagLimit; ++i) {
+        unsigned int v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(f) : "memory");
+        if ((int)(v - target) >= 0) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+}  // namespace tc
+
+// One layer of the fused inference for this CTA's tile.  Returns false if a wait ran out.
+template <int CIN, int COUT, int EPI>
+__device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, int tup, int tdn, int b, int h, int w0,
+                                            unsigned int base, uint32_t in_a, uint32_t w_a, uint32_t bar_a,
+                                            uint32_t& phase, uint32_t tmem, unsigned char* stf, unsigned char* stb) {
+    using FL = tc::FusedLay;
+    const int H = a.H, W = a.W;
+    const __nv_bfloat16* src = l == 0 ? a.x : a.act[l];
+    // the own row needs no wait: it is this CTA's previous output (or the input)
+    tc::fetch_row<CIN>(src, b, h, H, W, w0, in_a + (uint32_t)FL::SLOT_BYTES);
+    tc::cp_commit();
+    bool ok = true;
+    if (l > 0 && threadIdx.x == 0)
+        ok = tc::wait_flag(a.flags + tup, base + (unsigned)l) && tc::wait_flag(a.flags + tdn, base + (unsigned)l);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.err, 2);
+        tc::cp_wait_all();
+        return false;
+    }
+    tc::fetch_row<CIN>(src, b, (h - 1 + H) % H, H, W, w0, in_a);
+    tc::fetch_row<CIN>(src, b, (h + 1) % H, H, W, w0, in_a + 2u * (uint32_t)FL::SLOT_BYTES);
+    tc::cp_commit();
+    tc::cp_wait_all();   // the rows and this layer's weights
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t ra[3] = {in_a, in_a + (uint32_t)FL::SLOT_BYTES, in_a + 2u * (uint32_t)FL::SLOT_BYTES};
+        tc::issue_tile<CIN, COUT>(tmem, ra, w_a, bar_a);
+    }
+    ok = tc::bar_wait(bar_a, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.err, 1);
+        tc::bar_wait(bar_a, phase ^ 1u);   // once more, bounded, before the caller frees the TMEM
+        return false;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    // the MMAs have read the weights: fetch the next layer's while the accumulator drains
+    if (l + 1 < a.L) {
+        tc::fetch_weights(a.wt[l + 1], a.ci[l + 1], a.co[l + 1], w_a);
+        tc::cp_commit();
+    }
+    const int warp = threadIdx.x / 32;
+    float breg[COUT == 64 ? 32 : 16];
+    {
+        constexpr int NCOL = COUT == 64 ? 32 : 16;
+        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+#pragma unroll
+        for (int j = 0; j < NCOL; ++j) breg[j] = a.bias[l][n0 + j];
+    }
+    const size_t p0 = ((size_t)b * H + h) * W + w0;
+    conv_tc_epilogue<CIN, COUT, EPI>(tmem, p0, breg, a.y, EPI == EPI_GELU_ACT ? a.act[l + 1] : nullptr, nullptr, stf,
+                                     stb, (size_t)a.B * H * W);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    if (l + 1 < a.L) {   // publish the row
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(a.flags + t, 1u);
+    } else {
+        __syncthreads();
+    }
+    return true;
+}
+
+template <int EPI>
+__device__ __forceinline__ bool fused_dispatch(const FusedArgs& a, int l, int t, int tup, int tdn, int b, int h,
+                                               int w0, unsigned int base, uint32_t in_a, uint32_t w_a, uint32_t bar_a,
+                                               uint32_t& phase, uint32_t tmem, unsigned char* stf, unsigned char* stb) {
+    const int ci = a.ci[l], co = a.co[l];
+    if (ci == 16 && co == 64)
+        return fused_layer<16, 64, EPI>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+    if (ci == 64 && co == 64)
+        return fused_layer<64, 64, EPI>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+    if (ci == 64 && co == 16)
+        return fused_layer<64, 16, EPI>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+    return fused_layer<16, 16, EPI>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_cnn_fused(FusedArgs a) {
+    QGN_PDL_ENTRY();
+    using FL = tc::FusedLay;
+    extern __shared__ __align__(1024) unsigned char smtc[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smtc + FL::BAR_OFF);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smtc + FL::BAR_OFF + 32);
+    unsigned int* sbase = reinterpret_cast<unsigned int*>(smtc + FL::BAR_OFF + 40);
+    const int warp = threadIdx.x / 32;
+    const uint32_t bar_a = smem_u32(bar), in_a = smem_u32(smtc), w_a = smem_u32(smtc + FL::W_OFF);
+    const int H = a.H, segs = a.W / kTileP;
+    const int t = blockIdx.x;
+    const int h = t % H, bs = t / H;
+    const int w0 = (bs % segs) * kTileP, b = bs / segs;
+    const int tup = t - h + (h - 1 + H) % H, tdn = t - h + (h + 1) % H;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "r"((uint32_t)FL::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        unsigned int v;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(a.flags + t) : "memory");
+        *sbase = v;
+    }
+    tc::fetch_weights(a.wt[0], a.ci[0], a.co[0], w_a);
+    tc::cp_commit();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+    const unsigned int base = *sbase;
+    unsigned char* stf = smtc + FL::STF_OFF;
+    unsigned char* stb = smtc + FL::STB_OFF;
+    uint32_t phase = 0u;
+    for (int l = 0; l < a.L; ++l) {
+        bool ok;
+        if (l + 1 < a.L)
+            ok = fused_dispatch<EPI_GELU_ACT>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+        else if (a.planar)
+            ok = fused_dispatch<EPI_PLANAR>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+        else
+            ok = fused_dispatch<EPI_LINEAR>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
+        if (!ok) break;
+    }
+    tc::cp_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)FL::TMEM_COLS));
+    }
+}
+
 template <int CIN, int COUT>
 constexpr int conv_smem() {
     return (9 * COUT + 3 * (kTileP + 2)) * RowPad<CIN>::LD * 2;
@@ -767,8 +978,13 @@ struct qgn_cnn {
     double* loss_host = nullptr;
     float* ytgt = nullptr;                           // gathered targets
     long long adam_t = 0;
-    int engine = 0;                                  // 0: tcgen05 (TMEM accumulators), 1: mma.sync
+    int engine = 0;                                  // 0: tcgen05, all layers in one launch when the
+                                                     // tiles fit one CTA each; 1: mma.sync; 2: tcgen05
+                                                     // one launch per layer
     int* d_err = nullptr;                            // device error word of the tcgen05 kernels
+    unsigned int* flags = nullptr;                   // per-tile layer counters of the fused inference
+    int fused_tiles = -1;                            // tile count the flags were last used with
+    int fused_max_tiles = 0;                         // co-resident CTAs of the fused kernel
     std::vector<void*> owned;
     std::string last_error;
 };
@@ -927,7 +1143,69 @@ int check_err(qgn_cnn* net) {
     int h = 0;
     NCK(cudaMemcpyAsync(&h, net->d_err, sizeof(int), cudaMemcpyDeviceToHost, net->stream));
     NCK(cudaStreamSynchronize(net->stream));
-    if (h) return cnn_err(net, QGN_ERR_CUDA, "a tensor-core convolution timed out waiting for its MMAs");
+    if (h) {
+        net->fused_tiles = -1;   // the layer counters may be uneven: the next fused launch clears them
+        return cnn_err(net, QGN_ERR_CUDA,
+                       (h & 2) ? "the fused inference timed out waiting for a neighbouring row"
+                               : "a tensor-core convolution timed out waiting for its MMAs");
+    }
+    return QGN_OK;
+}
+
+// the fused single-launch inference applies: tcgen05 engine, at most kMaxFusedLayers layers,
+// 128-pixel row segments, at least 3 rows, and one co-resident CTA per tile
+bool fused_ok(qgn_cnn* net, int batch) {
+    if (net->engine != 0 || net->layers > kMaxFusedLayers || net->H < 3 || net->W % kTileP != 0) return false;
+    if (net->fused_max_tiles == 0) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaFuncSetAttribute(k_cnn_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::FusedLay::SMEM) !=
+                cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cnn_fused, kThreads, tc::FusedLay::SMEM) !=
+                cudaSuccess)
+            per = 0;
+        net->fused_max_tiles = per > 0 ? sms * per : -1;
+    }
+    return (long long)batch * net->H * (net->W / kTileP) <= net->fused_max_tiles;
+}
+
+int forward_fused(qgn_cnn* net, int batch, const __nv_bfloat16* x, float* y, bool planar) {
+    const int L = net->layers;
+    const int tiles = batch * net->H * (net->W / kTileP);
+    if (tiles != net->fused_tiles) {
+        NCK(cudaMemsetAsync(net->flags, 0, sizeof(unsigned int) * tiles, net->stream));
+        net->fused_tiles = tiles;
+    }
+    FusedArgs a = {};
+    a.x = x;
+    for (int l = 0; l < L; ++l) {
+        a.act[l] = net->act[l];
+        a.wt[l] = net->wf[l];
+        a.bias[l] = net->bias[l];
+        a.ci[l] = net->ci[l];
+        a.co[l] = net->co[l];
+    }
+    a.L = L;
+    a.B = batch;
+    a.H = net->H;
+    a.W = net->W;
+    a.planar = planar ? 1 : 0;
+    a.y = y;
+    a.flags = net->flags;
+    a.err = net->d_err;
+    // cooperative: every CTA is resident at once, which the waits on neighbouring rows need
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = tc::FusedLay::SMEM;
+    cfg.stream = net->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    NCK(cudaLaunchKernelEx(&cfg, k_cnn_fused, a));
     return QGN_OK;
 }
 
@@ -954,7 +1232,8 @@ int infer(qgn_cnn* net, const void* x, float* y, int batch, cudaStream_t stream,
     if (batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
     cudaStream_t own = net->stream;
     net->stream = stream;
-    const int rc = forward(net, batch, static_cast<const __nv_bfloat16*>(x), y, planar);
+    const __nv_bfloat16* xb = static_cast<const __nv_bfloat16*>(x);
+    const int rc = fused_ok(net, batch) ? forward_fused(net, batch, xb, y, planar) : forward(net, batch, xb, y, planar);
     net->stream = own;
     return rc;
 }
@@ -1024,10 +1303,11 @@ int qgn_cnn_create(int cin, int width, int cout, int layers, int H, int W, int m
     if (nalloc(net, &net->act[layers], 16) || nalloc(net, &net->gA, NP * net->width) ||
         nalloc(net, &net->gB, NP * net->width) || nalloc(net, &net->part, part) ||
         nalloc(net, &net->loss_part, 148) || nalloc(net, &net->ytgt, NP * pad16(cout)) ||
-        nalloc(net, &net->d_err, 1))
+        nalloc(net, &net->d_err, 1) || nalloc(net, &net->flags, 1024))
         return fail(QGN_ERR_CUDA);
     net->part_elems = part;
-    if (const char* e = std::getenv("QGN_CNN_MMA")) net->engine = (std::string(e) == "sync") ? 1 : 0;
+    if (const char* e = std::getenv("QGN_CNN_MMA"))
+        net->engine = (std::string(e) == "sync") ? 1 : (std::string(e) == "layers") ? 2 : 0;
     if (cudaMallocHost((void**)&net->loss_host, sizeof(double) * 148) != cudaSuccess) return fail(QGN_ERR_CUDA);
     if (cudaStreamSynchronize(net->stream) != cudaSuccess) return fail(QGN_ERR_CUDA);
     *out = net;
@@ -1157,7 +1437,7 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
 }
 
 int qgn_cnn_set_engine(qgn_cnn* net, int engine) {
-    if (!net || engine < 0 || engine > 1) return QGN_ERR_ARG;
+    if (!net || engine < 0 || engine > 2) return QGN_ERR_ARG;
     if (cudaStreamSynchronize(net->stream) != cudaSuccess) return QGN_ERR_CUDA;
     net->engine = engine;
     return QGN_OK;

@@ -1,14 +1,16 @@
 // fft.cuh -- FP64 shared-memory FFT building blocks for sm_100a.
 //
 // A transform of length N (power of two, 16..2048) is carried out by G = N/T threads
-// (T = 16 elements per thread, fewer for N < 16) as a sequence of Stockham
-// decimation-in-time radix passes: radix 16 for every pass except the last, which
+// (T = TP elements per thread, TP = 16 or 32, fewer for N < TP) as a sequence of Stockham
+// decimation-in-time radix passes: radix TP for every pass except the last, which
 // takes the remaining factor.  Each pass reads T values from shared memory into
 // registers, applies the inter-pass twiddles, performs register-resident radix-R
 // DFTs and writes the results back in place (the load and store halves of a pass
-// are separated by a block barrier).  Indices are padded by one element per 16
+// are separated by a barrier).  Indices are padded by one element per 16
 // (p -> p + p/16) so that both the strided stores of the first pass and the
 // contiguous accesses of later passes are free of 16-byte bank-group conflicts.
+// TP = 32 halves the shared-memory round trips of a 512- or 1024-point transform (two
+// passes instead of three) at twice the registers; the FP32 transforms use it.
 //
 // Twiddles come from a per-length table tw[m] = exp(-2*pi*i*m/N) computed on the
 // host in long double; DIR=-1 is the forward (exp(-i...)) transform of MKL's
@@ -80,7 +82,39 @@ __device__ __forceinline__ CT rot16(CT a, int m) {
     return cmk<CT>(a.x * c - a.y * s, a.x * s + a.y * c);
 }
 
-// In-register DFT of length R (1,2,4,8,16), natural order in and out, sign DIR.
+// Multiply by exp(DIR * 2*pi*i * m/32) for 0 <= m < 16; m is a compile-time constant after
+// unrolling.  Even m reduce to rot16; odd m use cos and sin of pi/16 and 3*pi/16.
+template <int DIR, class CT>
+__device__ __forceinline__ CT rot32(CT a, int m) {
+    using R = typename CTraits<CT>::R;
+    if ((m & 1) == 0) return rot16<DIR>(a, m >> 1);
+    constexpr R A = (R)0.98078528040323044913;  // cos(pi/16)
+    constexpr R B = (R)0.19509032201612826785;  // sin(pi/16)
+    constexpr R E = (R)0.83146961230254523708;  // cos(3 pi/16)
+    constexpr R F = (R)0.55557023301960222474;  // sin(3 pi/16)
+    R c, s;
+    switch (m & 15) {
+        case 1: c = A; s = B; break;
+        case 3: c = E; s = F; break;
+        case 5: c = F; s = E; break;
+        case 7: c = B; s = A; break;
+        case 9: c = -B; s = A; break;
+        case 11: c = -F; s = E; break;
+        case 13: c = -E; s = F; break;
+        default: c = -A; s = B; break;  // 15
+    }
+    s = DIR * s;
+    return cmk<CT>(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+// Multiply by exp(DIR * 2*pi*i * k/R), 0 <= k < R/2.
+template <int R, int DIR, class CT>
+__device__ __forceinline__ CT rot_root(CT a, int k) {
+    if constexpr (R == 32) return rot32<DIR>(a, k);
+    else return rot16<DIR>(a, k * (16 / R));
+}
+
+// In-register DFT of length R (1,2,4,8,16,32), natural order in and out, sign DIR.
 template <int R, int DIR>
 struct RegDFT {
     template <class CT>
@@ -92,7 +126,7 @@ struct RegDFT {
         RegDFT<R / 2, DIR>::run(o);
 #pragma unroll
         for (int k = 0; k < R / 2; ++k) {
-            CT t = rot16<DIR>(o[k], k * (16 / R));
+            CT t = rot_root<R, DIR>(o[k], k);
             v[k] = cadd(e[k], t);
             v[k + R / 2] = csub(e[k], t);
         }
@@ -113,9 +147,9 @@ struct RegDFT<2, DIR> {
     }
 };
 
-template <int N>
+template <int N, int TP = 16>
 struct FFTShape {
-    static constexpr int T = N < 16 ? N : 16;   // elements per thread
+    static constexpr int T = N < TP ? N : TP;   // elements per thread
     static constexpr int G = N / T;             // threads per transform
 };
 
@@ -155,6 +189,17 @@ __device__ __forceinline__ void apply_twiddles(CT* v, int k, const CT* __restric
                     v[13] = cmul(v[13], cmul(w8, w5));
                     v[14] = cmul(v[14], cmul(w8, w6));
                     v[15] = cmul(v[15], cmul(w8, w7));
+                    if constexpr (R > 16) {
+                        // w^(16+r) = w16 * w^r; the low powers are formed again from the table
+                        const CT w16 = ldw(16);
+                        const CT u[8] = {w16, cmul(w16, w1), cmul(w16, w2), cmul(w16, w3),
+                                         cmul(w16, w4), cmul(w16, w5), cmul(w16, w6), cmul(w16, w7)};
+#pragma unroll
+                        for (int r = 0; r < 8; ++r) {
+                            v[16 + r] = cmul(v[16 + r], u[r]);
+                            v[24 + r] = cmul(v[24 + r], cmul(u[r], w8));
+                        }
+                    }
                 }
             }
         }
@@ -170,14 +215,26 @@ enum FftDst { DST_SMEM = 0, DST_FN = 1 };
 // write through st(idx, value); every other access goes to x.  Barriers: a pass that reads
 // the shared buffer it overwrites syncs between its reads and writes, and a pass that
 // writes the shared buffer syncs after its writes.  With SRC_FN the caller guarantees
-// that no thread still reads x when the pass starts writing it.
-template <int N, int NS, int DIR, int SRC, int DST, class CT, class Ld, class St>
+// that no thread still reads x when the pass starts writing it.  WS (warp-synchronous):
+// the G threads of a transform lie in one warp and share it with no thread that touches
+// another transform's buffer, so the barriers that only order accesses to x are __syncwarp;
+// the barrier after a loader that reads other buffers (SRC_FN_SMEM) and the barrier that
+// ends a transform written to shared memory (the caller may read across transforms) stay
+// block-wide.
+template <bool BLOCK, bool WS>
+__device__ __forceinline__ void fft_sync() {
+    if constexpr (WS && !BLOCK) __syncwarp();
+    else __syncthreads();
+}
+
+template <int N, int NS, int DIR, int SRC, int DST, int TP, bool WS, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
-    constexpr int T = FFTShape<N>::T;
-    constexpr int G = FFTShape<N>::G;
-    constexpr int R = (N / NS >= 16) ? 16 : N / NS;
+    constexpr int T = FFTShape<N, TP>::T;
+    constexpr int G = FFTShape<N, TP>::G;
+    constexpr int R = (N / NS >= TP) ? TP : N / NS;
     constexpr int BPT = T / R;
     constexpr int STRIDE = N / R;
+    constexpr bool LAST = (NS * R == N);
     CT v[T];
     if (active) {
 #pragma unroll
@@ -191,7 +248,7 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
             }
         }
     }
-    if constexpr (DST == DST_SMEM && SRC != SRC_FN) __syncthreads();
+    if constexpr (DST == DST_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
     if (active) {
 #pragma unroll
         for (int b = 0; b < BPT; ++b) {
@@ -208,18 +265,18 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
             }
         }
     }
-    if constexpr (DST == DST_SMEM) __syncthreads();
+    if constexpr (DST == DST_SMEM) fft_sync<LAST, WS>();
 }
 
-template <int N, int NS, int DIR, int SRC0, int DSTL, class CT, class Ld, class St>
+template <int N, int NS, int DIR, int SRC0, int DSTL, int TP, bool WS, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_rec(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
-    constexpr int R = (N / NS >= 16) ? 16 : N / NS;
+    constexpr int R = (N / NS >= TP) ? TP : N / NS;
     constexpr bool FIRST = (NS == 1);
     constexpr bool LAST = (NS * R == N);
     constexpr int SRC = FIRST ? SRC0 : SRC_SMEM;
     constexpr int DST = LAST ? DSTL : DST_SMEM;
-    fft_pass_io<N, NS, DIR, SRC, DST>(x, lane, active, tw, ld, st);
-    if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
+    fft_pass_io<N, NS, DIR, SRC, DST, TP, WS>(x, lane, active, tw, ld, st);
+    if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL, TP, WS>(x, lane, active, tw, ld, st);
 }
 
 template <class CT>
@@ -229,20 +286,21 @@ struct NoIOT {
 };
 using NoIO = NoIOT<double2>;
 
-// N-point transform of one slot by the G threads with lane in [0,G), reading its input
-// through ld (SRC0 = SRC_FN / SRC_FN_SMEM) or from x (SRC_SMEM, written and synced by the
-// caller) and delivering its output through st (DSTL = DST_FN) or into x (DST_SMEM, synced
-// on return).  Every thread of the block calls this (it may contain __syncthreads).
-template <int N, int DIR, int SRC0, int DSTL, class CT, class Ld, class St>
+// N-point transform of one slot by the G = FFTShape<N, TP>::G threads with lane in [0,G),
+// reading its input through ld (SRC0 = SRC_FN / SRC_FN_SMEM) or from x (SRC_SMEM, written and
+// synced by the caller) and delivering its output through st (DSTL = DST_FN) or into x
+// (DST_SMEM, synced block-wide on return).  Every thread of the block calls this (it may
+// contain __syncthreads).  WS as for fft_pass_io.
+template <int N, int DIR, int SRC0, int DSTL, int TP = 16, bool WS = false, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_fused(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld ld, St st) {
-    fft_rec<N, 1, DIR, SRC0, DSTL>(x, lane, active, tw, ld, st);
+    fft_rec<N, 1, DIR, SRC0, DSTL, TP, WS>(x, lane, active, tw, ld, st);
 }
 
 // In-place N-point transform of the padded array x (caller syncs before; ends with a barrier).
-template <int N, int DIR, class CT>
+template <int N, int DIR, int TP = 16, class CT>
 __device__ __forceinline__ void fft_block(CT* x, int lane, bool active, const CT* __restrict__ tw) {
     NoIOT<CT> io;
-    fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM>(x, lane, active, tw, io, io);
+    fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM, TP, false>(x, lane, active, tw, io, io);
 }
 
 }  // namespace qgn

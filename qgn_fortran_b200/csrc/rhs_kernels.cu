@@ -71,7 +71,8 @@ __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY,
 
 template <int NX, bool DRAG, class CT, int TV = 0>
 __global__ void __launch_bounds__(XCfg<NX, DRAG, CT, TV>::THREADS,
-                                  minb(XCfg<NX, DRAG, CT, TV>::THREADS, regcap<CT>(NX >= 1024 ? 112 : 128, 80)))
+                                  minb(XCfg<NX, DRAG, CT, TV>::THREADS,
+                                       XCfg<NX, DRAG, CT, TV>::TP == 32 ? 112 : regcap<CT>(NX >= 1024 ? 112 : 128, 80)))
     k_xpass(Geom g, int layer0, const CT* __restrict__ pq, const CT* __restrict__ pv,
             const CT* __restrict__ pu, CT* __restrict__ pp, CT* __restrict__ pd,
             const CT* __restrict__ twx) {
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
         return make_double2((double)yl[pix] * rsc, (double)yl[pix + NX] * rsc);
     };
     NoIO none;
-    fft_fused<NX, -1, SRC_FN, DST_SMEM>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
+    fft_fused<NX, -1, SRC_FN, DST_SMEM, C::TP, (C::G <= 32)>(sm + slot * C::TS, lane, rp < npairs, twx, ld, none);
     const int nkx = g.nkx;
     for (int e = tid; e < C::RP * nkx; e += C::THREADS) {
         const int r = e / nkx, k = e % nkx;
@@ -174,7 +175,7 @@ __global__ void __launch_bounds__(YInvCfg<NY>::THREADS, minb(YInvCfg<NY>::THREAD
         if (kx == 0 && m == 0) v = make_double2(0.0, 0.0);
         out[colbase + m] = v;
     };
-    fft_fused<NY, -1, SRC_FN, DST_FN>(sm + slot * C::TS, lane, true, twy, ld, st);
+    fft_fused<NY, -1, SRC_FN, DST_FN, C::TP>(sm + slot * C::TS, lane, true, twy, ld, st);
 }
 
 // ------------------------------------------------------------------------------------

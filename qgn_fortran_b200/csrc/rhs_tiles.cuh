@@ -44,9 +44,17 @@ __host__ __device__ constexpr int regcap(int fp64 = 128, int fp32 = 64) { return
 // the single-field launches; a non-zero value is the CTA size in threads (per slot group for
 // the x pass), the same for every transform length, which lets one launch cover fields of
 // different sizes (ensembles).
+// elements per thread of an x transform (fft.cuh): 32 for the FP32 512- and 1024-point
+// transforms of the single-field x pass (two radix passes instead of three, each transform in
+// one warp), 16 otherwise.  The y passes keep 16: their CTAs interleave columns across warps,
+// and at 32 elements they had half the threads per column and ran 1.3-1.7x slower on B200.
+template <class CT, int N, int TV>
+__host__ __device__ constexpr int fft_tp() { return (TV == 0 && sizeof(CT) == 8 && (N == 512 || N == 1024)) ? 32 : 16; }
+
 template <int NY, class CT = double2, int TV = 0>
 struct YInvCfg {
-    static constexpr int G = FFTShape<NY>::G;
+    static constexpr int TP = 16;
+    static constexpr int G = FFTShape<NY, TP>::G;
     static constexpr int TKX = TV == 0 ? cmin(cmax(4, 128 / G), 16) : cmax(1, TV / G);
     static constexpr int THREADS = TKX * G;
     static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT));
@@ -55,7 +63,8 @@ struct YInvCfg {
 
 template <int NX, bool DRAG, class CT = double2, int TV = 0>
 struct XCfg {
-    static constexpr int G = FFTShape<NX>::G;
+    static constexpr int TP = fft_tp<CT, NX, TV>();
+    static constexpr int G = FFTShape<NX, TP>::G;
     static constexpr int RP = cmax(1, (TV == 0 ? 64 : TV) / G);   // row pairs per CTA
     static constexpr int SP = DRAG ? 4 : 3;             // slots per row pair
     static constexpr int THREADS = SP * RP * G;
@@ -65,7 +74,8 @@ struct XCfg {
 
 template <int NY, bool DRAG, class CT = double2, int TV = 0>
 struct YFwdCfg {
-    static constexpr int G = FFTShape<NY>::G;
+    static constexpr int TP = 16;
+    static constexpr int G = FFTShape<NY, TP>::G;
     // tid ^ TKX stays in the warp
     static constexpr int TKX = TV == 0 ? cmin(cmax(2, 64 / G), 16) : cmin(cmax(1, TV / (2 * G)), 16);
     static constexpr int SLOTS = 2 * TKX;
@@ -182,7 +192,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             }
             return v;
         };
-        fft_fused<NY, +1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
+        fft_fused<NY, +1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ld, none);
         // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
         CT* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
         for (int e = tid; e < (NY / 2) * C::TKX; e += C::THREADS) {
@@ -233,7 +243,7 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
         return cmk<CT>(0.0, 0.0);
     };
     NoIOT<CT> none;
-    fft_fused<NX, +1, SRC_FN, DST_SMEM>(xs, lane, pair_ok && s_of < 3, twx, ld_inv, none);
+    fft_fused<NX, +1, SRC_FN, DST_SMEM, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < 3, twx, ld_inv, none);
 
     // ---- forward: slot 0 = u1 q1 + i v1 q1, 1 = u2 q2 + i v2 q2 (grid/(nx*ny) scaling as in
     //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
@@ -254,7 +264,8 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
         if (k < nkx) out[k] = v;
         else if (k > NX - nkx) out[g.nkxp + (NX - k)] = v;
     };
-    fft_fused<NX, -1, SRC_FN_SMEM, DST_FN>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd, st_fwd);
+    fft_fused<NX, -1, SRC_FN_SMEM, DST_FN, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd,
+                                                                   st_fwd);
 }
 
 // ------------------------------------------------------------------------------------
@@ -309,7 +320,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
         auto ldd = [&](int y) -> CT {
             return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, colok, C::TKX);
         };
-        fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ldd, none);
+        fft_fused<NY, -1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ldd, none);
         const RT dc = (RT)lc->dragc;
         for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
             const int cc = e / nky, m = e % nky;
@@ -329,7 +340,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
     auto ld = [&](int y) -> CT { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
                                                          fld, colok, C::TKX); };
-    fft_fused<NY, -1, SRC_FN, DST_SMEM>(xs, lane, true, twy, ld, none);
+    fft_fused<NY, -1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ld, none);
 
     const RT ub = (RT)lc->uBar[l], bq = (RT)lc->betaq[l];
     const RT ek = (RT)lc->ekman;
@@ -381,7 +392,8 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
 // ------------------------------------------------------------------------------------
 template <int NX, int TV = 0>
 struct X1Cfg {
-    static constexpr int G = FFTShape<NX>::G;
+    static constexpr int TP = 16;
+    static constexpr int G = FFTShape<NX, TP>::G;
     static constexpr int RP = cmax(1, (TV == 0 ? 128 : TV) / G);
     static constexpr int THREADS = RP * G;
     static constexpr int TS = slot_stride(NX, 2);
@@ -430,7 +442,7 @@ __device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const do
             xout[(pix + NX) * cin_p + chan] = __float2bfloat16_rn((float)(a.y * g.inv_nxny) * sf);
         }
     };
-    fft_fused<NX, +1, SRC_FN, DST_FN>(sm + slot * C::TS, lane, ok, twx, ld, st);
+    fft_fused<NX, +1, SRC_FN, DST_FN, C::TP, (C::G <= 32)>(sm + slot * C::TS, lane, ok, twx, ld, st);
     if (EPI == 0) {
         // block max of non-negative doubles (NaN as the largest bit pattern)
         unsigned long long bits = (unsigned long long)__double_as_longlong(mx);

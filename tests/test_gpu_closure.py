@@ -83,6 +83,32 @@ def test_tcgen05_and_mma_sync_engines_agree(cuda_ok, layers):
         assert rel(a, b) <= 1e-3
 
 
+@pytest.mark.parametrize("batch_seq", [(1,), (3, 1, 3, 2)])
+def test_fused_inference_equals_per_layer(cuda_ok, batch_seq):
+    """All layers in one cooperative launch (rows exchanged between CTAs through L2 with
+    per-tile counters) against one tcgen05 launch per layer: bit-identical outputs, also when
+    the batch, and so the number of tiles, changes between calls."""
+    import torch
+    net = cl.ClosureNet(nz=4, H=32, W=128, layers=6, max_batch=3, seed=21)
+    rng = np.random.default_rng(21)
+    net.set_weights([(w, 0.1 * rng.standard_normal(b.shape).astype(np.float32)) for w, b in net.get_weights()])
+    for i, batch in enumerate(batch_seq):
+        x, _ = sample(net, batch, 40 + i)
+        xd = to_dev_bf16(x)
+        outs = []
+        for engine in ("tcgen05", "tcgen05-layers"):
+            net.set_engine(engine)
+            y = torch.zeros((batch, net.H, net.W, net.cout_p), dtype=torch.float32, device="cuda")
+            net.forward(xd, y, batch)
+            net.check()
+            outs.append(y.cpu().numpy())
+        assert np.array_equal(outs[0], outs[1]), batch
+        ref, _, _ = CNNOracle(net.get_weights(), net.cout).forward(x)
+        # six layers of BF16 activations: an activation that rounds the other way in one layer
+        # (FP32 summation order differs from the oracle's) moves the output by ~1e-3
+        assert rel(outs[0], ref) <= 3e-3
+
+
 def test_cnn_gradients_match_oracle(cuda_ok):
     net, ws = small_net(seed=5)
     x, t = sample(net, 2, 2)
