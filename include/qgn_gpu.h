@@ -262,6 +262,9 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
 int qgn_cnn_set_engine(qgn_cnn* net, int engine);
 /* waits for the network's stream; QGN_ERR_CUDA if a tensor-core kernel reported a timeout */
 int qgn_cnn_check(qgn_cnn* net);
+/* failure injection for tests: set the fused inference's layer counter of one tile (a large
+ * value makes that tile's bounded wait run out in the next fused launch) */
+int qgn_cnn_debug_set_counter(qgn_cnn* net, int tile, unsigned int value);
 int qgn_cnn_stream(qgn_cnn* net, void** stream);
 const char* qgn_cnn_last_error(const qgn_cnn* net);
 int qgn_cnn_destroy(qgn_cnn* net);

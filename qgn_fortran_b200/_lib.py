@@ -79,6 +79,7 @@ SIGNATURES = {
                                      C.POINTER(C.c_double)]),
     "qgn_cnn_set_engine": (C.c_int, [C.c_void_p, C.c_int]),
     "qgn_cnn_check": (C.c_int, [C.c_void_p]),
+    "qgn_cnn_debug_set_counter": (C.c_int, [C.c_void_p, C.c_int, C.c_uint]),
     "qgn_cnn_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "qgn_cnn_last_error": (C.c_char_p, [C.c_void_p]),
     "qgn_cnn_destroy": (C.c_int, [C.c_void_p]),

@@ -101,6 +101,10 @@ class ClosureNet:
     def check(self):
         self._check(self.lib.qgn_cnn_check(self.net), "qgn_cnn_check")
 
+    def debug_set_counter(self, tile: int, value: int):
+        """Failure injection for tests: set one tile's layer counter of the fused inference."""
+        self._check(self.lib.qgn_cnn_debug_set_counter(self.net, tile, value), "qgn_cnn_debug_set_counter")
+
     def stream(self):
         sp = C.c_void_p()
         self._check(self.lib.qgn_cnn_stream(self.net, C.byref(sp)), "qgn_cnn_stream")

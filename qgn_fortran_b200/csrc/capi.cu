@@ -228,7 +228,7 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
         CK(launch_modal_mixed(g, b, b.q, f32(b.err), f32(b.psi), st));
         CK(launch_rhs32(g, b, f32(b.err), f32(b.psi), f32(b.N[0]), drag_on(ctx), st));
     } else {
-        CK(launch_modal(g, b.mc, b.q, b.psi, st));
+        CK(launch_modal(g, b, b.q, b.psi, st));
         // the learned closure (if attached): S of this step's state and the budget check that
         // keeps it (background A8) or falls back to the Leith A8L just computed
         if (ctx->closure) RET(closure_eval(ctx));
@@ -397,7 +397,7 @@ int step_bsrk3(qgn_ctx* ctx) {
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
     if (ctx->first_call) {
-        CK(launch_modal(g, b.mc, b.q, b.psi, st));
+        CK(launch_modal(g, b, b.q, b.psi, st));
         RET(rhs_of(ctx, b.q, b.psi, b.N[0]));     // RHS0 (kept between calls, FSAL)
         ctx->first_call = false;
     }
@@ -436,7 +436,7 @@ int step_rk4(qgn_ctx* ctx) {
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
-    CK(launch_modal(g, b.mc, b.q, b.psi, st));
+    CK(launch_modal(g, b, b.q, b.psi, st));
     RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
     Combo c1{{b.N[0]}, {0.5}, 1};
     CK(launch_combo(g, b, c1, b.q, b.Qs[1], b.psi, true, st));
@@ -459,7 +459,7 @@ int step_ab3(qgn_ctx* ctx) {
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
-    CK(launch_modal(g, b.mc, b.q, b.psi, st));
+    CK(launch_modal(g, b, b.q, b.psi, st));
     if (ctx->ab_calls == 0) {
         RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
         Combo c{{b.N[0]}, {1.0}, 1};
@@ -711,6 +711,8 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
         for (int k = 0; k < nz; ++k) Hw[k] = H[k] / p->Htot;
         if (e == cudaSuccess) e = cudaMemcpy(b.lc, &lc, sizeof(lc), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(b.mc, &mc, sizeof(mc), cudaMemcpyHostToDevice);
+        ctx->mc_host = mc;
+        b.mc_h = &ctx->mc_host;
         if (e == cudaSuccess) e = cudaMemcpy(b.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(b.Hw, Hw, sizeof(Hw), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) fail("constant upload", e);
@@ -807,7 +809,7 @@ int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
         CK(cudaStreamSynchronize(ctx->stream));
         return QGN_OK;
     }
-    CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
+    CK(launch_modal(ctx->g, b, b.err, b.psi, ctx->stream));
     CK(launch_rhs(ctx->g, b, b.err, b.psi, b.qnew, drag_on(ctx), ctx->stream));
     RET(download_full(ctx, b.qnew, rhs));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -821,7 +823,7 @@ int qgn_psi(qgn_ctx* ctx, const double* q_hat, double* psi_hat) {
     CK(cudaSetDevice(ctx->device));
     Buffers& b = ctx->b;
     RET(upload_kept(ctx, q_hat, b.err));
-    CK(launch_modal(ctx->g, b.mc, b.err, b.psi, ctx->stream));
+    CK(launch_modal(ctx->g, b, b.err, b.psi, ctx->stream));
     RET(download_full(ctx, b.psi, psi_hat));
     CK(cudaStreamSynchronize(ctx->stream));
     return QGN_OK;
@@ -850,7 +852,7 @@ int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins)
     const size_t need = (size_t)g.nz * (1 + (spectrum ? nbins : 0));
     if (b.diag) { cudaFree(b.diag); b.diag = nullptr; }
     CK(dalloc(&b.diag, need));
-    CK(launch_modal(g, b.mc, b.q, b.psi, ctx->stream));
+    CK(launch_modal(g, b, b.q, b.psi, ctx->stream));
     CK(launch_ke(g, b, b.psi, b.Hw, b.diag, ctx->stream));
     if (spectrum) CK(launch_ke_spectrum(g, b.psi, b.Hw, nbins, b.diag + g.nz, ctx->stream));
     CK(cudaMemcpyAsync(ke_layer, b.diag, sizeof(double) * g.nz, cudaMemcpyDeviceToHost, ctx->stream));
@@ -879,7 +881,7 @@ int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_
         CK(cudaMemcpyAsync(q_phys, b.phys, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (psi_phys) {
-        CK(launch_modal(g, b.mc, src, b.psi, ctx->stream));
+        CK(launch_modal(g, b, src, b.psi, ctx->stream));
         CK(launch_to_phys(g, b, b.psi, b.phys, ctx->stream));
         CK(cudaMemcpyAsync(psi_phys, b.phys, sizeof(double) * np, cudaMemcpyDeviceToHost, ctx->stream));
     }

@@ -331,11 +331,11 @@ int qgn_closure_snapshot(qgn_ctx* fine, qgn_ctx* coarse, const float* in_scale, 
         cudaMemcpyAsync(sc + 2 * nz, out_scale, sizeof(float) * nz, cudaMemcpyHostToDevice, s) != cudaSuccess)
         return QGN_ERR_CUDA;
     // high-resolution GetRHS (no hyperviscosity for implicit schemes: is_explicit as configured)
-    if (launch_modal(gf, bf.mc, bf.q, bf.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_modal(gf, bf, bf.q, bf.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_rhs(gf, bf, bf.q, bf.psi, bf.N[5], fine->p.C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (coarse_grain_on(fine, coarse, bf.N[5], bc.N[4], s) != cudaSuccess) return QGN_ERR_CUDA;
     // coarse GetRHS of the coarse-grained state
-    if (launch_modal(gc, bc.mc, bc.q, bc.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_modal(gc, bc, bc.q, bc.psi, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_rhs(gc, bc, bc.q, bc.psi, bc.N[5], coarse->p.C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
     ::qgn::launch(k_sub, grid_of(gc.csize()), 256, 0, s, gc.csize(), bc.N[4], bc.N[5], bc.err);
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;

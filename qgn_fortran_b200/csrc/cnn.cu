@@ -1145,6 +1145,7 @@ int check_err(qgn_cnn* net) {
     NCK(cudaStreamSynchronize(net->stream));
     if (h) {
         net->fused_tiles = -1;   // the layer counters may be uneven: the next fused launch clears them
+        NCK(cudaMemsetAsync(net->d_err, 0, sizeof(int), net->stream));   // reported once
         return cnn_err(net, QGN_ERR_CUDA,
                        (h & 2) ? "the fused inference timed out waiting for a neighbouring row"
                                : "a tensor-core convolution timed out waiting for its MMAs");
@@ -1440,6 +1441,16 @@ int qgn_cnn_set_engine(qgn_cnn* net, int engine) {
     if (!net || engine < 0 || engine > 2) return QGN_ERR_ARG;
     if (cudaStreamSynchronize(net->stream) != cudaSuccess) return QGN_ERR_CUDA;
     net->engine = engine;
+    return QGN_OK;
+}
+
+// failure injection for tests: set the fused inference's layer counter of one tile.  A large
+// value makes that tile's CTA wait, in the next fused launch, for neighbour counters that
+// never reach it; the bounded wait runs out and qgn_cnn_check reports it.
+int qgn_cnn_debug_set_counter(qgn_cnn* net, int tile, unsigned int value) {
+    if (!net || tile < 0 || tile >= 1024) return QGN_ERR_ARG;
+    NCK(cudaMemcpyAsync(net->flags + tile, &value, sizeof(value), cudaMemcpyHostToDevice, net->stream));
+    NCK(cudaStreamSynchronize(net->stream));
     return QGN_OK;
 }
 

@@ -51,6 +51,70 @@ struct ModalConst {
     double Htot;
 };
 
+// GetPsi constants of a fixed layer count (2, 4, 8, 16) passed by value as a kernel parameter:
+// the unrolled arithmetic reads the matrix entries straight from the constant bank, with no
+// shared-memory staging and no load instructions
+template <int NZ>
+struct ModalParams {
+    double proj[NZ * NZ];
+    double back[NZ * NZ];
+    double ev[NZ];
+    double Htot;
+};
+template <int NZ>
+inline ModalParams<NZ> modal_params(const ModalConst& mc) {
+    ModalParams<NZ> m;
+    for (int i = 0; i < NZ * NZ; ++i) {
+        m.proj[i] = mc.proj[i];
+        m.back[i] = mc.back[i];
+    }
+    for (int i = 0; i < NZ; ++i) m.ev[i] = mc.evals[i];
+    m.Htot = mc.Htot;
+    return m;
+}
+
+// The GetPsi constants as a kernel argument: by value for a fixed layer count, else the device
+// copy, which the kernel stages in shared memory (modal_view)
+template <int NZ>
+struct ModalArg {
+    ModalParams<NZ> m;
+};
+template <>
+struct ModalArg<0> {
+    const ModalConst* mc;
+};
+
+// shared-memory staging arrays of a GetPsi kernel (used only for NZ = 0)
+#define QGN_MODAL_SHARED(NZ)                                                      \
+    __shared__ double s_proj[(NZ) > 0 ? 1 : kMaxNZ * kMaxNZ];                     \
+    __shared__ double s_back[(NZ) > 0 ? 1 : kMaxNZ * kMaxNZ];                     \
+    __shared__ double s_ev[(NZ) > 0 ? 1 : kMaxNZ]
+
+struct ModalView {
+    const double* proj;
+    const double* back;
+    const double* ev;
+    double Htot;
+};
+
+// where the kernel reads the constants from; for NZ = 0 every thread of the block must call
+// this (it stages the device copy and synchronises)
+template <int NZ>
+__device__ __forceinline__ ModalView modal_view(const ModalArg<NZ>& a, double* s_proj, double* s_back, double* s_ev,
+                                                int nz) {
+    if constexpr (NZ > 0) {
+        return ModalView{a.m.proj, a.m.back, a.m.ev, a.m.Htot};
+    } else {
+        for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) {
+            s_proj[i] = a.mc->proj[i];
+            s_back[i] = a.mc->back[i];
+        }
+        for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = a.mc->evals[i];
+        __syncthreads();
+        return ModalView{s_proj, s_back, s_ev, a.mc->Htot};
+    }
+}
+
 // Device scalars of the adaptive controllers.  The controller kernel makes every
 // accept/reject/halt decision on the device, so a step can run without host round trips.
 struct DevScalars {
@@ -94,8 +158,16 @@ struct Buffers {
     double* snap = nullptr;           // closure training-sample work space (lazy)
     LayerConst* lc = nullptr;
     ModalConst* mc = nullptr;
+    const ModalConst* mc_h = nullptr;   // host copy of *mc, the source of ModalParams
     DevScalars* sc = nullptr;
 };
+
+// the kernel argument of the GetPsi constants (NZ = 0, or no host copy: the device copy)
+template <int NZ>
+inline ModalArg<NZ> modal_arg(const Buffers& b) {
+    if constexpr (NZ > 0) return ModalArg<NZ>{modal_params<NZ>(*b.mc_h)};
+    else return ModalArg<0>{b.mc};
+}
 
 }  // namespace qgn
 
@@ -118,6 +190,7 @@ struct qgn_ctx {
     bool halted = false;           // a step failed; cleared by the next state upload
     long long state_version = 0;   // bumped by every call that changes the state outside an ensemble
     qgn::Closure* closure = nullptr;   // learned closure of a coarse ARK43_QGLeith model (closure.cu)
+    qgn::ModalConst mc_host{};     // host copy of b.mc (b.mc_h points here)
     double* host_pin = nullptr;    // pinned scalar readback
     std::vector<void*> owned;      // every device allocation made at creation
     std::string last_error;
@@ -149,7 +222,7 @@ const double2* closure_tendency(const qgn_ctx* ctx);
 void drop_graphs(qgn_ctx* ctx);
 
 // ---- launch wrappers (rhs_kernels.cu) -------------------------------------------------
-cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, double2* psi, cudaStream_t s);
+cudaError_t launch_modal(const Geom& g, const Buffers& b, const double2* q, double2* psi, cudaStream_t s);
 // extra (optional, compact): a tendency added to the RHS on the kept modes (learned closure)
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
                        bool do_drag, cudaStream_t s, const double2* extra = nullptr);

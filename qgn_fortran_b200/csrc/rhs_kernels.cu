@@ -28,14 +28,12 @@
 namespace qgn {
 
 template <int NZ>
-__global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __restrict__ mc,
+__global__ void __launch_bounds__(256, 2) k_modal(Geom g, const __grid_constant__ ModalArg<NZ> ma,
                                                const double2* __restrict__ q, double2* __restrict__ psi) {
     QGN_PDL_ENTRY();
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    QGN_MODAL_SHARED(NZ);
     const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
-    __syncthreads();
+    const ModalView mv = modal_view<NZ>(ma, s_proj, s_back, s_ev, nz);
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
@@ -47,7 +45,7 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const ModalConst* __re
 #pragma unroll
     for (int k = 0; k < NZC; ++k)
         if (k < nz) qv[k] = q[(size_t)k * P + p];
-    modal_invert<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+    modal_invert<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int k = 0; k < NZC; ++k)
         if (k < nz) psi[(size_t)k * P + p] = pv[k];
@@ -212,16 +210,16 @@ static cudaError_t set_smem(K kernel, int bytes) {
     return e;
 }
 
-cudaError_t launch_modal(const Geom& g, const ModalConst* mc, const double2* q, double2* psi, cudaStream_t s) {
+cudaError_t launch_modal(const Geom& g, const Buffers& b, const double2* q, double2* psi, cudaStream_t s) {
     const size_t P = (size_t)g.nkx * g.nky;
     dim3 grid((unsigned)((P + 255) / 256));
     const double nb = 2.0 * 16.0 * (double)g.csize();
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<2>, grid, 256, 0, s, g, mc, q, psi)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<4>, grid, 256, 0, s, g, mc, q, psi)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<8>, grid, 256, 0, s, g, mc, q, psi)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<16>, grid, 256, 0, s, g, mc, q, psi)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<0>, grid, 256, 0, s, g, mc, q, psi)); break;
+    switch (b.mc_h ? g.nz : 0) {
+        case 2: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<2>, grid, 256, 0, s, g, modal_arg<2>(b), q, psi)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<4>, grid, 256, 0, s, g, modal_arg<4>(b), q, psi)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<8>, grid, 256, 0, s, g, modal_arg<8>(b), q, psi)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<16>, grid, 256, 0, s, g, modal_arg<16>(b), q, psi)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, s, ::qgn::launch(k_modal<0>, grid, 256, 0, s, g, modal_arg<0>(b), q, psi)); break;
     }
     return cudaGetLastError();
 }
@@ -618,7 +616,7 @@ cudaError_t launch_modal_fields(const Geom& g, const Buffers& b, const double2* 
     double* Pu = phys3 + np;
     double* Pv = phys3 + 2 * np;
     // GetPsi, u_hat, v_hat and the physical fields of the Jacobian (QGN_Module.f90:218-234)
-    if ((e = launch_modal(g, b.mc, q, b.psi, s)) != cudaSuccess) return e;
+    if ((e = launch_modal(g, b, q, b.psi, s)) != cudaSuccess) return e;
     QGN_LAUNCH(KID_LAYOUT, 48.0 * (double)g.csize(), s, ::qgn::launch(k_uv_hat, blocks, 256, 0, s, g, b.psi, fa, fb));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_to_phys(g, b, q, Pq, s)) != cudaSuccess) return e;

@@ -176,13 +176,14 @@ extern "C" int qgn_rhs_static(const qgn_params* p, const double* H, const double
     mc.Htot = p->Htot;
     if (cudaMemcpyAsync(b.lc, &lc, sizeof(lc), cudaMemcpyHostToDevice, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (cudaMemcpyAsync(b.mc, &mc, sizeof(mc), cudaMemcpyHostToDevice, s) != cudaSuccess) return QGN_ERR_CUDA;
+    b.mc_h = &mc;   // read while this call launches its kernels
 
     ::qgn::launch(k_twiddle_table, (g.nx + 255) / 256, 256, 0, s, g.nx, b.twx);
     ::qgn::launch(k_twiddle_table, (g.ny + 255) / 256, 256, 0, s, g.ny, b.twy);
     const int blocks = 148 * 8;
     ::qgn::launch(k_full_to_compact_dev, blocks, 256, 0, s, g, reinterpret_cast<const double2*>(q_hat_dev), qc);
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
-    if (launch_modal(g, b.mc, qc, pc, s) != cudaSuccess) return QGN_ERR_CUDA;
+    if (launch_modal(g, b, qc, pc, s) != cudaSuccess) return QGN_ERR_CUDA;
     if (launch_rhs(g, b, qc, pc, oc, p->C_d != 0.0, s) != cudaSuccess) return QGN_ERR_CUDA;
     ::qgn::launch(k_compact_to_full_dev, blocks, 256, 0, s, g, oc, reinterpret_cast<double2*>(rhs_dev));
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;

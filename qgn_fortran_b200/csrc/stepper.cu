@@ -236,14 +236,12 @@ __global__ void __launch_bounds__(256) k_ark_comb(Geom g, CombPtrs<T> cp, const 
 
 // GetPsi of an FP32 field with FP64 arithmetic (mixed mode)
 template <int NZ>
-__global__ void __launch_bounds__(256, 2) k_modal_f32(Geom g, const ModalConst* __restrict__ mc,
+__global__ void __launch_bounds__(256, 2) k_modal_f32(Geom g, const __grid_constant__ ModalArg<NZ> ma,
                                                       const float2* __restrict__ q, float2* __restrict__ psi) {
     QGN_PDL_ENTRY();
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    QGN_MODAL_SHARED(NZ);
     const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
-    __syncthreads();
+    const ModalView mv = modal_view<NZ>(ma, s_proj, s_back, s_ev, nz);
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
@@ -258,7 +256,7 @@ __global__ void __launch_bounds__(256, 2) k_modal_f32(Geom g, const ModalConst* 
             const float2 v = q[(size_t)l * P + p];
             qv[l] = make_double2(v.x, v.y);
         }
-    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+    modal_invert_s<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int l = 0; l < NZC; ++l)
         if (l < nz) psi[(size_t)l * P + p] = make_float2((float)pv[l].x, (float)pv[l].y);
@@ -313,15 +311,13 @@ __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp
 
 // FP32 copy of the FP64 state and its GetPsi (FP64 arithmetic, FP32 result)
 template <int NZ>
-__global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const ModalConst* __restrict__ mc,
+__global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const __grid_constant__ ModalArg<NZ> ma,
                                                      const double2* __restrict__ q, float2* __restrict__ q32,
                                                      float2* __restrict__ psi32) {
     QGN_PDL_ENTRY();
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    QGN_MODAL_SHARED(NZ);
     const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
-    __syncthreads();
+    const ModalView mv = modal_view<NZ>(ma, s_proj, s_back, s_ev, nz);
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
@@ -333,7 +329,7 @@ __global__ void __launch_bounds__(256, 2) k_modal_mixed(Geom g, const ModalConst
 #pragma unroll
     for (int l = 0; l < NZC; ++l)
         if (l < nz) qv[l] = q[(size_t)l * P + p];
-    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+    modal_invert_s<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int l = 0; l < NZC; ++l) {
         if (l < nz) {
@@ -353,14 +349,12 @@ __global__ void k_f2d(size_t n, const float2* __restrict__ a, double2* __restric
 template <int NZ>
 __global__ void __launch_bounds__(256, 2) k_combo(Geom g, Combo cb, const double2* __restrict__ q,
                                                double2* __restrict__ out, double2* __restrict__ psi,
-                                               const ModalConst* __restrict__ mc,
+                                               const __grid_constant__ ModalArg<NZ> ma,
                                                const DevScalars* __restrict__ sc, int want_psi) {
     QGN_PDL_ENTRY();
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    QGN_MODAL_SHARED(NZ);
     const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
-    __syncthreads();
+    const ModalView mv = modal_view<NZ>(ma, s_proj, s_back, s_ev, nz);
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
@@ -384,7 +378,7 @@ __global__ void __launch_bounds__(256, 2) k_combo(Geom g, Combo cb, const double
             qv[l] = v;
         }
     }
-    if (want_psi) modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+    if (want_psi) modal_invert_s<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int l = 0; l < NZC; ++l) {
         if (l < nz) {
@@ -627,14 +621,12 @@ template <int S, int NZ>
 __global__ void __launch_bounds__(256, 2) k_ark_stage_small(Geom g, CombPtrs<double2> cp, const double2* __restrict__ q,
                                                            double2* __restrict__ qout, double2* __restrict__ psi,
                                                            const LayerConst* __restrict__ lc,
-                                                           const ModalConst* __restrict__ mc,
+                                                           const __grid_constant__ ModalArg<NZ> ma,
                                                            const DevScalars* __restrict__ sc) {
     QGN_PDL_ENTRY();
-    __shared__ double s_proj[kMaxNZ * kMaxNZ], s_back[kMaxNZ * kMaxNZ], s_ev[kMaxNZ];
+    QGN_MODAL_SHARED(NZ);
     const int nz = g.nz;
-    for (int i = threadIdx.x; i < nz * nz; i += blockDim.x) { s_proj[i] = mc->proj[i]; s_back[i] = mc->back[i]; }
-    for (int i = threadIdx.x; i < nz; i += blockDim.x) s_ev[i] = mc->evals[i];
-    __syncthreads();
+    const ModalView mv = modal_view<NZ>(ma, s_proj, s_back, s_ev, nz);
     const size_t P = (size_t)g.nkx * g.nky;
     const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
@@ -663,7 +655,7 @@ __global__ void __launch_bounds__(256, 2) k_ark_stage_small(Geom g, CombPtrs<dou
             qout[e] = qv[l];
         }
     }
-    modal_invert_s<NZ>(s_proj, s_back, s_ev, mc->Htot, nz, k2, p == 0, qv, pv);
+    modal_invert_s<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int l = 0; l < NZC; ++l)
         if (l < nz) psi[(size_t)l * P + p] = pv[l];
@@ -680,11 +672,11 @@ static cudaError_t launch_stage_small_nz(const Geom& g, const Buffers& b, int s,
     const double C = (double)g.csize(), nb = 16.0 * C * (2.0 * s + 2.0);
     double2* qo = b.Qs[s];
     switch (s) {
-        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<1, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<2, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<3, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<4, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
-        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<5, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, b.mc, b.sc))); break;
+        case 1: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<1, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, modal_arg<NZ>(b), b.sc))); break;
+        case 2: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<2, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, modal_arg<NZ>(b), b.sc))); break;
+        case 3: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<3, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, modal_arg<NZ>(b), b.sc))); break;
+        case 4: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<4, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, modal_arg<NZ>(b), b.sc))); break;
+        case 5: QGN_LAUNCH(KID_STAGE, nb, st, (::qgn::launch(k_ark_stage_small<5, NZ>, nbk, 256, 0, st, g, cp, b.q, qo, b.psi, b.lc, modal_arg<NZ>(b), b.sc))); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -694,19 +686,19 @@ cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, f
     const size_t P = (size_t)g.nkx * g.nky;
     dim3 grid(blocks_for(P, 256));
     const double nb = 16.0 * (double)g.csize();
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<2>, grid, 256, 0, st, g, b.mc, q, psi)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<4>, grid, 256, 0, st, g, b.mc, q, psi)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<8>, grid, 256, 0, st, g, b.mc, q, psi)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<16>, grid, 256, 0, st, g, b.mc, q, psi)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<0>, grid, 256, 0, st, g, b.mc, q, psi)); break;
+    switch (b.mc_h ? g.nz : 0) {
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<2>, grid, 256, 0, st, g, modal_arg<2>(b), q, psi)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<4>, grid, 256, 0, st, g, modal_arg<4>(b), q, psi)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<8>, grid, 256, 0, st, g, modal_arg<8>(b), q, psi)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<16>, grid, 256, 0, st, g, modal_arg<16>(b), q, psi)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_f32<0>, grid, 256, 0, st, g, modal_arg<0>(b), q, psi)); break;
     }
     return cudaGetLastError();
 }
 
 // stage s of ARK4(3)6L[2]SA: q_s (streaming combination), then psi_s = GetPsi(q_s)
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
-    if (g.csize() <= kSmallStage) {
+    if (g.csize() <= kSmallStage && b.mc_h) {
         switch (g.nz) {
             case 2: return launch_stage_small_nz<2>(g, b, s, st);
             case 4: return launch_stage_small_nz<4>(g, b, s, st);
@@ -717,7 +709,7 @@ cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_
     }
     cudaError_t e = launch_comb<double2>(g, b, s, st);
     if (e != cudaSuccess) return e;
-    return launch_modal(g, b.mc, b.Qs[s], b.psi, st);
+    return launch_modal(g, b, b.Qs[s], b.psi, st);
 }
 
 static StagePtrs32 stage_ptrs32(const Buffers& b) {
@@ -748,12 +740,12 @@ cudaError_t launch_modal_mixed(const Geom& g, const Buffers& b, const double2* q
     const size_t P = (size_t)g.nkx * g.nky;
     dim3 grid(blocks_for(P, 256));
     const double nb = 32.0 * (double)g.csize();
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<2>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
-        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<4>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
-        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<8>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
-        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<16>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
-        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<0>, grid, 256, 0, st, g, b.mc, q, q32, psi32)); break;
+    switch (b.mc_h ? g.nz : 0) {
+        case 2: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<2>, grid, 256, 0, st, g, modal_arg<2>(b), q, q32, psi32)); break;
+        case 4: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<4>, grid, 256, 0, st, g, modal_arg<4>(b), q, q32, psi32)); break;
+        case 8: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<8>, grid, 256, 0, st, g, modal_arg<8>(b), q, q32, psi32)); break;
+        case 16: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<16>, grid, 256, 0, st, g, modal_arg<16>(b), q, q32, psi32)); break;
+        default: QGN_LAUNCH(KID_MODAL, nb, st, ::qgn::launch(k_modal_mixed<0>, grid, 256, 0, st, g, modal_arg<0>(b), q, q32, psi32)); break;
     }
     return cudaGetLastError();
 }
@@ -777,12 +769,12 @@ cudaError_t launch_combo(const Geom& g, const Buffers& b, const Combo& cb, const
     dim3 grid(blocks_for(P, 256));
     const int wp = want_psi ? 1 : 0;
     const double nb = 16.0 * (double)g.csize() * (1.0 + cb.n + 1.0 + wp);
-    switch (g.nz) {
-        case 2: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<2>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 4: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<4>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 8: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<8>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        case 16: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<16>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
-        default: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<0>, grid, 256, 0, st, g, cb, q, out, psi, b.mc, b.sc, wp)); break;
+    switch (b.mc_h ? g.nz : 0) {
+        case 2: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<2>, grid, 256, 0, st, g, cb, q, out, psi, modal_arg<2>(b), b.sc, wp)); break;
+        case 4: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<4>, grid, 256, 0, st, g, cb, q, out, psi, modal_arg<4>(b), b.sc, wp)); break;
+        case 8: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<8>, grid, 256, 0, st, g, cb, q, out, psi, modal_arg<8>(b), b.sc, wp)); break;
+        case 16: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<16>, grid, 256, 0, st, g, cb, q, out, psi, modal_arg<16>(b), b.sc, wp)); break;
+        default: QGN_LAUNCH(KID_COMBO, nb, st, ::qgn::launch(k_combo<0>, grid, 256, 0, st, g, cb, q, out, psi, modal_arg<0>(b), b.sc, wp)); break;
     }
     return cudaGetLastError();
 }

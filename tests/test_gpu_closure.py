@@ -109,6 +109,30 @@ def test_fused_inference_equals_per_layer(cuda_ok, batch_seq):
         assert rel(outs[0], ref) <= 3e-3
 
 
+def test_fused_inference_wait_runs_out_and_recovers(cuda_ok):
+    """A tile whose counter is far ahead waits for neighbour counters that nothing advances:
+    the bounded wait runs out (about a second), the check reports it, and the next call,
+    with the counters cleared, gives the right answer again."""
+    import torch
+    from qgn_fortran_b200._lib import QGNError
+    net = cl.ClosureNet(nz=4, H=16, W=128, layers=3, max_batch=1, seed=4)
+    x, _ = sample(net, 1, 8)
+    xd = to_dev_bf16(x)
+    y = torch.zeros((1, net.H, net.W, net.cout_p), dtype=torch.float32, device="cuda")
+    net.forward(xd, y, 1)
+    net.check()
+    good = y.cpu().numpy()
+    net.debug_set_counter(0, 1 << 30)
+    net.forward(xd, y, 1)
+    with pytest.raises(QGNError) as ei:
+        net.check()
+    assert "timed out" in str(ei.value)
+    y.zero_()
+    net.forward(xd, y, 1)
+    net.check()
+    assert np.array_equal(y.cpu().numpy(), good)
+
+
 def test_cnn_gradients_match_oracle(cuda_ok):
     net, ws = small_net(seed=5)
     x, t = sample(net, 2, 2)
