@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const __grid_constant_
 // TV selects a tile width (0: the default; see the configs in rhs_tiles.cuh)
 // with more than one field, the narrow variants spread the fields over CTAs (blockIdx.z)
 template <int NY, int NF, class CT, int TV = 0>
-__global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, regcap<CT>()))
+__global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, YInvCfg<NY, CT, TV>::TP == 8 ? 64 : regcap<CT>()))
     k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
            CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
     QGN_PDL_ENTRY();
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(XCfg<NX, DRAG, CT, TV>::THREADS,
 
 template <int NY, bool DRAG, class CT, int TV = 0>
 __global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT, TV>::THREADS,
-                                  minb(YFwdCfg<NY, DRAG, CT, TV>::THREADS, regcap<CT>()))
+                                  minb(YFwdCfg<NY, DRAG, CT, TV>::THREADS, YFwdCfg<NY, DRAG, CT, TV>::TP == 8 ? 64 : regcap<CT>()))
     k_yfwd(Geom g, int layer0, const LayerConst* __restrict__ lc, const CT* __restrict__ q,
            const CT* __restrict__ psi, const CT* __restrict__ pp, const CT* __restrict__ pd,
            CT* __restrict__ out, const CT* __restrict__ twy, const CT* __restrict__ extra) {

@@ -46,14 +46,21 @@ __host__ __device__ constexpr int regcap(int fp64 = 128, int fp32 = 64) { return
 // different sizes (ensembles).
 // elements per thread of an x transform (fft.cuh): 32 for the FP32 512- and 1024-point
 // transforms of the single-field x pass (two radix passes instead of three, each transform in
-// one warp), 16 otherwise.  The y passes keep 16: their CTAs interleave columns across warps,
-// and at 32 elements they had half the threads per column and ran 1.3-1.7x slower on B200.
+// one warp), 16 otherwise.  The y passes keep 16 in FP32: their CTAs interleave columns across
+// warps, and at 32 elements they had half the threads per column and ran 1.3-1.7x slower on
+// B200.
 template <class CT, int N, int TV>
 __host__ __device__ constexpr int fft_tp() { return (TV == 0 && sizeof(CT) == 8 && (N == 512 || N == 1024)) ? 32 : 16; }
+// elements per thread of a y transform: 8 for the FP64 512- and 1024-point columns of the
+// single-field launches, 16 otherwise.  Half the registers per thread (64, two 512-thread CTAs
+// per SM) doubles the resident warps of these latency-bound kernels at the price of a fourth
+// radix pass at 1024 points: on B200 the 512^2 step ran 11 % and the 1024^2 step 1 % faster.
+template <class CT, int N, int TV>
+__host__ __device__ constexpr int fft_tp_y() { return (TV == 0 && sizeof(CT) == 16 && N >= 512) ? 8 : 16; }
 
 template <int NY, class CT = double2, int TV = 0>
 struct YInvCfg {
-    static constexpr int TP = 16;
+    static constexpr int TP = fft_tp_y<CT, NY, TV>();
     static constexpr int G = FFTShape<NY, TP>::G;
     static constexpr int TKX = TV == 0 ? cmin(cmax(4, 128 / G), 16) : cmax(1, TV / G);
     static constexpr int THREADS = TKX * G;
@@ -74,7 +81,7 @@ struct XCfg {
 
 template <int NY, bool DRAG, class CT = double2, int TV = 0>
 struct YFwdCfg {
-    static constexpr int TP = 16;
+    static constexpr int TP = fft_tp_y<CT, NY, TV>();
     static constexpr int G = FFTShape<NY, TP>::G;
     // tid ^ TKX stays in the warp
     static constexpr int TKX = TV == 0 ? cmin(cmax(2, 64 / G), 16) : cmin(cmax(1, TV / (2 * G)), 16);
