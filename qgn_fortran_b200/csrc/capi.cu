@@ -210,9 +210,13 @@ int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop
         }
     }
     // the update kernels also clear the max reduction of the error transform
-    if (mixed(ctx)) CK(launch_ark_update_mixed(g, b, st));
-    else CK(launch_ark_update(g, b, st));
-    CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
+    if (mixed(ctx)) {
+        CK(launch_ark_update_mixed(g, b, st));
+        CK(launch_maxabs_phys32(g, b, f32(b.err), b.sc, st));
+    } else {
+        CK(launch_ark_update(g, b, st));
+        CK(launch_maxabs_phys(g, b, b.err, b.sc, st));
+    }
     CK(launch_controller(g, b, leith ? 0 : 1, ctx->p.TOL, ctx->p.dt_max, max_rejects(ctx), loop, st));
     return QGN_OK;
 }

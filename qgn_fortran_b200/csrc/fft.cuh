@@ -6,9 +6,9 @@
 // takes the remaining factor.  Each pass reads T values from shared memory into
 // registers, applies the inter-pass twiddles, performs register-resident radix-R
 // DFTs and writes the results back in place (the load and store halves of a pass
-// are separated by a barrier).  Indices are padded by one element per 16
-// (p -> p + p/16) so that both the strided stores of the first pass and the
-// contiguous accesses of later passes are free of 16-byte bank-group conflicts.
+// are separated by a barrier).  Indices are padded by one element per TP
+// (p -> p + p/TP) so that both the strided stores of the first pass and the
+// contiguous accesses of later passes are free of bank-group conflicts.
 // TP = 32 halves the shared-memory round trips of a 512- or 1024-point transform (two
 // passes instead of three) at twice the registers; the FP32 transforms use it.
 //
@@ -44,10 +44,14 @@ template <class CT> __device__ __forceinline__ CT czero() { return cmk<CT>(0, 0)
 
 __host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
 
-// padded shared-memory index of element p of a transform
-__device__ __forceinline__ int fpad(int p) { return p + (p >> 4); }
+// padded shared-memory index of element p of a transform whose radix passes take TP elements
+// per thread: one pad element per TP, so that the first pass's stores (stride TP) and the later
+// passes' contiguous accesses hit distinct bank groups
+template <int TP = 16>
+__device__ __forceinline__ int fpad(int p) { return p + p / TP; }
 // padded length of one transform of length N
-__host__ __device__ constexpr int fpadlen(int N) { return N + (N >> 4); }
+template <int TP = 16>
+__host__ __device__ constexpr int fpadlen(int N) { return N + N / TP; }
 
 // Multiply by exp(DIR * 2*pi*i * m/16); m is a compile-time constant after unrolling.
 template <int DIR, class CT>
@@ -243,7 +247,7 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int idx = j + r * STRIDE;
-                if constexpr (SRC == SRC_SMEM) v[b * R + r] = x[fpad(idx)];
+                if constexpr (SRC == SRC_SMEM) v[b * R + r] = x[fpad<TP>(idx)];
                 else v[b * R + r] = ld(idx);
             }
         }
@@ -260,7 +264,7 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 const int idx = base + r * NS;
-                if constexpr (DST == DST_SMEM) x[fpad(idx)] = v[b * R + r];
+                if constexpr (DST == DST_SMEM) x[fpad<TP>(idx)] = v[b * R + r];
                 else st(idx, v[b * R + r]);
             }
         }

@@ -230,6 +230,7 @@ cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const
                          cudaStream_t s);
 // y-inverse + x-pass of one compact field with a max|.| reduction into sc->maxbits
 cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s);
+cudaError_t launch_maxabs_phys32(const Geom& g, const Buffers& b, const float2* f, DevScalars* sc, cudaStream_t s);
 // physical field (c2r/(nx*ny)) of a compact field into b.phys ([nz][ny][nx])
 cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, double* out, cudaStream_t s);
 // the fields of WriteQPmodal (QGN_Module.f90:381-440): q_mode, psi_mode and J_mode in physical

@@ -88,12 +88,12 @@ __global__ void __launch_bounds__(YFwdCfg<NY, DRAG, CT, TV>::THREADS,
     yfwd_tile<NY, DRAG, CT, TV>(g, blockIdx.x, layer0 + blockIdx.y, lc, q, psi, pp, pd, out, twy, extra);
 }
 
-template <int NX, int EPI, int TV = 0>
-__global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::THREADS))
-    k_xinv1(Geom g, const double2* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
-            const double2* __restrict__ twx) {
+template <int NX, int EPI, int TV = 0, class CT = double2>
+__global__ void __launch_bounds__(X1Cfg<NX, TV, CT>::THREADS, minb(X1Cfg<NX, TV, CT>::THREADS))
+    k_xinv1(Geom g, const CT* __restrict__ hq, DevScalars* __restrict__ sc, double* __restrict__ outp,
+            const CT* __restrict__ twx) {
     QGN_PDL_ENTRY();
-    xinv1_tile<NX, EPI, TV>(g, blockIdx.x, blockIdx.y, hq, sc, outp, twx);
+    xinv1_tile<NX, EPI, TV, CT>(g, blockIdx.x, blockIdx.y, hq, sc, outp, twx);
 }
 
 // Small grids launch few CTAs with the default tiles (at 128^2 x 4: 12 for the y-inverse),
@@ -142,8 +142,8 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
         const int r = e / nkx, k = e % nkx;
         const int rq = blockIdx.x * C::RP + r;
         if (rq >= npairs) continue;
-        const double2 X = sm[r * C::TS + fpad(k)];
-        const double2 Y = cconj(sm[r * C::TS + fpad((NX - k) & (NX - 1))]);
+        const double2 X = sm[r * C::TS + fpad<C::TP>(k)];
+        const double2 Y = cconj(sm[r * C::TS + fpad<C::TP>((NX - k) & (NX - 1))]);
         const size_t row = ((size_t)l * g.ny + 2 * rq) * g.nkxp + k;
         hq[row] = make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y));
         hq[row + g.nkxp] = make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
@@ -383,35 +383,46 @@ cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const
     return launch_yfwd<float2>(g, b.lc, q, psi, hpp, hpd, out, b.twy32, do_drag, s);
 }
 
-template <int NX, int EPI, int TV>
-static cudaError_t xinv1_go(const Geom& g, const Buffers& b, DevScalars* sc, double* outp, cudaStream_t s) {
-    using C = X1Cfg<NX, TV>;
+template <int NX, int EPI, int TV, class CT>
+static cudaError_t xinv1_go(const Geom& g, const CT* hq, const CT* twx, DevScalars* sc, double* outp, cudaStream_t s) {
+    using C = X1Cfg<NX, TV, CT>;
     cudaError_t e;
-    if ((e = set_smem(k_xinv1<NX, EPI, TV>, C::SMEM)) != cudaSuccess) return e;
+    if ((e = set_smem(k_xinv1<NX, EPI, TV, CT>, C::SMEM)) != cudaSuccess) return e;
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
-    const double hb = 16.0 * (double)g.nz * g.ny * g.nkx;
+    const double hb = (double)sizeof(CT) * (double)g.nz * g.ny * g.nkx;
     QGN_LAUNCH(KID_XINV1, hb + (EPI == 1 ? 8.0 * (double)g.nz * g.ny * NX : 0.0), s,
-               ::qgn::launch(k_xinv1<NX, EPI, TV>, grid, C::THREADS, C::SMEM, s, g, b.hq, sc, outp, b.twx));
+               ::qgn::launch(k_xinv1<NX, EPI, TV, CT>, grid, C::THREADS, C::SMEM, s, g, hq, sc, outp, twx));
     return cudaGetLastError();
 }
 
-template <int EPI>
-static cudaError_t launch_xinv1(const Geom& g, const Buffers& b, DevScalars* sc, double* outp, cudaStream_t s) {
+template <int EPI, class CT = double2>
+static cudaError_t launch_xinv1(const Geom& g, const CT* hq, const CT* twx, DevScalars* sc, double* outp,
+                                cudaStream_t s) {
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
         if constexpr (has_narrow<NX>()) {
-            const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * g.nz;
-            const long long cn = (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * g.nz;
-            if (narrow_better(cd, cn)) return xinv1_go<NX, EPI, kNarrowX1>(g, b, sc, outp, s);
+            using CD = X1Cfg<NX, 0, CT>;
+            using CN = X1Cfg<NX, kNarrowX1, CT>;
+            const long long cd = (long long)((g.ny / 2 + CD::RP - 1) / CD::RP) * g.nz;
+            const long long cn = (long long)((g.ny / 2 + CN::RP - 1) / CN::RP) * g.nz;
+            if (narrow_better(cd, cn)) return xinv1_go<NX, EPI, kNarrowX1, CT>(g, hq, twx, sc, outp, s);
         }
-        return xinv1_go<NX, EPI, 0>(g, b, sc, outp, s);
+        return xinv1_go<NX, EPI, 0, CT>(g, hq, twx, sc, outp, s);
     });
 }
 
 cudaError_t launch_maxabs_phys(const Geom& g, const Buffers& b, const double2* f, DevScalars* sc, cudaStream_t s) {
     cudaError_t e;
     if ((e = launch_yinv<double2>(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
-    return launch_xinv1<0>(g, b, sc, nullptr, s);
+    return launch_xinv1<0>(g, b.hq, b.twx, sc, nullptr, s);
+}
+
+// the same from an FP32 spectrum with FP32 transforms (the mixed mode's error norm)
+cudaError_t launch_maxabs_phys32(const Geom& g, const Buffers& b, const float2* f, DevScalars* sc, cudaStream_t s) {
+    cudaError_t e;
+    float2* hq = reinterpret_cast<float2*>(b.hq);
+    if ((e = launch_yinv<float2>(g, 1, f, nullptr, hq, nullptr, nullptr, b.twy32, s)) != cudaSuccess) return e;
+    return launch_xinv1<0, float2>(g, hq, b.twx32, sc, nullptr, s);
 }
 
 template <int NX, int SRC, int TV>
@@ -459,7 +470,7 @@ cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys
 cudaError_t launch_to_phys(const Geom& g, const Buffers& b, const double2* f, double* out, cudaStream_t s) {
     cudaError_t e;
     if ((e = launch_yinv<double2>(g, 1, f, nullptr, b.hq, nullptr, nullptr, b.twy, s)) != cudaSuccess) return e;
-    return launch_xinv1<1>(g, b, nullptr, out, s);
+    return launch_xinv1<1>(g, b.hq, b.twx, nullptr, out, s);
 }
 
 

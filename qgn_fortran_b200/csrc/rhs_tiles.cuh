@@ -21,8 +21,8 @@ __host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
 // slot stride (in elements) of a padded transform such that slot*stride spreads the bank
 // groups of one shared-memory wavefront: W = 128 bytes / element size elements per wavefront
 // (8 for double2, 16 for float2); target is the stride's residue mod W.
-__host__ __device__ constexpr int slot_stride(int N, int target, int elem_bytes = 16) {
-    return fpadlen(N) + ((target - (fpadlen(N) % (128 / elem_bytes))) + (128 / elem_bytes)) % (128 / elem_bytes);
+__host__ __device__ constexpr int slot_stride(int N, int target, int elem_bytes = 16, int tp = 16) {
+    return (N + N / tp) + ((target - ((N + N / tp) % (128 / elem_bytes))) + (128 / elem_bytes)) % (128 / elem_bytes);
 }
 // residue for `slots` lane-interleaved slots: consecutive threads hit different slots
 __host__ __device__ constexpr int interleave_target(int slots, int elem_bytes) {
@@ -64,7 +64,7 @@ struct YInvCfg {
     static constexpr int G = FFTShape<NY, TP>::G;
     static constexpr int TKX = TV == 0 ? cmin(cmax(4, 128 / G), 16) : cmax(1, TV / G);
     static constexpr int THREADS = TKX * G;
-    static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT));
+    static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT), TP);
     static constexpr int SMEM = TKX * TS * (int)sizeof(CT);
 };
 
@@ -75,7 +75,7 @@ struct XCfg {
     static constexpr int RP = cmax(1, (TV == 0 ? 64 : TV) / G);   // row pairs per CTA
     static constexpr int SP = DRAG ? 4 : 3;             // slots per row pair
     static constexpr int THREADS = SP * RP * G;
-    static constexpr int TS = slot_stride(NX, 2);
+    static constexpr int TS = slot_stride(NX, 2, (int)sizeof(CT), TP);
     static constexpr int SMEM = SP * RP * TS * (int)sizeof(CT);
 };
 
@@ -87,7 +87,7 @@ struct YFwdCfg {
     static constexpr int TKX = TV == 0 ? cmin(cmax(2, 64 / G), 16) : cmin(cmax(1, TV / (2 * G)), 16);
     static constexpr int SLOTS = 2 * TKX;
     static constexpr int THREADS = SLOTS * G;
-    static constexpr int TS = slot_stride(NY, interleave_target(SLOTS, (int)sizeof(CT)), (int)sizeof(CT));
+    static constexpr int TS = slot_stride(NY, interleave_target(SLOTS, (int)sizeof(CT)), (int)sizeof(CT), TP);
     static constexpr int SMEM = SLOTS * TS * (int)sizeof(CT);
 };
 
@@ -206,7 +206,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             const int p = e / C::TKX, c = e % C::TKX;
             const int k = kx0 + c;
             if (k >= g.nkxp) continue;
-            const CT f1 = sm[c * C::TS + fpad(2 * p)], f2 = sm[c * C::TS + fpad(2 * p + 1)];
+            const CT f1 = sm[c * C::TS + fpad<C::TP>(2 * p)], f2 = sm[c * C::TS + fpad<C::TP>(2 * p + 1)];
             const bool ok = k < g.nkx;
             CT* row = dl + (size_t)p * 2 * g.nkxp;
             // Re parts at kx = 0 and at the kx Nyquist column (kept only in the full-spectrum geometry)
@@ -256,7 +256,8 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
     //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
     const RT sc = (RT)g.inv_nxny;
     auto ld_fwd = [&](int x) -> CT {
-        const CT a = base[fpad(x)], bu = base[C::TS + fpad(x)], cv = base[2 * C::TS + fpad(x)];
+        const int px = fpad<C::TP>(x);
+        const CT a = base[px], bu = base[C::TS + px], cv = base[2 * C::TS + px];
         const bool second = (s_of & 1) != 0;
         const RT qv = (second ? a.y : a.x) * sc;
         const RT uv = (second ? bu.y : bu.x) * sc;
@@ -335,7 +336,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
             if (kx >= g.nkx) continue;
             const int j = g.jfull(m);
             const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
-            const CT fu = sm[cc * C::TS + fpad(j)], fv = sm[(C::TKX + cc) * C::TS + fpad(j)];
+            const CT fu = sm[cc * C::TS + fpad<C::TP>(j)], fv = sm[(C::TKX + cc) * C::TS + fpad<C::TP>(j)];
             CT d = cmk<CT>(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
             d = cmk<CT>(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
             out[(colbase + kx) * nky + m] = cmk<CT>(dc * d.x, dc * d.y);
@@ -359,7 +360,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
         const int j = g.jfull(m);
         const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
         const size_t idx = (colbase + kx) * nky + m;
-        const CT fuq = sm[cc * C::TS + fpad(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad(j)];
+        const CT fuq = sm[cc * C::TS + fpad<C::TP>(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad<C::TP>(j)];
         const CT qv = q[idx], pv = psi[idx];
         // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)
         const CT jac = cmk<CT>(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);
@@ -397,27 +398,29 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
 //   EPI 0: max |grid| (unnormalised) into sc->maxbits
 //   EPI 1: physical field grid/(nx*ny) into out[nz][ny][nx]
 // ------------------------------------------------------------------------------------
-template <int NX, int TV = 0>
+template <int NX, int TV = 0, class CT = double2>
 struct X1Cfg {
     static constexpr int TP = 16;
     static constexpr int G = FFTShape<NX, TP>::G;
     static constexpr int RP = cmax(1, (TV == 0 ? 128 : TV) / G);
     static constexpr int THREADS = RP * G;
-    static constexpr int TS = slot_stride(NX, 2);
-    static constexpr int SMEM = RP * TS * (int)sizeof(double2);
+    static constexpr int TS = slot_stride(NX, 2, (int)sizeof(CT));
+    static constexpr int SMEM = RP * TS * (int)sizeof(CT);
 };
 
-template <int NX, int EPI, int TV = 0>
+// CT = float2 (the mixed mode's error norm) supports EPI 0 only
+template <int NX, int EPI, int TV = 0, class CT = double2>
 // EPI 2 (the learned closure's input): channel chan of the NHWC BF16 tensor xout with
 // cin_p channels per pixel, grid/(nx*ny) * scale[chan]
-__device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const double2* __restrict__ hq,
+__device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const CT* __restrict__ hq,
                                            DevScalars* __restrict__ sc, double* __restrict__ outp,
-                                           const double2* __restrict__ twx, const float* __restrict__ scale = nullptr,
+                                           const CT* __restrict__ twx, const float* __restrict__ scale = nullptr,
                                            __nv_bfloat16* __restrict__ xout = nullptr, int cin_p = 0,
                                            int chan = 0) {
-    using C = X1Cfg<NX, TV>;
+    static_assert(EPI == 0 || sizeof(CT) == 16, "FP32 rows: max only");
+    using C = X1Cfg<NX, TV, CT>;
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = reinterpret_cast<double2*>(sm_raw);
+    CT* sm = reinterpret_cast<CT*>(sm_raw);
     __shared__ double smax[32];
     const int tid = threadIdx.x;
     const int npairs = g.ny / 2;
@@ -425,21 +428,21 @@ __device__ __forceinline__ void xinv1_tile(const Geom g, int bx, int l, const do
     const int slot = tid / C::G, lane = tid % C::G;
     const int rp = bx * C::RP + slot;
     const bool ok = rp < npairs;
-    const double2* F = hq + ((size_t)l * npairs + rp) * 2 * g.nkxp;   // packed row pair
-    auto ld = [&](int k) -> double2 {
+    const CT* F = hq + ((size_t)l * npairs + rp) * 2 * g.nkxp;   // packed row pair
+    auto ld = [&](int k) -> CT {
         if (k < nkx) return F[k];
         if (k > NX - nkx) return F[g.nkxp + (NX - k)];
-        return make_double2(0.0, 0.0);
+        return cmk<CT>(0.0, 0.0);
     };
     double mx = 0.0;
     const size_t prow = ((size_t)l * g.ny + 2 * rp) * NX;
-    auto st = [&](int x, double2 a) {
-        if (EPI == 0) {
+    auto st = [&](int x, CT a) {
+        if constexpr (EPI == 0) {
             // NaN is kept as the largest value
-            const double m1 = fabs(a.x), m2 = fabs(a.y);
+            const double m1 = fabs((double)a.x), m2 = fabs((double)a.y);
             if (!(m1 == m1) || !(m2 == m2)) mx = __longlong_as_double(0x7ff8000000000000LL);
             else if (mx == mx) mx = fmax(mx, fmax(m1, m2));
-        } else if (EPI == 1) {
+        } else if constexpr (EPI == 1) {
             outp[prow + x] = a.x * g.inv_nxny;
             outp[prow + NX + x] = a.y * g.inv_nxny;
         } else {

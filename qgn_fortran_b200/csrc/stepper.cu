@@ -270,7 +270,7 @@ struct StagePtrs32 {
 
 // update + embedded error in FP64 from FP32 stage values (ARK43_QGLeith.f90:120-134)
 __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp, const double2* __restrict__ q,
-                                                          double2* __restrict__ qnew, double2* __restrict__ err,
+                                                          double2* __restrict__ qnew, float2* __restrict__ err,
                                                           const LayerConst* __restrict__ lc,
                                                           DevScalars* __restrict__ sc) {
     QGN_PDL_ENTRY();
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(256) k_ark_update_mixed(Geom g, StagePtrs32 sp
         uc.x += c_b[i] * nlx;
         uc.y += c_b[i] * nly;
     }
-    err[e] = ec;
+    err[e] = make_float2((float)ec.x, (float)ec.y);   // its norm is taken with FP32 transforms
     qnew[e] = (p == 0) ? make_double2(0.0, 0.0) : make_double2(q0.x + dt * uc.x, q0.y + dt * uc.y);
 }
 
@@ -730,8 +730,9 @@ cudaError_t launch_ark_stage_mixed(const Geom& g, const Buffers& b, int s, cudaS
 cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_t st) {
     const StagePtrs32 sp = stage_ptrs32(b);
     const double C = (double)g.csize();
-    QGN_LAUNCH(KID_UPDATE, 16.0 * C * 3.0 + 8.0 * C * 9.0, st,
-               ::qgn::launch(k_ark_update_mixed, blocks_for(g.csize(), 256), 256, 0, st, g, sp, b.q, b.qnew, b.err, b.lc, b.sc));
+    QGN_LAUNCH(KID_UPDATE, 16.0 * C * 2.0 + 8.0 * C * 10.0, st,
+               ::qgn::launch(k_ark_update_mixed, blocks_for(g.csize(), 256), 256, 0, st, g, sp, b.q, b.qnew,
+                             reinterpret_cast<float2*>(b.err), b.lc, b.sc));
     return cudaGetLastError();
 }
 
