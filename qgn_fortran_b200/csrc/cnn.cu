@@ -500,11 +500,13 @@ __device__ __forceinline__ void issue_tile(uint32_t dacc, const uint32_t* ra, ui
                  : "memory");
 }
 
-// a layer's weights [9][COUT][CIN] (BF16) into the K-major operand layout [9][CIN/8][COUT][8]
+// a layer's weights [9][COUT][CIN] (BF16) into the K-major operand layout [9][CIN/8][COUT][8];
+// cin and cout are powers of two (16 or 64), so the index split is shifts and masks
 __device__ __forceinline__ void fetch_weights(const __nv_bfloat16* __restrict__ wt, int cin, int cout, uint32_t w) {
-    const int c8n = cin / 8;
+    const int c8n = cin >> 3;
+    const int lc8 = __ffs(c8n) - 1, lco = __ffs(cout) - 1;
     for (int i = threadIdx.x; i < 9 * cout * c8n; i += kThreads) {
-        const int c8 = i % c8n, n = (i / c8n) % cout, tap = i / (c8n * cout);
+        const int c8 = i & (c8n - 1), n = (i >> lc8) & (cout - 1), tap = i >> (lc8 + lco);
         cp16(w + (uint32_t)(((tap * c8n + c8) * cout + n) * 16), wt + ((size_t)tap * cout + n) * cin + c8 * 8);
     }
 }
@@ -513,11 +515,12 @@ __device__ __forceinline__ void fetch_weights(const __nv_bfloat16* __restrict__ 
 template <int CIN>
 __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, int b, int hh, int H, int W, int w0,
                                          uint32_t slot_addr) {
+    const size_t row = ((size_t)b * H + hh) * W;
     for (int i = threadIdx.x; i < kPixS * (CIN / 8); i += kThreads) {
         const int c8 = i % (CIN / 8), px = i / (CIN / 8);
-        int ww = w0 - 1 + px;
-        ww = (ww % W + W) % W;
-        cp16(slot_addr + (uint32_t)((c8 * kPixS + px) * 16), x + (((size_t)b * H + hh) * W + ww) * CIN + c8 * 8);
+        int ww = w0 - 1 + px;   // in [-1, W]: one periodic wrap at either end
+        ww = ww < 0 ? ww + W : (ww >= W ? ww - W : ww);
+        cp16(slot_addr + (uint32_t)((c8 * kPixS + px) * 16), x + (row + ww) * CIN + c8 * 8);
     }
 }
 

@@ -212,7 +212,9 @@ __device__ __forceinline__ void apply_twiddles(CT* v, int k, const CT* __restric
 
 // Where a pass takes its input from / puts its output to.
 enum FftSrc { SRC_SMEM = 0, SRC_FN = 1, SRC_FN_SMEM = 2 };   // SRC_FN_SMEM: a functor that reads this smem
-enum FftDst { DST_SMEM = 0, DST_FN = 1 };
+// DST_SMEM_MAP: the last pass writes x[st(idx)] (st maps an output index to a shared-memory
+// offset) with the barriers of DST_SMEM
+enum FftDst { DST_SMEM = 0, DST_FN = 1, DST_SMEM_MAP = 2 };
 
 // One Stockham DIT pass (sub-length NS, radix R) of an N-point transform whose
 // intermediate lives padded at x.  Pass 0 may read through ld(idx), the last pass may
@@ -252,7 +254,8 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
             }
         }
     }
-    if constexpr (DST == DST_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
+    constexpr bool TO_SMEM = (DST == DST_SMEM || DST == DST_SMEM_MAP);
+    if constexpr (TO_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
     if (active) {
 #pragma unroll
         for (int b = 0; b < BPT; ++b) {
@@ -265,11 +268,12 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
             for (int r = 0; r < R; ++r) {
                 const int idx = base + r * NS;
                 if constexpr (DST == DST_SMEM) x[fpad<TP>(idx)] = v[b * R + r];
+                else if constexpr (DST == DST_SMEM_MAP) x[st(idx)] = v[b * R + r];
                 else st(idx, v[b * R + r]);
             }
         }
     }
-    if constexpr (DST == DST_SMEM) fft_sync<LAST, WS>();
+    if constexpr (TO_SMEM) fft_sync<LAST, WS>();
 }
 
 template <int N, int NS, int DIR, int SRC0, int DSTL, int TP, bool WS, class CT, class Ld, class St>

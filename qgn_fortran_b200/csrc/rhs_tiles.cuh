@@ -66,6 +66,12 @@ struct YInvCfg {
     static constexpr int THREADS = TKX * G;
     static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT), TP);
     static constexpr int SMEM = TKX * TS * (int)sizeof(CT);
+    // de-interleaved output rows (yinv_tile): odd rows start at HY.  A wavefront holds W
+    // elements, LP = W/TKX consecutive rows of each slot; HY = NY/2 + LP/2 puts their even and
+    // odd halves on distinct bank groups.
+    static constexpr int LP = cmax(1, (128 / (int)sizeof(CT)) / TKX);
+    static constexpr int HY = NY / 2 + LP / 2;
+    static_assert(2 * HY <= TS, "de-interleaved rows fit the slot");
 };
 
 template <int NX, bool DRAG, class CT = double2, int TV = 0>
@@ -199,14 +205,18 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             }
             return v;
         };
-        fft_fused<NY, +1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ld, none);
+        // the last pass writes rows y de-interleaved: even y at y/2, odd y at HY + y/2, so the
+        // packing loop below reads consecutive offsets (free of bank-group conflicts; HY
+        // offsets the odd half so that the last pass's stores are conflict-free too)
+        auto omap = [](int y) { return (y & 1) * C::HY + (y >> 1); };
+        fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
         // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
         CT* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
         for (int e = tid; e < (NY / 2) * C::TKX; e += C::THREADS) {
             const int p = e / C::TKX, c = e % C::TKX;
             const int k = kx0 + c;
             if (k >= g.nkxp) continue;
-            const CT f1 = sm[c * C::TS + fpad<C::TP>(2 * p)], f2 = sm[c * C::TS + fpad<C::TP>(2 * p + 1)];
+            const CT f1 = sm[c * C::TS + p], f2 = sm[c * C::TS + C::HY + p];
             const bool ok = k < g.nkx;
             CT* row = dl + (size_t)p * 2 * g.nkxp;
             // Re parts at kx = 0 and at the kx Nyquist column (kept only in the full-spectrum geometry)
