@@ -200,10 +200,24 @@ int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
-    for (int s = 1; s < 6; ++s) {
+    const bool columns = !mixed(ctx) && stage_yinv_ok(g, b);
+    if (columns && !drag_on(ctx)) {
+        // small grids: stage s with the y-inverse of its RHS, and the y-forward of RHS s-1
+        // with both, in one launch per column (two launches per stage instead of four)
+        const double2* extra = closure_tendency(ctx);
+        CK(launch_ark_stage_yinv(g, b, 1, st));
+        for (int s = 1; s < 6; ++s) {
+            CK(launch_rhs_x(g, b, false, st));
+            if (s < 5) CK(launch_yfwd_stage_yinv(g, b, s + 1, extra, st));
+            else CK(launch_rhs_yfwd(g, b, b.Qs[5], b.psi, b.N[5], false, st, extra));
+        }
+    } else for (int s = 1; s < 6; ++s) {
         if (mixed(ctx)) {
             CK(launch_ark_stage_mixed(g, b, s, st));
             CK(launch_rhs32(g, b, f32(b.Qs[s]), f32(b.psi), f32(b.N[s]), drag_on(ctx), st));
+        } else if (columns) {   // small grids with quadratic drag: the stage with the y-inverse
+            CK(launch_ark_stage_yinv(g, b, s, st));
+            CK(launch_rhs_tail(g, b, b.Qs[s], b.psi, b.N[s], true, st, closure_tendency(ctx)));
         } else {
             CK(launch_ark_stage(g, b, s, st));
             RET(rhs_of(ctx, b.Qs[s], b.psi, b.N[s]));
@@ -231,6 +245,16 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
         // FP32 copy of q_hat for the FP32 RHS lives in the error buffer until the update
         CK(launch_modal_mixed(g, b, b.q, f32(b.err), f32(b.psi), st));
         CK(launch_rhs32(g, b, f32(b.err), f32(b.psi), f32(b.N[0]), drag_on(ctx), st));
+    } else if (stage_yinv_ok(g, b)) {
+        // small grids: GetPsi and the y-inverse of the first RHS in one launch per column.  An
+        // attached closure needs psi first, and its input transform reuses the packed-row
+        // buffers, so it runs after a separate GetPsi (which the column kernel repeats).
+        if (ctx->closure) {
+            CK(launch_modal(g, b, b.q, b.psi, st));
+            RET(closure_eval(ctx));
+        }
+        CK(launch_ark_stage_yinv(g, b, 0, st));
+        CK(launch_rhs_tail(g, b, b.q, b.psi, b.N[0], drag_on(ctx), st, closure_tendency(ctx)));
     } else {
         CK(launch_modal(g, b, b.q, b.psi, st));
         // the learned closure (if attached): S of this step's state and the budget check that

@@ -226,6 +226,12 @@ cudaError_t launch_modal(const Geom& g, const Buffers& b, const double2* q, doub
 // extra (optional, compact): a tendency added to the RHS on the kept modes (learned closure)
 cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
                        bool do_drag, cudaStream_t s, const double2* extra = nullptr);
+// the x and y-forward passes of launch_rhs, when the y-inverse already ran, and each alone
+cudaError_t launch_rhs_tail(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
+                            bool do_drag, cudaStream_t s, const double2* extra = nullptr);
+cudaError_t launch_rhs_x(const Geom& g, const Buffers& b, bool do_drag, cudaStream_t s);
+cudaError_t launch_rhs_yfwd(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
+                            bool do_drag, cudaStream_t s, const double2* extra = nullptr);
 cudaError_t launch_rhs32(const Geom& g, const Buffers& b, const float2* q, const float2* psi, float2* out, bool do_drag,
                          cudaStream_t s);
 // y-inverse + x-pass of one compact field with a max|.| reduction into sc->maxbits
@@ -257,6 +263,9 @@ struct Combo {
 };
 cudaError_t launch_leith(const Geom& g, const Buffers& b, const double2* q, double c12, cudaStream_t s);
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
+bool stage_yinv_ok(const Geom& g, const Buffers& b);
+cudaError_t launch_ark_stage_yinv(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
+cudaError_t launch_yfwd_stage_yinv(const Geom& g, const Buffers& b, int stage, const double2* extra, cudaStream_t s);
 cudaError_t launch_ark_update(const Geom& g, const Buffers& b, cudaStream_t s);
 cudaError_t launch_ark_stage_mixed(const Geom& g, const Buffers& b, int stage, cudaStream_t s);
 cudaError_t launch_ark_update_mixed(const Geom& g, const Buffers& b, cudaStream_t s);

@@ -364,7 +364,22 @@ cudaError_t launch_rhs(const Geom& g, const Buffers& b, const double2* q, const 
                        bool do_drag, cudaStream_t s, const double2* extra) {
     cudaError_t e;
     if ((e = launch_yinv<double2>(g, 3, q, psi, b.hq, b.hp, b.hu, b.twy, s)) != cudaSuccess) return e;
-    if ((e = launch_xpass<double2>(g, b.hq, b.hp, b.hu, b.hpp, b.hpd, b.twx, do_drag, s)) != cudaSuccess) return e;
+    return launch_rhs_tail(g, b, q, psi, out, do_drag, s, extra);
+}
+
+cudaError_t launch_rhs_tail(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
+                            bool do_drag, cudaStream_t s, const double2* extra) {
+    cudaError_t e;
+    if ((e = launch_rhs_x(g, b, do_drag, s)) != cudaSuccess) return e;
+    return launch_rhs_yfwd(g, b, q, psi, out, do_drag, s, extra);
+}
+
+cudaError_t launch_rhs_x(const Geom& g, const Buffers& b, bool do_drag, cudaStream_t s) {
+    return launch_xpass<double2>(g, b.hq, b.hp, b.hu, b.hpp, b.hpd, b.twx, do_drag, s);
+}
+
+cudaError_t launch_rhs_yfwd(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* out,
+                            bool do_drag, cudaStream_t s, const double2* extra) {
     return launch_yfwd<double2>(g, b.lc, q, psi, b.hpp, b.hpd, out, b.twy, do_drag, s, extra);
 }
 

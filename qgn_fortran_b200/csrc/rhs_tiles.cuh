@@ -331,14 +331,17 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     const size_t colbase = (size_t)l * g.nkx;
     const bool bottom = (l == g.nz - 1);
     CT* xs = sm + slot * C::TS;
-    NoIOT<CT> none;
+    // the last radix pass writes the transformed column unpadded (row y at y): the assembly
+    // loops below read 8-16 consecutive rows per wavefront, which a pad element every TP rows
+    // would split across one bank group twice
+    auto omap = [](int y) { return y; };
 
     if (DRAG) {
         // drag_hat = i ky (|u|u)^ - i kx (|u|v)^ on the bottom layer (QGN_Module.f90:284-292)
         auto ldd = [&](int y) -> CT {
             return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, colok, C::TKX);
         };
-        fft_fused<NY, -1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ldd, none);
+        fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ldd, omap);
         const RT dc = (RT)lc->dragc;
         for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
             const int cc = e / nky, m = e % nky;
@@ -346,7 +349,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
             if (kx >= g.nkx) continue;
             const int j = g.jfull(m);
             const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
-            const CT fu = sm[cc * C::TS + fpad<C::TP>(j)], fv = sm[(C::TKX + cc) * C::TS + fpad<C::TP>(j)];
+            const CT fu = sm[cc * C::TS + j], fv = sm[(C::TKX + cc) * C::TS + j];
             CT d = cmk<CT>(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
             d = cmk<CT>(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
             out[(colbase + kx) * nky + m] = cmk<CT>(dc * d.x, dc * d.y);
@@ -358,7 +361,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
     auto ld = [&](int y) -> CT { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
                                                          fld, colok, C::TKX); };
-    fft_fused<NY, -1, SRC_FN, DST_SMEM, C::TP>(xs, lane, true, twy, ld, none);
+    fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
 
     const RT ub = (RT)lc->uBar[l], bq = (RT)lc->betaq[l];
     const RT ek = (RT)lc->ekman;
@@ -370,7 +373,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
         const int j = g.jfull(m);
         const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
         const size_t idx = (colbase + kx) * nky + m;
-        const CT fuq = sm[cc * C::TS + fpad<C::TP>(j)], fvq = sm[(C::TKX + cc) * C::TS + fpad<C::TP>(j)];
+        const CT fuq = sm[cc * C::TS + j], fvq = sm[(C::TKX + cc) * C::TS + j];
         const CT qv = q[idx], pv = psi[idx];
         // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)
         const CT jac = cmk<CT>(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);

@@ -10,6 +10,11 @@
 #include "qgn_internal.cuh"
 #include "prof.cuh"
 #include "ctrl.cuh"
+#include "rhs_tiles.cuh"
+
+#include <cstdlib>
+#include <mutex>
+#include <unordered_set>
 
 namespace qgn {
 
@@ -680,6 +685,311 @@ static cudaError_t launch_stage_small_nz(const Geom& g, const Buffers& b, int s,
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+// ---- small grids: the stage, GetPsi and the y passes of one kx column in one CTA -------------
+// On a grid of at most kSmallStage kept mode-layers every kernel of a step is a few
+// microseconds of latency, so launches are what a step costs.  A stage's combination and
+// GetPsi work per mode (all layers of one (kx, ky)), and the y transforms per kx column, so one
+// CTA per column can do both without waiting for other CTAs.
+template <int NY, int NZ>
+struct StageYinvCfg {
+    static constexpr int G = FFTShape<NY, 16>::G;
+    static constexpr int SLOTS = 3 * NZ;   // (q, u, v) x layers
+    static constexpr int THREADS = SLOTS * G;
+    static constexpr int TS = slot_stride(NY, 2, 16, 16);
+    // rows are written de-interleaved (even y at y/2, odd y at HY + y/2): the 8 lanes of a
+    // quarter-warp hold 4 even and 4 odd rows, so HY = 4 mod 8 keeps their stores on distinct
+    // bank groups, and the packing reads are consecutive
+    static constexpr int HY = NY / 2 + 4;
+    static_assert(2 * HY <= TS, "de-interleaved rows fit the slot");
+    static_assert(G >= 8 && G <= 32, "one slot per 8..32 lanes");
+    static constexpr int SLOT_BYTES = SLOTS * TS * 16;
+};
+
+// Stage S (S = 0: the state itself) of column kx: q_S at every kept mode of the column for all
+// layers (the arithmetic of k_ark_stage_small), GetPsi of it, both kept in shared memory;
+// then the 3*NZ inverse y transforms of q, u = -i ky psi, v = i kx psi of the column, one per
+// slot of G threads, packed into row pairs for the x pass (the arithmetic of yinv_tile).
+template <int S, int NZ, int NY>
+__device__ __forceinline__ void stage_yinv_col(const Geom& g, int kx, const CombPtrs<double2>& cp,
+                                               const double2* __restrict__ q, double2* __restrict__ qout,
+                                               double2* __restrict__ psi, const LayerConst* __restrict__ lc,
+                                               const ModalView& mv, const DevScalars* __restrict__ sc,
+                                               double2* __restrict__ pq, double2* __restrict__ pv,
+                                               double2* __restrict__ pu, const double2* __restrict__ twy,
+                                               unsigned char* sm_raw) {
+    using C = StageYinvCfg<NY, NZ>;
+    double2* slots = reinterpret_cast<double2*>(sm_raw);
+    const int nky = g.nky;
+    double2* qcol = reinterpret_cast<double2*>(sm_raw + C::SLOT_BYTES);   // [NZ][nky]
+    double2* pcol = qcol + NZ * nky;
+    const int tid = threadIdx.x;
+    const size_t P = (size_t)g.nkx * nky;
+    const double kxv = g.dkx * kx;
+    const double dt = sc->dt;
+    for (int m = tid; m < nky; m += C::THREADS) {
+        const size_t p = (size_t)kx * nky + m;
+        const double kyv = g.kyval(g.jfull(m));
+        const double k2 = kxv * kxv + kyv * kyv;
+        const double k8 = (k2 * k2) * (k2 * k2);
+        double2 qv[NZ], pvv[NZ];
+#pragma unroll
+        for (int l = 0; l < NZ; ++l) {
+            const size_t e = (size_t)l * P + p;
+            if constexpr (S == 0) {
+                qv[l] = q[e];
+            } else {
+                const double D = lc->A2 * k2 + sc->A8L[l] * k8;
+                double2 nn[S], qq[S];
+#pragma unroll
+                for (int j = 0; j < S; ++j) nn[j] = cp.N[j][e];
+#pragma unroll
+                for (int j = 1; j < S; ++j) qq[j] = cp.Q[j][e];
+                const double2 q0 = q[e];
+                double ax, ay;
+                comb_sum64<S>(nn, qq, q0, D, ax, ay);
+                const double Mq = 1.0 / (1.0 + 0.25 * dt * D);
+                qv[l] = make_double2(Mq * (q0.x + dt * ax), Mq * (q0.y + dt * ay));
+                qout[e] = qv[l];
+            }
+            qcol[l * nky + m] = qv[l];
+        }
+        modal_invert_s<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, NZ, k2, p == 0, qv, pvv);
+#pragma unroll
+        for (int l = 0; l < NZ; ++l) {
+            psi[(size_t)l * P + p] = pvv[l];
+            pcol[l * nky + m] = pvv[l];
+        }
+    }
+    __syncthreads();
+    const int slot = tid / C::G, lane = tid % C::G;
+    const int f = slot / NZ, l = slot % NZ;
+    double2* xs = slots + slot * C::TS;
+    const double2* col = (f == 0 ? qcol : pcol) + l * nky;
+    auto ld = [&](int j) -> double2 {
+        const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
+        if (!kept) return make_double2(0.0, 0.0);
+        double2 v = col[j < g.kylo ? j : j - g.kyshift];
+        if (f == 1) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
+            const double kyv = g.kyval(j);
+            v = make_double2(kyv * v.y, -kyv * v.x);
+        } else if (f == 2) {   // v_hat = i kx psi_hat  (QGN_Module.f90:224)
+            v = make_double2(-kxv * v.y, kxv * v.x);
+        }
+        return v;
+    };
+    auto omap = [](int y) { return (y & 1) * C::HY + (y >> 1); };
+    fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, 16, true>(xs, lane, true, twy, ld, omap);
+    double2* dst = (f == 0 ? pq : (f == 1 ? pu : pv)) + (size_t)l * (NY / 2) * 2 * g.nkxp;
+    for (int pr = lane; pr < NY / 2; pr += C::G) {
+        const double2 f1 = xs[pr], f2 = xs[C::HY + pr];
+        double2* row = dst + (size_t)pr * 2 * g.nkxp;
+        row[kx] = pack_lo(f1, f2, kx == 0 || 2 * kx == g.nx);
+        row[g.nkxp + kx] = kx > 0 ? pack_hi(f1, f2) : make_double2(0.0, 0.0);
+    }
+}
+
+template <int S, int NZ, int NY>
+__global__ void __launch_bounds__(StageYinvCfg<NY, NZ>::THREADS)
+    k_stage_yinv(Geom g, CombPtrs<double2> cp, const double2* __restrict__ q, double2* __restrict__ qout,
+                 double2* __restrict__ psi, const LayerConst* __restrict__ lc, const __grid_constant__ ModalArg<NZ> ma,
+                 const DevScalars* __restrict__ sc, double2* __restrict__ pq, double2* __restrict__ pv,
+                 double2* __restrict__ pu, const double2* __restrict__ twy) {
+    QGN_PDL_ENTRY();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const ModalView mv = modal_view<NZ>(ma, nullptr, nullptr, nullptr, NZ);
+    stage_yinv_col<S, NZ, NY>(g, blockIdx.x, cp, q, qout, psi, lc, mv, sc, pq, pv, pu, twy, sm_raw);
+}
+
+// Stages 2..5 without quadratic drag: the y-forward pass that finishes N_{S-1} for column kx
+// (all layers; the assembly of yfwd_tile), then stage S and its y-inverse for the same column.
+// N_{S-1} of the column is complete before stage S reads it, so no other CTA's output is
+// needed: the y-forward, stage and y-inverse launches become one.
+template <int S, int NZ, int NY>
+__global__ void __launch_bounds__(StageYinvCfg<NY, NZ>::THREADS)
+    k_yfwd_stage_yinv(Geom g, const double2* __restrict__ pp, const double2* __restrict__ qprev,
+                      double2* __restrict__ nout, const double2* __restrict__ extra, CombPtrs<double2> cp,
+                      const double2* __restrict__ q, double2* __restrict__ qout, double2* __restrict__ psi,
+                      const LayerConst* __restrict__ lc, const __grid_constant__ ModalArg<NZ> ma,
+                      const DevScalars* __restrict__ sc, double2* __restrict__ pq, double2* __restrict__ pv,
+                      double2* __restrict__ pu, const double2* __restrict__ twy) {
+    QGN_PDL_ENTRY();
+    using C = StageYinvCfg<NY, NZ>;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    double2* slots = reinterpret_cast<double2*>(sm_raw);
+    const ModalView mv = modal_view<NZ>(ma, nullptr, nullptr, nullptr, NZ);
+    const int tid = threadIdx.x;
+    const int kx = blockIdx.x;
+    const int nky = g.nky;
+    {   // forward y transforms of (uq)^ (slots 0..NZ-1) and (vq)^ (slots NZ..2NZ-1), unpadded
+        const int slot = tid / C::G, lane = tid % C::G;
+        const int f = slot / NZ, l = slot % NZ;
+        const bool act = slot < 2 * NZ;
+        double2* xs = slots + slot * C::TS;
+        const double2* rows = pp + (size_t)(act ? l : 0) * NY * 2 * g.nkxp;
+        auto ld = [&](int y) -> double2 {
+            const double2* row = rows + (size_t)y * 2 * g.nkxp;
+            const double2 X = row[kx];
+            const double2 Y = kx == 0 ? cconj(X) : cconj(row[g.nkxp + kx]);
+            return f == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
+                          : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
+        };
+        auto omap = [](int y) { return y; };
+        fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, 16, true>(xs, lane, act, twy, ld, omap);
+    }
+    const double kxv = g.dkx * kx;
+    const bool expl = lc->explicit_diss != 0;
+    for (int m = tid; m < nky; m += C::THREADS) {
+        const int j = g.jfull(m);
+        const double kyv = g.kyval(j);
+#pragma unroll
+        for (int l = 0; l < NZ; ++l) {
+            const size_t idx = ((size_t)l * g.nkx + kx) * nky + m;
+            const double2 fuq = slots[l * C::TS + j], fvq = slots[(NZ + l) * C::TS + j];
+            const double2 qv = qprev[idx], pvv = psi[idx];
+            // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)
+            const double2 jac = make_double2(-kxv * fuq.y - kyv * fvq.y, kxv * fuq.x + kyv * fvq.x);
+            double2 r = make_double2(-jac.x, -jac.y);
+            // - uBar i kx q_hat - (beta+qyBar) v_hat   (QGN_Module.f90:270-273)
+            const double uk = lc->uBar[l] * kxv;
+            const double2 vh = make_double2(-kxv * pvv.y, kxv * pvv.x);
+            const double bq = lc->betaq[l];
+            r = make_double2(r.x + uk * qv.y, r.y - uk * qv.x);
+            r = make_double2(r.x - bq * vh.x, r.y - bq * vh.y);
+            const double k2 = kxv * kxv + kyv * kyv;
+            if (expl) {   // QGN_Module.f90:275-280
+                const double k4 = k2 * k2, k8 = k4 * k4;
+                const double dcoef = lc->A2 * k2 + lc->A8 * k8;
+                r = make_double2(r.x - dcoef * qv.x, r.y - dcoef * qv.y);
+            }
+            if (l == NZ - 1) {   // Ekman, QGN_Module.f90:282
+                const double ekk = lc->ekman * k2;
+                r = make_double2(r.x + ekk * pvv.x, r.y + ekk * pvv.y);
+            }
+            if (extra) {
+                const double2 x = extra[idx];
+                r = make_double2(r.x + x.x, r.y + x.y);
+            }
+            if (kx == 0 && m == 0) r = make_double2(0.0, 0.0);
+            nout[idx] = r;
+        }
+    }
+    __syncthreads();   // N_{S-1} of the column is written; the slots are free
+    stage_yinv_col<S, NZ, NY>(g, kx, cp, q, qout, psi, lc, mv, sc, pq, pv, pu, twy, sm_raw);
+}
+
+// the (ny, nz) pairs built: a CTA keeps its registers without spilling
+constexpr bool stage_yinv_built(int ny, int nz) {
+    return (ny == 128 && nz <= 16) || (ny == 256 && nz <= 8) || (ny == 512 && nz <= 4);
+}
+
+// the dynamic shared-memory limit of each column kernel, raised once per kernel
+static cudaError_t column_smem(const void* kern, int bytes) {
+    static std::mutex mu;
+    static std::unordered_set<const void*> done;
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count(kern)) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess) done.insert(kern);
+    return e;
+}
+
+template <int NZ, int NY, class Kern, class... Args>
+static cudaError_t stage_yinv_launch(const Geom& g, Kern kern, int kid, double nb, cudaStream_t st, Args... args) {
+    using C = StageYinvCfg<NY, NZ>;
+    const int smem = C::SLOT_BYTES + 2 * NZ * g.nky * 16;
+    cudaError_t e = column_smem(reinterpret_cast<const void*>(kern), smem);
+    if (e != cudaSuccess) return e;
+    QGN_LAUNCH(kid, nb, st, ::qgn::launch(kern, g.nkx, C::THREADS, smem, st, args...));
+    return cudaGetLastError();
+}
+
+template <int S, int NZ, int NY>
+static cudaError_t stage_yinv_s(const Geom& g, const Buffers& b, cudaStream_t st) {
+    const double Cb = 16.0 * (double)g.csize(), Hb = 16.0 * (double)g.nz * NY * g.nkx;
+    const double nb = Cb * (S == 0 ? 2.0 : 2.0 * S + 2.0) + 3.0 * Hb;
+    return stage_yinv_launch<NZ, NY>(g, k_stage_yinv<S, NZ, NY>, KID_STAGE, nb, st, g, comb_ptrs<double2>(b), b.q,
+                                     b.Qs[S], b.psi, b.lc, modal_arg<NZ>(b), b.sc, b.hq, b.hp, b.hu, b.twy);
+}
+
+template <int S, int NZ, int NY>
+static cudaError_t yfwd_stage_yinv_s(const Geom& g, const Buffers& b, const double2* extra, cudaStream_t st) {
+    const double Cb = 16.0 * (double)g.csize(), Hb = 16.0 * (double)g.nz * NY * g.nkx;
+    const double nb = 2.0 * Hb + 3.0 * Cb + Cb * (2.0 * S + 2.0) + 3.0 * Hb;
+    return stage_yinv_launch<NZ, NY>(g, k_yfwd_stage_yinv<S, NZ, NY>, KID_YFWD, nb, st, g, b.hpp, b.Qs[S - 1],
+                                     b.N[S - 1], extra, comb_ptrs<double2>(b), b.q, b.Qs[S], b.psi, b.lc,
+                                     modal_arg<NZ>(b), b.sc, b.hq, b.hp, b.hu, b.twy);
+}
+
+// fused = false: stage s and its y-inverse; true: the y-forward of RHS s-1 as well (s = 2..5)
+template <int NZ, int NY>
+static cudaError_t stage_yinv_go(const Geom& g, const Buffers& b, int s, bool fused, const double2* extra,
+                                 cudaStream_t st) {
+    if (!fused) {
+        switch (s) {
+            case 0: return stage_yinv_s<0, NZ, NY>(g, b, st);
+            case 1: return stage_yinv_s<1, NZ, NY>(g, b, st);
+            case 2: return stage_yinv_s<2, NZ, NY>(g, b, st);
+            case 3: return stage_yinv_s<3, NZ, NY>(g, b, st);
+            case 4: return stage_yinv_s<4, NZ, NY>(g, b, st);
+            case 5: return stage_yinv_s<5, NZ, NY>(g, b, st);
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (s) {
+        case 2: return yfwd_stage_yinv_s<2, NZ, NY>(g, b, extra, st);
+        case 3: return yfwd_stage_yinv_s<3, NZ, NY>(g, b, extra, st);
+        case 4: return yfwd_stage_yinv_s<4, NZ, NY>(g, b, extra, st);
+        case 5: return yfwd_stage_yinv_s<5, NZ, NY>(g, b, extra, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int NZ>
+static cudaError_t stage_yinv_nz(const Geom& g, const Buffers& b, int s, bool fused, const double2* extra,
+                                 cudaStream_t st) {
+    switch (g.ny) {
+        case 128: return stage_yinv_go<NZ, 128>(g, b, s, fused, extra, st);
+        case 256:
+            if constexpr (stage_yinv_built(256, NZ)) return stage_yinv_go<NZ, 256>(g, b, s, fused, extra, st);
+            return cudaErrorInvalidValue;
+        case 512:
+            if constexpr (stage_yinv_built(512, NZ)) return stage_yinv_go<NZ, 512>(g, b, s, fused, extra, st);
+            return cudaErrorInvalidValue;
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+static cudaError_t stage_yinv_dispatch(const Geom& g, const Buffers& b, int s, bool fused, const double2* extra,
+                                       cudaStream_t st) {
+    switch (g.nz) {
+        case 2: return stage_yinv_nz<2>(g, b, s, fused, extra, st);
+        case 4: return stage_yinv_nz<4>(g, b, s, fused, extra, st);
+        case 8: return stage_yinv_nz<8>(g, b, s, fused, extra, st);
+        case 16: return stage_yinv_nz<16>(g, b, s, fused, extra, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// small grids (at most kSmallStage kept mode-layers, a built (ny, nz) pair, the shared memory
+// fits) take the column kernels; QGN_NO_FUSED_STAGE=1 keeps the separate kernels
+bool stage_yinv_ok(const Geom& g, const Buffers& b) {
+    if (!b.mc_h || g.csize() > kSmallStage || std::getenv("QGN_NO_FUSED_STAGE")) return false;
+    if (g.nz != 2 && g.nz != 4 && g.nz != 8 && g.nz != 16) return false;
+    if (!stage_yinv_built(g.ny, g.nz)) return false;
+    const int TS = g.ny + g.ny / 16 + 8;
+    const size_t smem = (size_t)3 * g.nz * TS * 16 + (size_t)2 * g.nz * g.nky * 16;
+    return smem <= 220 * 1024;
+}
+
+cudaError_t launch_ark_stage_yinv(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
+    return stage_yinv_dispatch(g, b, s, false, nullptr, st);
+}
+
+cudaError_t launch_yfwd_stage_yinv(const Geom& g, const Buffers& b, int s, const double2* extra, cudaStream_t st) {
+    return stage_yinv_dispatch(g, b, s, true, extra, st);
 }
 
 cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, float2* psi, cudaStream_t st) {
