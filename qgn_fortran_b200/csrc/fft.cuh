@@ -214,7 +214,9 @@ __device__ __forceinline__ void apply_twiddles(CT* v, int k, const CT* __restric
 enum FftSrc { SRC_SMEM = 0, SRC_FN = 1, SRC_FN_SMEM = 2 };   // SRC_FN_SMEM: a functor that reads this smem
 // DST_SMEM_MAP: the last pass writes x[st(idx)] (st maps an output index to a shared-memory
 // offset) with the barriers of DST_SMEM
-enum FftDst { DST_SMEM = 0, DST_FN = 1, DST_SMEM_MAP = 2 };
+// DST_SMEM_STORE: the last pass hands each output to st(idx, value), which stores it in the
+// transform's own shared buffer in a layout of its choice, with the barriers of DST_SMEM
+enum FftDst { DST_SMEM = 0, DST_FN = 1, DST_SMEM_MAP = 2, DST_SMEM_STORE = 3 };
 
 // One Stockham DIT pass (sub-length NS, radix R) of an N-point transform whose
 // intermediate lives padded at x.  Pass 0 may read through ld(idx), the last pass may
@@ -254,7 +256,7 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
             }
         }
     }
-    constexpr bool TO_SMEM = (DST == DST_SMEM || DST == DST_SMEM_MAP);
+    constexpr bool TO_SMEM = (DST == DST_SMEM || DST == DST_SMEM_MAP || DST == DST_SMEM_STORE);
     if constexpr (TO_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
     if (active) {
 #pragma unroll

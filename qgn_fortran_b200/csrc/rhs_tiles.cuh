@@ -259,19 +259,26 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
         if (k > NX - nkx) return F[g.nkxp + (NX - k)];
         return cmk<CT>(0.0, 0.0);
     };
-    NoIOT<CT> none;
-    fft_fused<NX, +1, SRC_FN, DST_SMEM, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < 3, twx, ld_inv, none);
+    // the last pass stores the two rows apart, as real planes: row 2p at RT offset 0 of the
+    // slot, row 2p+1 at RT offset TS, so that each forward transform below reads only its
+    // own row (half the bytes of reading the packed complex values)
+    RT* plane = reinterpret_cast<RT*>(xs);
+    auto st_inv = [&](int x, CT v) {
+        plane[x] = v.x;
+        plane[C::TS + x] = v.y;
+    };
+    fft_fused<NX, +1, SRC_FN, DST_SMEM_STORE, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < 3, twx, ld_inv,
+                                                                     st_inv);
 
     // ---- forward: slot 0 = u1 q1 + i v1 q1, 1 = u2 q2 + i v2 q2 (grid/(nx*ny) scaling as in
     //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
     const RT sc = (RT)g.inv_nxny;
+    // this slot's row in the planes of the q, u, v slots (RT offsets 0, 2 TS, 4 TS)
+    const RT* rows = reinterpret_cast<const RT*>(base) + ((s_of & 1) ? C::TS : 0);
     auto ld_fwd = [&](int x) -> CT {
-        const int px = fpad<C::TP>(x);
-        const CT a = base[px], bu = base[C::TS + px], cv = base[2 * C::TS + px];
-        const bool second = (s_of & 1) != 0;
-        const RT qv = (second ? a.y : a.x) * sc;
-        const RT uv = (second ? bu.y : bu.x) * sc;
-        const RT vv = (second ? cv.y : cv.x) * sc;
+        const RT qv = rows[x] * sc;
+        const RT uv = rows[2 * C::TS + x] * sc;
+        const RT vv = rows[4 * C::TS + x] * sc;
         if (s_of < 2) return cmk<CT>(uv * qv, vv * qv);
         const RT m = sqrt(uv * uv + vv * vv);   // URMS, QGN_Module.f90:285
         return cmk<CT>(m * uv, m * vv);
