@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY,
 template <int NX, bool DRAG, class CT, int TV = 0>
 __global__ void __launch_bounds__(XCfg<NX, DRAG, CT, TV>::THREADS,
                                   minb(XCfg<NX, DRAG, CT, TV>::THREADS,
-                                       XCfg<NX, DRAG, CT, TV>::TP == 32 ? 112 : regcap<CT>(NX >= 1024 ? 112 : 128, 80)))
+                                       XCfg<NX, DRAG, CT, TV>::TP == 32 ? (sizeof(CT) == 16 ? 168 : 112) : regcap<CT>(NX >= 1024 ? 112 : 128, 80)))
     k_xpass(Geom g, int layer0, const CT* __restrict__ pq, const CT* __restrict__ pv,
             const CT* __restrict__ pu, CT* __restrict__ pp, CT* __restrict__ pd,
             const CT* __restrict__ twx) {

@@ -44,13 +44,14 @@ __host__ __device__ constexpr int regcap(int fp64 = 128, int fp32 = 64) { return
 // the single-field launches; a non-zero value is the CTA size in threads (per slot group for
 // the x pass), the same for every transform length, which lets one launch cover fields of
 // different sizes (ensembles).
-// elements per thread of an x transform (fft.cuh): 32 for the FP32 512- and 1024-point
-// transforms of the single-field x pass (two radix passes instead of three, each transform in
-// one warp), 16 otherwise.  The y passes keep 16 in FP32: their CTAs interleave columns across
-// warps, and at 32 elements they had half the threads per column and ran 1.3-1.7x slower on
-// B200.
+// elements per thread of an x transform (fft.cuh): 32 for the 512- and 1024-point transforms of
+// the single-field x pass (two radix passes instead of three, each transform in one warp: the
+// FP32 x pass ran 9 % faster, the FP64 one cut the 1024^2 x 8 step by 2 % despite 168
+// registers), 16 otherwise.  The y passes keep 16 in FP32: their CTAs interleave columns
+// across warps, and at 32 elements they had half the threads per column and ran 1.3-1.7x
+// slower on B200.
 template <class CT, int N, int TV>
-__host__ __device__ constexpr int fft_tp() { return (TV == 0 && sizeof(CT) == 8 && (N == 512 || N == 1024)) ? 32 : 16; }
+__host__ __device__ constexpr int fft_tp() { return (TV == 0 && (N == 512 || N == 1024)) ? 32 : 16; }
 // elements per thread of a y transform: 8 for the FP64 512- and 1024-point columns of the
 // single-field launches, 16 otherwise.  Half the registers per thread (64, two 512-thread CTAs
 // per SM) doubles the resident warps of these latency-bound kernels at the price of a fourth
