@@ -55,13 +55,19 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const __grid_constant_
 // Single-field launches of the tile bodies (rhs_tiles.cuh): one CTA per tile, tile = blockIdx
 // ------------------------------------------------------------------------------------
 // TV selects a tile width (0: the default; see the configs in rhs_tiles.cuh)
-// with more than one field, the narrow variants spread the fields over CTAs (blockIdx.z)
+// with more than one field, the narrow variants and the FP64 512- and 1024-point launches
+// spread the fields over CTAs (blockIdx.z): 688 CTAs of one FP64 1024^2 x 8 launch filled 2.3
+// waves of the 296 resident slots, three times as many fill 7 (the 1024^2 x 8 step ran 3 %
+// faster, 512^2 x 4 8 %)
+template <int NY, class CT, int TV>
+constexpr bool yinv_spread() { return TV != 0 || (sizeof(CT) == 16 && NY >= 512); }
+
 template <int NY, int NF, class CT, int TV = 0>
 __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, YInvCfg<NY, CT, TV>::TP == 8 ? 64 : regcap<CT>()))
     k_yinv(Geom g, const CT* __restrict__ q, const CT* __restrict__ psi, CT* __restrict__ pq,
            CT* __restrict__ pv, CT* __restrict__ pu, const CT* __restrict__ twy) {
     QGN_PDL_ENTRY();
-    if (TV != 0 && NF > 1)
+    if constexpr (yinv_spread<NY, CT, TV>() && NF > 1)
         yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy, blockIdx.z, blockIdx.z + 1);
     else
         yinv_tile<NY, NF, CT, TV>(g, blockIdx.x, blockIdx.y, q, psi, pq, pv, pu, twy);
@@ -230,7 +236,7 @@ static cudaError_t yinv_go(const Geom& g, const CT* q, const CT* psi, CT* hq, CT
     using C = YInvCfg<NY, CT, TV>;
     cudaError_t e;
     if ((e = set_smem(k_yinv<NY, NF, CT, TV>, C::SMEM)) != cudaSuccess) return e;
-    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz, (TV != 0 && NF > 1) ? NF : 1);
+    dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz, (yinv_spread<NY, CT, TV>() && NF > 1) ? NF : 1);
     const double es = (double)sizeof(CT);
     const double Cb = es * (double)g.csize(), Hb = es * (double)g.nz * NY * g.nkx;
     QGN_LAUNCH(KID_YINV, NF == 3 ? 2.0 * Cb + 3.0 * Hb : NF * (Cb + Hb), s,
