@@ -55,12 +55,12 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const __grid_constant_
 // Single-field launches of the tile bodies (rhs_tiles.cuh): one CTA per tile, tile = blockIdx
 // ------------------------------------------------------------------------------------
 // TV selects a tile width (0: the default; see the configs in rhs_tiles.cuh)
-// with more than one field, the narrow variants and the FP64 512- and 1024-point launches
-// spread the fields over CTAs (blockIdx.z): 688 CTAs of one FP64 1024^2 x 8 launch filled 2.3
-// waves of the 296 resident slots, three times as many fill 7 (the 1024^2 x 8 step ran 3 %
-// faster, 512^2 x 4 8 %)
+// with more than one field, the narrow variants and the 512- and 1024-point launches spread the
+// fields over CTAs (blockIdx.z): 688 CTAs of one FP64 1024^2 x 8 launch filled 2.3 waves of the
+// 296 resident slots, three times as many fill 7 (the 1024^2 x 8 step ran 3 % faster, 512^2 x 4
+// 8 %); in FP32 the same spread cut the mixed-precision 1024^2 x 8 step by 4 %
 template <int NY, class CT, int TV>
-constexpr bool yinv_spread() { return TV != 0 || (sizeof(CT) == 16 && NY >= 512); }
+constexpr bool yinv_spread() { return TV != 0 || NY >= 512; }
 
 template <int NY, int NF, class CT, int TV = 0>
 __global__ void __launch_bounds__(YInvCfg<NY, CT, TV>::THREADS, minb(YInvCfg<NY, CT, TV>::THREADS, YInvCfg<NY, CT, TV>::TP == 8 ? 64 : regcap<CT>()))
