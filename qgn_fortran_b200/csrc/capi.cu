@@ -247,11 +247,20 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
         CK(launch_rhs32(g, b, f32(b.err), f32(b.psi), f32(b.N[0]), drag_on(ctx), st));
     } else if (stage_yinv_ok(g, b)) {
         // small grids: GetPsi and the y-inverse of the first RHS in one launch per column.  An
-        // attached closure needs psi first, and its input transform reuses the packed-row
-        // buffers, so it runs after a separate GetPsi (which the column kernel repeats).
+        // attached closure (its own GetPsi, the network, the budget check) runs on its own
+        // stream beside that launch and the x pass, which read none of its outputs; the
+        // y-forward pass that adds S waits for it.
+        if (ctx->closure && !drag_on(ctx)) {
+            RET(closure_fork(ctx));
+            CK(launch_ark_stage_yinv(g, b, 0, st));
+            CK(launch_rhs_x(g, b, false, st));
+            RET(closure_join(ctx));
+            CK(launch_rhs_yfwd(g, b, b.q, b.psi, b.N[0], false, st, closure_tendency(ctx)));
+            return QGN_OK;
+        }
         if (ctx->closure) {
             CK(launch_modal(g, b, b.q, b.psi, st));
-            RET(closure_eval(ctx));
+            RET(closure_eval(ctx, b.psi, st));
         }
         CK(launch_ark_stage_yinv(g, b, 0, st));
         CK(launch_rhs_tail(g, b, b.q, b.psi, b.N[0], drag_on(ctx), st, closure_tendency(ctx)));
@@ -259,7 +268,7 @@ int ark_prologue(qgn_ctx* ctx, bool leith) {
         CK(launch_modal(g, b, b.q, b.psi, st));
         // the learned closure (if attached): S of this step's state and the budget check that
         // keeps it (background A8) or falls back to the Leith A8L just computed
-        if (ctx->closure) RET(closure_eval(ctx));
+        if (ctx->closure) RET(closure_eval(ctx, b.psi, st));
         RET(rhs_of(ctx, b.q, b.psi, b.N[0]));
     }
     return QGN_OK;

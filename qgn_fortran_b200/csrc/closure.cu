@@ -45,6 +45,11 @@ struct Closure {
     __nv_bfloat16* x = nullptr;       // [ny][nx][cin_p]
     float* y = nullptr;               // [cout_p][ny*nx] (planar network output)
     double2* S = nullptr;             // compact closure tendency
+    double2* psi = nullptr;           // GetPsi of the state (compact), the closure's own copy
+    double2* hq = nullptr;            // packed-row scratch of the input and output transforms
+    double2* hu = nullptr;
+    cudaStream_t side = nullptr;      // the closure's stream when it runs beside the first RHS
+    cudaEvent_t fork = nullptr, join = nullptr;
     double* red = nullptr;            // 3 x nblocks partial sums
     double* flag = nullptr;           // 1 passing, 0 fallback
     ClosureStats* stats = nullptr;
@@ -141,9 +146,12 @@ __global__ void __launch_bounds__(256) k_budget_spec(Geom g, const double2* __re
     const size_t P = (size_t)g.nkx * g.nky;
     const int nb = gridDim.x;
     double a = 0.0, b = 0.0, c = 0.0;
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+    const size_t ne = (size_t)g.nz * P;   // one (layer, mode) per thread and pass
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += (size_t)gridDim.x * blockDim.x) {
+        const int l = (int)(e / P);
+        const size_t p = e - (size_t)l * P;
         const int kx = (int)(p / g.nky), m = (int)(p % g.nky);
-        for (int l = 0; l < g.nz; ++l) {
+        {
             const size_t lP = (size_t)l * P;
             double2 hq, hp, hs;
             double f;
@@ -193,13 +201,32 @@ __global__ void __launch_bounds__(256) k_budget_spec(Geom g, const double2* __re
     __syncthreads();
     if (!s_last) return;
     __shared__ int s_pass;
+    // the last block sums the partials with all its threads (a fixed order: per thread, then
+    // the warp's butterfly, then the warps in order)
+    __threadfence();
+    a = b = c = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        a += __ldcg(&red[i]);
+        b += __ldcg(&red[nb + i]);
+        c += __ldcg(&red[2 * nb + i]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (threadIdx.x % 32 == 0) {
+        sm[0][threadIdx.x / 32] = a;
+        sm[1][threadIdx.x / 32] = b;
+        sm[2][threadIdx.x / 32] = c;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
         double sa = 0.0, sb = 0.0, sc2 = 0.0;
-        for (int i = 0; i < nb; ++i) {
-            sa += __ldcg(&red[i]);
-            sb += __ldcg(&red[nb + i]);
-            sc2 += __ldcg(&red[2 * nb + i]);
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) {
+            sa += sm[0][i];
+            sb += sm[1][i];
+            sc2 += sm[2][i];
         }
         const double N = (double)g.nx * (double)g.ny, inv = 1.0 / (N * N);
         const double dE = -sa * inv, dZ = sb * inv, E = -0.5 * sc2 * inv;
@@ -241,29 +268,55 @@ bool compatible(const qgn_ctx* f, const qgn_ctx* c) {
 // the closure's tendency (compact) for the stage right-hand sides, or NULL
 const double2* closure_tendency(const qgn_ctx* ctx) { return ctx->closure ? ctx->closure->S : nullptr; }
 
-// evaluate the network on the state (b.q, with b.psi = GetPsi(b.q)) and run the budget check:
-// y-inverse of (q, psi) and an x-inverse that writes the network input, the network, the
-// forward transform of its output, the budget kernel -- eleven launches with the six convolutions
-int closure_eval(qgn_ctx* ctx) {
+// evaluate the network on the state (b.q, with psi = GetPsi(b.q)) on stream st and run the
+// budget check: y-inverse of (q, psi) and an x-inverse that writes the network input, the
+// network, the forward transform of its output, the budget kernel.  It writes only the
+// closure's own buffers and, when the check passes, the layers' A8 in the device scalars.
+int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st) {
     Closure* c = ctx->closure;
     const Geom& g = ctx->g;
     const Buffers& b = ctx->b;
-    cudaStream_t st = ctx->stream;
-    if (launch_closure_input(g, b, b.q, b.psi, c->scales, c->x, c->cin_p, st) != cudaSuccess) return QGN_ERR_CUDA;
-    if (cnn::infer(c->net, c->x, c->y, 1, st, true) != QGN_OK) return QGN_ERR_CUDA;   // planar output
-    if (launch_closure_output(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->S, st) != cudaSuccess)
+    if (launch_closure_input(g, b, b.q, psi, c->hq, c->hu, c->scales, c->x, c->cin_p, st) != cudaSuccess)
         return QGN_ERR_CUDA;
-    const int nb = (int)std::min<size_t>(((size_t)g.nkx * g.nky + 255) / 256, (size_t)c->nblocks);
+    if (cnn::infer(c->net, c->x, c->y, 1, st, true) != QGN_OK) return QGN_ERR_CUDA;   // planar output
+    if (launch_closure_output(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->hq, c->S, st) != cudaSuccess)
+        return QGN_ERR_CUDA;
+    const int nb = (int)std::min<size_t>((g.csize() + 255) / 256, (size_t)c->nblocks);
     QGN_LAUNCH(KID_PARSEVAL, 48.0 * g.csize(), st,
-               ::qgn::launch(k_budget_spec, nb, 256, 0, st, g, b.q, b.psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
+               ::qgn::launch(k_budget_spec, nb, 256, 0, st, g, b.q, psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
                                                   c->stats, c->flag));
     if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
     return QGN_OK;
 }
 
+// The closure on its own stream, forked from the context's stream: GetPsi into the closure's
+// copy, then closure_eval.  The context's stream may meanwhile run work that reads b.q and
+// writes none of the closure's buffers, S, or the A8 of the device scalars (the first RHS's
+// y-inverse and x pass); closure_join makes it wait for the closure before anything reads S.
+int closure_fork(qgn_ctx* ctx) {
+    Closure* c = ctx->closure;
+    if (cudaEventRecord(c->fork, ctx->stream) != cudaSuccess || cudaStreamWaitEvent(c->side, c->fork, 0) != cudaSuccess)
+        return QGN_ERR_CUDA;
+    if (launch_modal(ctx->g, ctx->b, ctx->b.q, c->psi, c->side) != cudaSuccess) return QGN_ERR_CUDA;
+    const int rc = closure_eval(ctx, c->psi, c->side);
+    if (rc != QGN_OK) return rc;
+    return cudaEventRecord(c->join, c->side) == cudaSuccess ? QGN_OK : QGN_ERR_CUDA;
+}
+
+int closure_join(qgn_ctx* ctx) {
+    return cudaStreamWaitEvent(ctx->stream, ctx->closure->join, 0) == cudaSuccess ? QGN_OK : QGN_ERR_CUDA;
+}
+
 void closure_free(qgn_ctx* ctx) {
     Closure* c = ctx->closure;
     if (!c) return;
+    if (c->side) cudaStreamSynchronize(c->side);
+    cudaFree(c->psi);
+    cudaFree(c->hq);
+    cudaFree(c->hu);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
+    if (c->side) cudaStreamDestroy(c->side);
     cudaFree(c->scales);
     cudaFree(c->x);
     cudaFree(c->y);
@@ -371,11 +424,17 @@ int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const 
     c->cin_p = cnn::padded_in(net);
     c->cout_p = cnn::padded_out(net);
     c->nblocks = kBudgetBlocks;
-    const size_t npix = (size_t)g.nx * g.ny, np = npix * g.nz;
+    const size_t npix = (size_t)g.nx * g.ny;
     bool ok = cudaMalloc((void**)&c->scales, sizeof(float) * 3 * g.nz) == cudaSuccess &&
               cudaMalloc((void**)&c->x, sizeof(__nv_bfloat16) * npix * c->cin_p) == cudaSuccess &&
               cudaMalloc((void**)&c->y, sizeof(float) * npix * c->cout_p) == cudaSuccess &&
               cudaMalloc((void**)&c->S, sizeof(double2) * g.csize()) == cudaSuccess &&
+              cudaMalloc((void**)&c->psi, sizeof(double2) * g.csize()) == cudaSuccess &&
+              cudaMalloc((void**)&c->hq, sizeof(double2) * g.hsize()) == cudaSuccess &&
+              cudaMalloc((void**)&c->hu, sizeof(double2) * g.hsize()) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc((void**)&c->red, sizeof(double) * 3 * c->nblocks) == cudaSuccess &&
               cudaMalloc((void**)&c->flag, sizeof(double)) == cudaSuccess &&
               cudaMalloc((void**)&c->stats, sizeof(ClosureStats)) == cudaSuccess;

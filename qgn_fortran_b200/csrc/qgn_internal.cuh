@@ -209,14 +209,17 @@ namespace qgn {
 
 // the learned closure's tensors (rhs_kernels.cu): xout = NHWC BF16 [ny][nx][cin_p] with
 // channels (q_0..q_nz-1, psi_0..psi_nz-1) * scale; out = forward transform (compact, dealiased)
-// of channel l of the planar FP32 y[channel][ny*nx] divided by osc[l].  Both use b.hq/b.hu as scratch.
-cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
-                                 const float* scale, void* xout, int cin_p, cudaStream_t s);
+// of channel l of the planar FP32 y[channel][ny*nx] divided by osc[l].  hq, hu and h are
+// packed-row scratch of g.hsize() elements each (h may be hq).
+cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* hq,
+                                 double2* hu, const float* scale, void* xout, int cin_p, cudaStream_t s);
 cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
-                                  double2* out, cudaStream_t s);
+                                  double2* h, double2* out, cudaStream_t s);
 
 // ---- learned closure (closure.cu) and graph invalidation (capi.cu) -----------------------
-int closure_eval(qgn_ctx* ctx);
+int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st);
+int closure_fork(qgn_ctx* ctx);
+int closure_join(qgn_ctx* ctx);
 void closure_free(qgn_ctx* ctx);
 const double2* closure_tendency(const qgn_ctx* ctx);
 void drop_graphs(qgn_ctx* ctx);

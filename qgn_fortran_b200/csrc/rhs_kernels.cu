@@ -448,33 +448,34 @@ cudaError_t launch_maxabs_phys32(const Geom& g, const Buffers& b, const float2* 
 
 template <int NX, int SRC, int TV>
 static cudaError_t xfwd1_go(const Geom& g, const Buffers& b, const double* phys, const float* y, int cout_p,
-                            const float* osc, cudaStream_t s) {
+                            const float* osc, double2* dst, cudaStream_t s) {
     using C = X1Cfg<NX, TV>;
     cudaError_t e;
     if ((e = set_smem(k_xfwd1<NX, SRC, TV>, C::SMEM)) != cudaSuccess) return e;
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, g.nz);
     QGN_LAUNCH(KID_XFWD1, (SRC ? 4.0 : 8.0) * (double)g.nz * g.ny * NX + 16.0 * (double)g.nz * g.ny * g.nkx, s,
-               ::qgn::launch(k_xfwd1<NX, SRC, TV>, grid, C::THREADS, C::SMEM, s, g, phys, b.hq, b.twx, y, cout_p, osc));
+               ::qgn::launch(k_xfwd1<NX, SRC, TV>, grid, C::THREADS, C::SMEM, s, g, phys, dst, b.twx, y, cout_p, osc));
     return cudaGetLastError();
 }
 
 // forward x transform of a physical field (SRC 0) or of the closure's NHWC output (SRC 1)
+// into packed rows at dst
 template <int SRC>
 static cudaError_t launch_xfwd1(const Geom& g, const Buffers& b, const double* phys, const float* y, int cout_p,
-                                const float* osc, cudaStream_t s) {
+                                const float* osc, double2* dst, cudaStream_t s) {
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
         constexpr int NX = decltype(NXc)::value;
         if constexpr (has_narrow<NX>()) {
             const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * g.nz;
             const long long cn = (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * g.nz;
-            if (narrow_better(cd, cn)) return xfwd1_go<NX, SRC, kNarrowX1>(g, b, phys, y, cout_p, osc, s);
+            if (narrow_better(cd, cn)) return xfwd1_go<NX, SRC, kNarrowX1>(g, b, phys, y, cout_p, osc, dst, s);
         }
-        return xfwd1_go<NX, SRC, 0>(g, b, phys, y, cout_p, osc, s);
+        return xfwd1_go<NX, SRC, 0>(g, b, phys, y, cout_p, osc, dst, s);
     });
 }
 
 cudaError_t launch_from_phys(const Geom& g, const Buffers& b, const double* phys, double2* out, cudaStream_t s) {
-    cudaError_t e = launch_xfwd1<0>(g, b, phys, nullptr, 0, nullptr, s);
+    cudaError_t e = launch_xfwd1<0>(g, b, phys, nullptr, 0, nullptr, b.hq, s);
     if (e != cudaSuccess) return e;
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
@@ -511,20 +512,20 @@ __global__ void __launch_bounds__(X1Cfg<NX, TV>::THREADS, minb(X1Cfg<NX, TV>::TH
 }
 
 template <int NX, int TV>
-static cudaError_t xpack_go(const Geom& g, const Buffers& b, const float* scale, __nv_bfloat16* xout, int cin_p,
-                            cudaStream_t s) {
+static cudaError_t xpack_go(const Geom& g, const Buffers& b, const double2* hq, const double2* hu, const float* scale,
+                            __nv_bfloat16* xout, int cin_p, cudaStream_t s) {
     using C = X1Cfg<NX, TV>;
     cudaError_t e;
     if ((e = set_smem(k_xpack<NX, TV>, C::SMEM)) != cudaSuccess) return e;
     dim3 grid((g.ny / 2 + C::RP - 1) / C::RP, 2 * g.nz);
     QGN_LAUNCH(KID_XINV1, 2.0 * (16.0 * g.nz * g.ny * g.nkx + 2.0 * g.nz * g.ny * NX), s,
-               ::qgn::launch(k_xpack<NX, TV>, grid, C::THREADS, C::SMEM, s, g, b.hq, b.hu, b.twx, scale, xout, cin_p));
+               ::qgn::launch(k_xpack<NX, TV>, grid, C::THREADS, C::SMEM, s, g, hq, hu, b.twx, scale, xout, cin_p));
     return cudaGetLastError();
 }
 
-cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi,
-                                 const float* scale, void* xout, int cin_p, cudaStream_t s) {
-    cudaError_t e = launch_yinv<double2>(g, 2, q, psi, b.hq, nullptr, b.hu, b.twy, s);
+cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* hq,
+                                 double2* hu, const float* scale, void* xout, int cin_p, cudaStream_t s) {
+    cudaError_t e = launch_yinv<double2>(g, 2, q, psi, hq, nullptr, hu, b.twy, s);
     if (e != cudaSuccess) return e;
     __nv_bfloat16* x = static_cast<__nv_bfloat16*>(xout);
     return dispatch_n(g.nx, [&](auto NXc) -> cudaError_t {
@@ -533,15 +534,15 @@ cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2*
             const long long cd = (long long)((g.ny / 2 + X1Cfg<NX>::RP - 1) / X1Cfg<NX>::RP) * 2 * g.nz;
             const long long cn =
                 (long long)((g.ny / 2 + X1Cfg<NX, kNarrowX1>::RP - 1) / X1Cfg<NX, kNarrowX1>::RP) * 2 * g.nz;
-            if (narrow_better(cd, cn)) return xpack_go<NX, kNarrowX1>(g, b, scale, x, cin_p, s);
+            if (narrow_better(cd, cn)) return xpack_go<NX, kNarrowX1>(g, b, hq, hu, scale, x, cin_p, s);
         }
-        return xpack_go<NX, 0>(g, b, scale, x, cin_p, s);
+        return xpack_go<NX, 0>(g, b, hq, hu, scale, x, cin_p, s);
     });
 }
 
 cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
-                                  double2* out, cudaStream_t s) {
-    cudaError_t e = launch_xfwd1<1>(g, b, nullptr, y, cout_p, osc, s);
+                                  double2* h, double2* out, cudaStream_t s) {
+    cudaError_t e = launch_xfwd1<1>(g, b, nullptr, y, cout_p, osc, h, s);
     if (e != cudaSuccess) return e;
     return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
         constexpr int NY = decltype(NYc)::value;
@@ -550,7 +551,7 @@ cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* 
         if ((e2 = set_smem(k_yfwd1<NY>, C::SMEM)) != cudaSuccess) return e2;
         dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
         QGN_LAUNCH(KID_YFWD1, 16.0 * (double)g.nz * g.nkx * (NY + g.nky), s,
-                   ::qgn::launch(k_yfwd1<NY>, grid, C::THREADS, C::SMEM, s, g, b.hq, out, b.twy));
+                   ::qgn::launch(k_yfwd1<NY>, grid, C::THREADS, C::SMEM, s, g, h, out, b.twy));
         return cudaGetLastError();
     });
 }
