@@ -824,6 +824,15 @@ __device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, in
     // the own row needs no wait: it is this CTA's previous output (or the input)
     tc::fetch_row<CIN>(src, b, h, H, W, w0, in_a + (uint32_t)FL::SLOT_BYTES);
     tc::cp_commit();
+    // the epilogue's bias columns, loaded while the rows and the MMAs are in flight
+    const int warp = threadIdx.x / 32;
+    float breg[COUT == 64 ? 32 : 16];
+    {
+        constexpr int NCOL = COUT == 64 ? 32 : 16;
+        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+#pragma unroll
+        for (int j = 0; j < NCOL; ++j) breg[j] = a.bias[l][n0 + j];
+    }
     bool ok = true;
     if (l > 0 && threadIdx.x == 0)
         ok = tc::wait_flag(a.flags + tup, base + (unsigned)l) && tc::wait_flag(a.flags + tdn, base + (unsigned)l);
@@ -855,14 +864,6 @@ __device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, in
     if (l + 1 < a.L) {
         tc::fetch_weights(a.wt[l + 1], a.ci[l + 1], a.co[l + 1], w_a);
         tc::cp_commit();
-    }
-    const int warp = threadIdx.x / 32;
-    float breg[COUT == 64 ? 32 : 16];
-    {
-        constexpr int NCOL = COUT == 64 ? 32 : 16;
-        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
-#pragma unroll
-        for (int j = 0; j < NCOL; ++j) breg[j] = a.bias[l][n0 + j];
     }
     const size_t p0 = ((size_t)b * H + h) * W + w0;
     conv_tc_epilogue<CIN, COUT, EPI>(tmem, p0, breg, a.y, EPI == EPI_GELU_ACT ? a.act[l + 1] : nullptr, nullptr, stf,
