@@ -17,19 +17,16 @@
 //     dE = -sum_l H_l/Htot <psi_l S_l> <= limit * E / day,  E = -1/2 sum_l H_l/Htot <psi_l q_l>,
 // decides per step: passing, the step uses S with the background hyperviscosity A8_background;
 // failing, S is dropped and the step is plain QG-Leith (ARK43_QGLeith.f90:62-73).  The
-// averages are Parseval sums over the kept modes, taken inside the forward y transform of S.
+// averages are Parseval sums over the kept modes, so the check costs one launch.
 #include "qgn_internal.cuh"
 #include "cnn.cuh"
-#include "fft.cuh"
 #include "prof.cuh"
-#include "rhs_tiles.cuh"
 
 #include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cstring>
 #include <new>
-#include <type_traits>
 #include <vector>
 
 namespace qgn {
@@ -53,7 +50,7 @@ struct Closure {
     double2* hu = nullptr;
     cudaStream_t side = nullptr;      // the closure's stream when it runs beside the first RHS
     cudaEvent_t fork = nullptr, join = nullptr;
-    double* red = nullptr;            // 3 x nblocks partial sums of the budget check
+    double* red = nullptr;            // 3 x nblocks partial sums
     double* flag = nullptr;           // 1 passing, 0 fallback
     ClosureStats* stats = nullptr;
     double A8bg = 0.0, elimit = 0.0;
@@ -62,6 +59,7 @@ struct Closure {
 
 namespace {
 
+constexpr int kBudgetBlocks = 148;
 
 // sharp spectral cutoff: coarse compact <- fine compact on the coarse grid's kept modes,
 // rescaled for the unnormalised transforms
@@ -119,8 +117,8 @@ __global__ void k_pack_out(int nz, size_t npix, const double* __restrict__ s, co
         for (int c = 0; c < cout_p; ++c) y[p * cout_p + c] = c < nz ? (float)s[(size_t)c * npix + p] * osc[c] : 0.f;
 }
 
-// The energy-budget check of the applied tendency S (compact, dealiased), by Parseval on the
-// kept modes (the kx = 0 column in the Hermitian projection that the
+// The energy-budget check of the applied tendency S (compact, dealiased) in one launch, by
+// Parseval on the kept modes (the kx = 0 column in the Hermitian projection that the
 // inverse transform applies):
 //   <a b> = sum over the full plane of Re(conj(a_k) b_k) / (nx ny)^2,
 //   dE = -sum_l w_l <psi_l S_l>,  dZ = sum_l w_l <q_l S_l>,  E = -1/2 sum_l w_l <psi_l q_l>.
@@ -137,50 +135,74 @@ __device__ __forceinline__ double2 herm_proj(const Geom& g, const double2* __res
     return make_double2(0.5 * (v.x + fp.x), 0.5 * (v.y - fp.y));
 }
 
-// The block-level end of the budget check: a, b, c are this thread's partial sums of
-// <psi S>, <q S>, <psi q> (weighted).  The block's sums go to red[bid] (fixed order: the warp's
-// butterfly, then the warps in order); the block that finishes last sums the nb partials the
-// same way, decides, updates the statistics, and keeps S with the background A8 or zeroes S.
-__device__ __forceinline__ void budget_end(const Geom& g, double a, double b, double c, int bid, int nb,
-                                           double* __restrict__ red, double A8bg, double elimit,
-                                           DevScalars* __restrict__ sc, ClosureStats* __restrict__ st,
-                                           double* __restrict__ flag, double2* __restrict__ S) {
-    __shared__ double sm[3][32];
+__global__ void __launch_bounds__(256) k_budget_spec(Geom g, const double2* __restrict__ q,
+                                                     const double2* __restrict__ psi, double2* __restrict__ S,
+                                                     const double* __restrict__ Hw, double* __restrict__ red,
+                                                     double A8bg, double elimit, DevScalars* __restrict__ sc,
+                                                     ClosureStats* __restrict__ st, double* __restrict__ flag) {
+    QGN_PDL_ENTRY();
+    __shared__ double sm[3][8];
     __shared__ unsigned s_last;
-    __shared__ int s_pass;
-    const int nw = (int)(blockDim.x / 32);
-    auto block_sum = [&]() {
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_xor_sync(0xffffffffu, a, o);
-            b += __shfl_xor_sync(0xffffffffu, b, o);
-            c += __shfl_xor_sync(0xffffffffu, c, o);
-        }
-        if (threadIdx.x % 32 == 0) {
-            sm[0][threadIdx.x / 32] = a;
-            sm[1][threadIdx.x / 32] = b;
-            sm[2][threadIdx.x / 32] = c;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            a = b = c = 0.0;
-            for (int i = 0; i < nw; ++i) {
-                a += sm[0][i];
-                b += sm[1][i];
-                c += sm[2][i];
+    const size_t P = (size_t)g.nkx * g.nky;
+    const int nb = gridDim.x;
+    double a = 0.0, b = 0.0, c = 0.0;
+    const size_t ne = (size_t)g.nz * P;   // one (layer, mode) per thread and pass
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += (size_t)gridDim.x * blockDim.x) {
+        const int l = (int)(e / P);
+        const size_t p = e - (size_t)l * P;
+        const int kx = (int)(p / g.nky), m = (int)(p % g.nky);
+        {
+            const size_t lP = (size_t)l * P;
+            double2 hq, hp, hs;
+            double f;
+            if (kx > 0) {
+                hq = q[lP + p];
+                hp = psi[lP + p];
+                hs = S[lP + p];
+                f = 2.0;
+            } else {
+                bool pk;
+                hq = herm_proj(g, q, lP, m, pk);
+                hp = herm_proj(g, psi, lP, m, pk);
+                hs = herm_proj(g, S, lP, m, pk);
+                f = pk ? 1.0 : 2.0;
             }
+            const double w = Hw[l] * f;
+            a += w * (hp.x * hs.x + hp.y * hs.y);
+            b += w * (hq.x * hs.x + hq.y * hs.y);
+            c += w * (hp.x * hq.x + hp.y * hq.y);
         }
-    };
-    block_sum();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (threadIdx.x % 32 == 0) {
+        sm[0][threadIdx.x / 32] = a;
+        sm[1][threadIdx.x / 32] = b;
+        sm[2][threadIdx.x / 32] = c;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        red[bid] = a;
-        red[nb + bid] = b;
-        red[2 * nb + bid] = c;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) {
+            t0 += sm[0][i];
+            t1 += sm[1][i];
+            t2 += sm[2][i];
+        }
+        red[blockIdx.x] = t0;
+        red[nb + blockIdx.x] = t1;
+        red[2 * nb + blockIdx.x] = t2;
         __threadfence();
         const unsigned prev = atomicAdd(&st->red_count, 1u);
         s_last = (prev + 1 == (unsigned)nb) ? 1u : 0u;
     }
     __syncthreads();
     if (!s_last) return;
+    __shared__ int s_pass;
+    // the last block sums the partials with all its threads (a fixed order: per thread, then
+    // the warp's butterfly, then the warps in order)
     __threadfence();
     a = b = c = 0.0;
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
@@ -188,10 +210,26 @@ __device__ __forceinline__ void budget_end(const Geom& g, double a, double b, do
         b += __ldcg(&red[nb + i]);
         c += __ldcg(&red[2 * nb + i]);
     }
-    block_sum();
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (threadIdx.x % 32 == 0) {
+        sm[0][threadIdx.x / 32] = a;
+        sm[1][threadIdx.x / 32] = b;
+        sm[2][threadIdx.x / 32] = c;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
+        double sa = 0.0, sb = 0.0, sc2 = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) {
+            sa += sm[0][i];
+            sb += sm[1][i];
+            sc2 += sm[2][i];
+        }
         const double N = (double)g.nx * (double)g.ny, inv = 1.0 / (N * N);
-        const double dE = -a * inv, dZ = b * inv, E = -0.5 * c * inv;
+        const double dE = -sa * inv, dZ = sb * inv, E = -0.5 * sc2 * inv;
         const bool pass = (dZ <= 0.0) && (dE <= elimit * E / 86400.0) && (dE == dE) && (dZ == dZ);
         st->evaluations += 1;
         st->fallbacks += pass ? 0 : 1;
@@ -210,103 +248,6 @@ __device__ __forceinline__ void budget_end(const Geom& g, double a, double b, do
         const size_t n = g.csize();
         for (size_t e = threadIdx.x; e < n; e += blockDim.x) S[e] = make_double2(0.0, 0.0);
     }
-}
-
-// The forward y transform of the network's x-transformed output (packed rows h, the loop of
-// k_yfwd1 in rhs_kernels.cu) into the compact, dealiased S, fused with the budget check: each
-// thread adds the terms of the modes it stores (kx > 0, weight 2); after a barrier the block of
-// the kx = 0 column adds that column in the Hermitian projection, which pairs each mode with
-// its mirror.  One CTA per TKX kx columns of one layer.
-template <int NY>
-__global__ void __launch_bounds__(YInvCfg<NY>::THREADS)
-    k_yfwd_budget(Geom g, const double2* __restrict__ h, double2* __restrict__ S, const double2* __restrict__ twy,
-                  const double2* __restrict__ q, const double2* __restrict__ psi, const double* __restrict__ Hw,
-                  double* __restrict__ red, double A8bg, double elimit, DevScalars* __restrict__ sc,
-                  ClosureStats* __restrict__ st, double* __restrict__ flag) {
-    QGN_PDL_ENTRY();
-    using C = YInvCfg<NY>;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    double2* sm = reinterpret_cast<double2*>(sm_raw);
-    const int tid = threadIdx.x;
-    const int l = blockIdx.y;
-    const int slot = tid % C::TKX, lane = tid / C::TKX;
-    const int kx = blockIdx.x * C::TKX + slot;
-    const bool colok = kx < g.nkx;
-    const size_t lP = (size_t)l * g.nkx * g.nky;
-    const size_t colbase = lP + (size_t)kx * g.nky;
-    const double wl = Hw[l];
-    double a = 0.0, b = 0.0, c = 0.0;
-    auto ld = [&](int y) -> double2 {
-        return colok ? h[((size_t)l * NY + y) * g.nkxp + kx] : make_double2(0.0, 0.0);
-    };
-    auto stf = [&](int j, double2 v) {
-        const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
-        if (!colok || !kept) return;
-        const int m = j < g.kylo ? j : j - g.kyshift;
-        if (kx == 0 && m == 0) v = make_double2(0.0, 0.0);
-        S[colbase + m] = v;
-        if (kx > 0) {
-            const double2 hq = q[colbase + m], hp = psi[colbase + m];
-            const double w = 2.0 * wl;
-            a += w * (hp.x * v.x + hp.y * v.y);
-            b += w * (hq.x * v.x + hq.y * v.y);
-            c += w * (hp.x * hq.x + hp.y * hq.y);
-        }
-    };
-    fft_fused<NY, -1, SRC_FN, DST_FN, C::TP>(sm + slot * C::TS, lane, true, twy, ld, stf);
-    if (blockIdx.x == 0) {
-        __syncthreads();   // the block's stores of the kx = 0 column are visible to its threads
-        for (int m = tid; m < g.nky; m += C::THREADS) {
-            bool pk;
-            const double2 hq = herm_proj(g, q, lP, m, pk), hp = herm_proj(g, psi, lP, m, pk);
-            const int j = g.jfull(m), jp = (g.ny - j) % g.ny;
-            const double2 sv = __ldcg(&S[lP + m]);
-            double2 sp = make_double2(0.0, 0.0);
-            if (pk) sp = __ldcg(&S[lP + (jp < g.kylo ? jp : jp - g.kyshift)]);
-            const double2 hs = make_double2(0.5 * (sv.x + sp.x), 0.5 * (sv.y - sp.y));
-            const double w = wl * (pk ? 1.0 : 2.0);
-            a += w * (hp.x * hs.x + hp.y * hs.y);
-            b += w * (hq.x * hs.x + hq.y * hs.y);
-            c += w * (hp.x * hq.x + hp.y * hq.y);
-        }
-    }
-    budget_end(g, a, b, c, blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, red, A8bg, elimit, sc, st,
-               flag, S);
-}
-
-template <class F>
-cudaError_t with_ny(int ny, F&& f) {
-    switch (ny) {
-        case 16: return f(std::integral_constant<int, 16>{});
-        case 32: return f(std::integral_constant<int, 32>{});
-        case 64: return f(std::integral_constant<int, 64>{});
-        case 128: return f(std::integral_constant<int, 128>{});
-        case 256: return f(std::integral_constant<int, 256>{});
-        case 512: return f(std::integral_constant<int, 512>{});
-        case 1024: return f(std::integral_constant<int, 1024>{});
-        case 2048: return f(std::integral_constant<int, 2048>{});
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-// grid of k_yfwd_budget: TKX columns per CTA, one layer per grid row
-dim3 budget_grid(const Geom& g) {
-    dim3 grid(0, 0);
-    with_ny(g.ny, [&](auto NYc) -> cudaError_t {
-        constexpr int NY = decltype(NYc)::value;
-        grid = dim3((g.nkx + YInvCfg<NY>::TKX - 1) / YInvCfg<NY>::TKX, g.nz);
-        return cudaSuccess;
-    });
-    return grid;
-}
-
-// opt the fused kernel into its shared memory (outside any capture: at attach)
-cudaError_t budget_prepare(const Geom& g) {
-    return with_ny(g.ny, [&](auto NYc) -> cudaError_t {
-        constexpr int NY = decltype(NYc)::value;
-        if (YInvCfg<NY>::SMEM <= 48 * 1024) return cudaSuccess;
-        return cudaFuncSetAttribute(k_yfwd_budget<NY>, cudaFuncAttributeMaxDynamicSharedMemorySize, YInvCfg<NY>::SMEM);
-    });
 }
 
 int grid_of(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
@@ -329,9 +270,8 @@ const double2* closure_tendency(const qgn_ctx* ctx) { return ctx->closure ? ctx-
 
 // evaluate the network on the state (b.q, with psi = GetPsi(b.q)) on stream st and run the
 // budget check: y-inverse of (q, psi) and an x-inverse that writes the network input, the
-// network, the forward x transform of its output, and the forward y transform fused with the
-// budget check.  It writes only the closure's own buffers and, when the check passes, the
-// layers' A8 in the device scalars.
+// network, the forward transform of its output, the budget kernel.  It writes only the
+// closure's own buffers and, when the check passes, the layers' A8 in the device scalars.
 int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st) {
     Closure* c = ctx->closure;
     const Geom& g = ctx->g;
@@ -339,17 +279,14 @@ int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st) {
     if (launch_closure_input(g, b, b.q, psi, c->hq, c->hu, c->scales, c->x, c->cin_p, st) != cudaSuccess)
         return QGN_ERR_CUDA;
     if (cnn::infer(c->net, c->x, c->y, 1, st, true) != QGN_OK) return QGN_ERR_CUDA;   // planar output
-    if (launch_closure_output_x(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->hq, st) != cudaSuccess)
+    if (launch_closure_output(g, b, c->y, c->cout_p, c->scales + 2 * g.nz, c->hq, c->S, st) != cudaSuccess)
         return QGN_ERR_CUDA;
-    const cudaError_t e = with_ny(g.ny, [&](auto NYc) -> cudaError_t {
-        constexpr int NY = decltype(NYc)::value;
-        using C = YInvCfg<NY>;
-        QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.nz * g.nkx * (NY + g.nky) + 32.0 * g.csize(), st,
-                   ::qgn::launch(k_yfwd_budget<NY>, budget_grid(g), C::THREADS, C::SMEM, st, g, c->hq, c->S, b.twy,
-                                 b.q, psi, b.Hw, c->red, c->A8bg, c->elimit, b.sc, c->stats, c->flag));
-        return cudaGetLastError();
-    });
-    return e == cudaSuccess ? QGN_OK : QGN_ERR_CUDA;
+    const int nb = (int)std::min<size_t>((g.csize() + 255) / 256, (size_t)c->nblocks);
+    QGN_LAUNCH(KID_PARSEVAL, 48.0 * g.csize(), st,
+               ::qgn::launch(k_budget_spec, nb, 256, 0, st, g, b.q, psi, c->S, b.Hw, c->red, c->A8bg, c->elimit, b.sc,
+                                                  c->stats, c->flag));
+    if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+    return QGN_OK;
 }
 
 // The closure on its own stream, forked from the context's stream: GetPsi into the closure's
@@ -486,10 +423,7 @@ int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const 
     c->elimit = energy_limit;
     c->cin_p = cnn::padded_in(net);
     c->cout_p = cnn::padded_out(net);
-    {
-        const dim3 bg = budget_grid(g);
-        c->nblocks = (int)(bg.x * bg.y);
-    }
+    c->nblocks = kBudgetBlocks;
     const size_t npix = (size_t)g.nx * g.ny;
     bool ok = cudaMalloc((void**)&c->scales, sizeof(float) * 3 * g.nz) == cudaSuccess &&
               cudaMalloc((void**)&c->x, sizeof(__nv_bfloat16) * npix * c->cin_p) == cudaSuccess &&
@@ -501,7 +435,6 @@ int qgn_closure_attach(qgn_ctx* ctx, qgn_cnn* net, const float* in_scale, const 
               cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) == cudaSuccess &&
-              c->nblocks > 0 && budget_prepare(g) == cudaSuccess &&
               cudaMalloc((void**)&c->red, sizeof(double) * 3 * c->nblocks) == cudaSuccess &&
               cudaMalloc((void**)&c->flag, sizeof(double)) == cudaSuccess &&
               cudaMalloc((void**)&c->stats, sizeof(ClosureStats)) == cudaSuccess;

@@ -208,14 +208,13 @@ struct qgn_ctx {
 namespace qgn {
 
 // the learned closure's tensors (rhs_kernels.cu): xout = NHWC BF16 [ny][nx][cin_p] with
-// channels (q_0..q_nz-1, psi_0..psi_nz-1) * scale; h = forward x transform (packed rows) of
-// channel l of the planar FP32 y[channel][ny*nx] divided by osc[l], whose forward y transform
-// closure.cu fuses with the budget check.  hq, hu and h are packed-row scratch of g.hsize()
-// elements each (h may be hq).
+// channels (q_0..q_nz-1, psi_0..psi_nz-1) * scale; out = forward transform (compact, dealiased)
+// of channel l of the planar FP32 y[channel][ny*nx] divided by osc[l].  hq, hu and h are
+// packed-row scratch of g.hsize() elements each (h may be hq).
 cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double2* hq,
                                  double2* hu, const float* scale, void* xout, int cin_p, cudaStream_t s);
-cudaError_t launch_closure_output_x(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
-                                    double2* h, cudaStream_t s);
+cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
+                                  double2* h, double2* out, cudaStream_t s);
 
 // ---- learned closure (closure.cu) and graph invalidation (capi.cu) -----------------------
 int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st);

@@ -540,9 +540,20 @@ cudaError_t launch_closure_input(const Geom& g, const Buffers& b, const double2*
     });
 }
 
-cudaError_t launch_closure_output_x(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
-                                    double2* h, cudaStream_t s) {
-    return launch_xfwd1<1>(g, b, nullptr, y, cout_p, osc, h, s);
+cudaError_t launch_closure_output(const Geom& g, const Buffers& b, const float* y, int cout_p, const float* osc,
+                                  double2* h, double2* out, cudaStream_t s) {
+    cudaError_t e = launch_xfwd1<1>(g, b, nullptr, y, cout_p, osc, h, s);
+    if (e != cudaSuccess) return e;
+    return dispatch_n(g.ny, [&](auto NYc) -> cudaError_t {
+        constexpr int NY = decltype(NYc)::value;
+        using C = YInvCfg<NY>;
+        cudaError_t e2;
+        if ((e2 = set_smem(k_yfwd1<NY>, C::SMEM)) != cudaSuccess) return e2;
+        dim3 grid((g.nkx + C::TKX - 1) / C::TKX, g.nz);
+        QGN_LAUNCH(KID_YFWD1, 16.0 * (double)g.nz * g.nkx * (NY + g.nky), s,
+                   ::qgn::launch(k_yfwd1<NY>, grid, C::THREADS, C::SMEM, s, g, h, out, b.twy));
+        return cudaGetLastError();
+    });
 }
 
 // ------------------------------------------------------------------------------------
