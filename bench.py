@@ -322,7 +322,7 @@ def ours_arm(args):
         mms, mdays = reduce_over_ranks(mms, mdays, ws)
         mixed = {"value": mdays / (mms / 1000.0), "unit": UNIT, "ms_per_step": mms / args.steps,
                  "ms_per_step_vs_fp64": (ms_all / args.steps) / (mms / args.steps),
-                 "dtype": "f32 transforms/RHS/stage storage, f64 state/GetPsi/error norm/controller"}
+                 "dtype": "f32 transforms/RHS/stage storage/error spectrum and norm, f64 state/GetPsi/update/controller"}
         gm.cleanup()
 
     ensemble = None
