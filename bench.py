@@ -10,7 +10,7 @@ plus any rejected attempts).  Data are synthetic; the spin-up of the named confi
 ``value``: device-resident stepping (qgn_advance_resident, graph-launched steps), CUDA
 events on the library's stream.  ``e2e``: the drop-in path TimeStep (QGNModule.time_step ->
 qgn_step) with the host q_hat in pinned memory: every step copies the kept modes host->device
-and the whole array back.  ``mixed``: the same workload in the mixed-precision mode.
+and back.  ``mixed``: the same workload in the mixed-precision mode.
 ``cpu_baseline`` and ``--impl reference`` time the FP64 C/OpenMP restatement of the reference
 (oracle/qgn_ref.c) on all host threads.
 
@@ -290,10 +290,11 @@ def ours_arm(args):
         ems = e0.elapsed_time(e1)
         edays = (t - te0) / DAY
         ems, edays = reduce_over_ranks(ems, edays, ws)
+        # both directions move the kept modes only (two pitched copies each); TimeStep's
+        # trailing DeAlias (QGN_Module.f90:307) zeroes the rest of q_hat on the host
         kept = 16 * (w.params["nx"] // 3) * (w.params["ny"] - w.params["ny"] // 3 - 1) * w.params["nz"]
-        full = 16 * (w.params["nx"] // 2 + 1) * w.params["ny"] * w.params["nz"]
         e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
-               "d2h_bytes_per_step": full, "ms_per_step": ems / args.steps,
+               "d2h_bytes_per_step": kept, "ms_per_step": ems / args.steps,
                "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the IC"}
         gE.cleanup()
 

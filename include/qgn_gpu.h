@@ -80,9 +80,12 @@ int qgn_create(const qgn_params* p, const double* H, const double* S,
  * One call of TimeStep(q_hat,t,dt) (QGN_Module.f90:302-309) with the scheme chosen
  * at qgn_create.  q_hat is the host spectral array (interleaved complex, Fortran
  * order).  Only the modes that DeAlias keeps are read: the entries DeAlias zeroes
- * (QGN_Module.f90:194-204) are treated as zero on input.  On output the whole array is
- * written, with zeros where DeAlias zeroes (as after the reference's TimeStep, whose
- * trailing DeAlias call zeroes them).  t and dt are updated exactly as by the reference
+ * (QGN_Module.f90:194-204) are treated as zero on input.  On output only the kept modes
+ * are written (QGN_OUTPUT_KEPT, the default): the reference's TimeStep ends with
+ * `call DeAlias(q_hat)` (QGN_Module.f90:307), which zeroes the others on the host, and in a
+ * dealiased input -- every TimeStep output and Initialize's q_hat -- they are zero already.
+ * A caller that passes an array with data in the dealiased band and wants it cleared selects
+ * QGN_OUTPUT_FULL with qgn_set_output.  t and dt are updated exactly as by the reference
  * scheme.
  * Stepper memory (FSAL stage, AB history, err0) persists in the context like the
  * reference's `save` variables.
@@ -91,6 +94,16 @@ int qgn_step(qgn_ctx* ctx, double* q_hat, double* t, double* dt);
 
 /* nsteps consecutive TimeStep calls with one host<->device transfer of q_hat. */
 int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps);
+
+/*
+ * What qgn_step and qgn_advance write back to the host q_hat.  No counterpart in the
+ * reference (its TimeStep works on the host array in place).
+ *   QGN_OUTPUT_KEPT  the modes DeAlias keeps (two pitched copies, 44 % of the array bytes)
+ *   QGN_OUTPUT_FULL  the whole array, zeros where DeAlias zeroes
+ */
+#define QGN_OUTPUT_KEPT 0
+#define QGN_OUTPUT_FULL 1
+int qgn_set_output(qgn_ctx* ctx, int mode);
 
 /* Device-resident variants: the state lives on the GPU between calls. */
 int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt);
@@ -158,16 +171,6 @@ int qgn_profile_enable(qgn_ctx* ctx, int enable);
 int qgn_profile_read(qgn_ctx* ctx, int kernel, double* total_ms, double* bytes,
                      long long* timed_launches, long long* launches);
 const char* qgn_kernel_name(int kernel);
-
-/*
- * Debugging hook: copy one device work buffer to the host as interleaved doubles
- * (count = capacity in doubles).  which: 0 state q (compact [nz][nx/3][nky]), 1 psi of
- * the last evaluation (compact), 2..6 the half-transformed fields [nz][ny][nkxp] of the
- * last RHS as packed row pairs [nz][ny/2][2][nkxp]: 2 q, 3 v = i kx psi, 4 u = -i ky psi;
- * 5 the forward x transforms of u*q + i v*q, [nz][ny][2][nkxp] (P[k], P[nx-k] for k < nkx).
- * nkxp = nx/3 rounded up to a multiple of 4.
- */
-int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
 
 /* The cudaStream_t (as void*) all of this context's work is issued on. */
 int qgn_stream(qgn_ctx* ctx, void** stream);
@@ -262,9 +265,6 @@ int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, cons
 int qgn_cnn_set_engine(qgn_cnn* net, int engine);
 /* waits for the network's stream; QGN_ERR_CUDA if a tensor-core kernel reported a timeout */
 int qgn_cnn_check(qgn_cnn* net);
-/* failure injection for tests: set the fused inference's layer counter of one tile (a large
- * value makes that tile's bounded wait run out in the next fused launch) */
-int qgn_cnn_debug_set_counter(qgn_cnn* net, int tile, unsigned int value);
 int qgn_cnn_stream(qgn_cnn* net, void** stream);
 const char* qgn_cnn_last_error(const qgn_cnn* net);
 int qgn_cnn_destroy(qgn_cnn* net);

@@ -1,6 +1,6 @@
-"""ctypes binding of include/qgn_gpu.h.
+"""ctypes binding of include/qgn_gpu.h (and the test hooks of include/qgn_gpu_debug.h).
 
-This is the same binding a Python host (or the ctypes stub in INTEGRATION.md) makes.
+This is the same binding a Python host makes through ctypes.
 Loading fails loudly when the CUDA library has not been built: there is no CPU path.
 """
 from __future__ import annotations
@@ -20,6 +20,8 @@ QGN_ERR_ARG = 5
 QGN_ERR_NO_DEVICE = 6
 QGN_ERR_TOO_LARGE = 7
 QGN_STATIC_SCRATCH_BYTES = 32 * 1024 * 1024
+QGN_OUTPUT_KEPT = 0
+QGN_OUTPUT_FULL = 1
 QGN_KERNEL_FAMILIES = 14
 
 SCHEMES = {"ark43_qgleith": 0, "ark43": 1, "bsrk3": 2, "rk4": 3, "ab3": 4}
@@ -55,6 +57,7 @@ SIGNATURES = {
                              C.POINTER(C.c_void_p)]),
     "qgn_step": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_advance": (C.c_int, [_ctxp, _dp, _dp, _dp, C.c_int]),
+    "qgn_set_output": (C.c_int, [_ctxp, C.c_int]),
     "qgn_set_state": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),
     "qgn_get_state": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_advance_resident": (C.c_int, [_ctxp, C.c_int]),

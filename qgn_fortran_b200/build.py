@@ -36,7 +36,8 @@ def _stale(target: str, deps) -> bool:
 
 def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs.append(os.path.join(os.path.dirname(HERE), "include", "qgn_gpu.h"))
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    hs.extend(os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h"))
     return hs
 
 

@@ -125,17 +125,17 @@ int ensure_full(qgn_ctx* ctx) {
     return QGN_OK;
 }
 
-// compact device field -> host q_hat: the whole array in one contiguous copy, with zeros
-// where DeAlias zeroes (QGN_Module.f90:194-204) -- the values the reference's trailing
-// DeAlias in TimeStep leaves there
+int download_full(qgn_ctx* ctx, const double2* src, double* host);
+
+// compact device field -> host q_hat of TimeStep.  By default only the modes DeAlias keeps
+// cross the link (the same two pitched copies as the upload): the reference's TimeStep ends
+// with `call DeAlias(q_hat)` (QGN_Module.f90:307), which zeroes the others on the host, and
+// they are zero already in a dealiased input.  QGN_OUTPUT_FULL writes the whole array with
+// zeros in the dealiased band instead (one contiguous copy of 2.25x the bytes).
 int download_kept(qgn_ctx* ctx, const double2* src, double* host) {
-    RET(ensure_full(ctx));
-    const Geom& g = ctx->g;
-    CK(launch_compact_to_xfer(g, src, ctx->b.xfer, ctx->stream));
-    CK(launch_xfer_to_full(g, ctx->b.xfer, ctx->b.full, ctx->stream));
-    CK(cudaMemcpyAsync(host, ctx->b.full, sizeof(double2) * (size_t)g.nz * g.ny * g.nxh, cudaMemcpyDeviceToHost,
-                       ctx->stream));
-    return QGN_OK;
+    if (ctx->output_mode == QGN_OUTPUT_FULL) return download_full(ctx, src, host);
+    CK(launch_compact_to_xfer(ctx->g, src, ctx->b.xfer, ctx->stream));
+    return copy_kept(ctx, host, false);
 }
 
 // compact device field -> whole host q_hat (zeros in the dealiased band)
@@ -828,6 +828,13 @@ int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps) 
 }
 
 int qgn_step(qgn_ctx* ctx, double* q_hat, double* t, double* dt) { return qgn_advance(ctx, q_hat, t, dt, 1); }
+
+int qgn_set_output(qgn_ctx* ctx, int mode) {
+    if (!ctx) return QGN_ERR_ARG;
+    if (mode != QGN_OUTPUT_KEPT && mode != QGN_OUTPUT_FULL) return set_err(ctx, QGN_ERR_ARG, "unknown output mode");
+    ctx->output_mode = mode;
+    return QGN_OK;
+}
 
 int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
     if (!ctx) return QGN_ERR_ARG;

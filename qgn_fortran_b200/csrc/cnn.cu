@@ -1030,23 +1030,13 @@ cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat1
                           float* outf, __nv_bfloat16* outb, const float* zin) {
     if (n->engine == 0) {
         constexpr int SM = tc::Lay<CIN, COUT>::SMEM;
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-            if (e != cudaSuccess) return e;
-            attr = true;
-        }
+        if (cudaError_t e = smem_opt_in(k_conv_tc<CIN, COUT, EPI>, SM); e != cudaSuccess) return e;
         ::qgn::launch(k_conv_tc<CIN, COUT, EPI>, conv_grid(n, batch), kThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W,
                                                                                     outf, outb, zin, n->d_err);
         return cudaGetLastError();
     }
     constexpr int SM = conv_smem<CIN, COUT>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_conv<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (cudaError_t e = smem_opt_in(k_conv<CIN, COUT, EPI>, SM); e != cudaSuccess) return e;
     ::qgn::launch(k_conv<CIN, COUT, EPI>, conv_grid(n, batch), kThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W, outf,
                                                                              outb, zin);
     return cudaGetLastError();
@@ -1066,12 +1056,7 @@ template <int CIN, int COUT>
 cudaError_t launch_wgrad_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat16* g, int batch, float* part,
                            int* nchunks) {
     constexpr int SM = wgrad_smem<CIN, COUT>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (cudaError_t e = smem_opt_in(k_wgrad<CIN, COUT>, SM); e != cudaSuccess) return e;
     const int chunks = (batch * n->H + kWChunkRows - 1) / kWChunkRows;
     *nchunks = chunks;
     ::qgn::launch(k_wgrad<CIN, COUT>, dim3(chunks, 9), kThreads, SM, n->stream, x, g, batch, n->H, n->W, part);
@@ -1165,8 +1150,7 @@ bool fused_ok(qgn_cnn* net, int batch) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (cudaFuncSetAttribute(k_cnn_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::FusedLay::SMEM) !=
-                cudaSuccess ||
+        if (smem_opt_in(k_cnn_fused, tc::FusedLay::SMEM) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cnn_fused, kThreads, tc::FusedLay::SMEM) !=
                 cudaSuccess)
             per = 0;
@@ -1210,6 +1194,7 @@ int forward_fused(qgn_cnn* net, int batch, const __nv_bfloat16* x, float* y, boo
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    NCK(smem_opt_in(k_cnn_fused, tc::FusedLay::SMEM));   // per device: a no-op after the first
     NCK(cudaLaunchKernelEx(&cfg, k_cnn_fused, a));
     return QGN_OK;
 }

@@ -423,15 +423,7 @@ __global__ void k_ens_fsal_done(EnsMember* __restrict__ mem, int nm) {
 // attribute call happens while a graph is being captured
 template <class K>
 cudaError_t smem_attr(K kernel, int bytes) {
-    static std::mutex mu;
-    static std::unordered_set<const void*> done;
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    std::lock_guard<std::mutex> lk(mu);
-    const void* key = reinterpret_cast<const void*>(kernel);
-    if (done.count(key)) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) done.insert(key);
-    return e;
+    return smem_opt_in(kernel, bytes);
 }
 
 template <class CT, int TV>

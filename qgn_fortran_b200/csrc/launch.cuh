@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <utility>
 
 #define QGN_PDL_ENTRY() asm volatile("griddepcontrol.wait;" ::: "memory")
@@ -25,6 +27,30 @@
 namespace qgn {
 
 inline bool pdl_allowed() { return std::getenv("QGN_NO_PDL") == nullptr; }
+
+// Opt a kernel into `bytes` of dynamic shared memory (above the 48 KB default) on the current
+// device.  The attribute belongs to the device, so the opt-in is remembered per (device,
+// kernel) and made again for a larger size; later launches, including those recorded into CUDA
+// graphs, issue no attribute calls.
+inline cudaError_t smem_opt_in(const void* kernel, int bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair(dev, kernel);
+    const auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
+}
+template <class... KArgs>
+inline cudaError_t smem_opt_in(void (*kernel)(KArgs...), int bytes) {
+    return smem_opt_in(reinterpret_cast<const void*>(kernel), bytes);
+}
 
 // kernel<<<grid, block, smem, stream>>>(args...) with the programmatic-serialization attribute;
 // the error, if any, is left for cudaGetLastError like a <<<>>> launch.

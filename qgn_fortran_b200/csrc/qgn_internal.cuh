@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 #include "../../include/qgn_gpu.h"
+#include "../../include/qgn_gpu_debug.h"
 #include "prof.cuh"
 #include "launch.cuh"
 
@@ -185,6 +186,7 @@ struct qgn_ctx {
     std::vector<double> H, uBar, qyBar, Modes, EVals;
     // stepper memory (the reference's `save` variables); BSRK3's RHS0 and AB3's history
     // live in b.N[0..1], err0 / r0 in the device scalars
+    int output_mode = QGN_OUTPUT_KEPT;   // what qgn_step / qgn_advance write back (qgn_set_output)
     bool first_call = true;
     int ab_calls = 0;
     bool halted = false;           // a step failed; cleared by the next state upload

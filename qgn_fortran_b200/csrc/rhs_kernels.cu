@@ -200,20 +200,10 @@ static cudaError_t dispatch_n(int n, F&& f) {
     }
 }
 
-// Opt a kernel into more than 48 KB of dynamic shared memory once per process, so that
-// later launches -- including those recorded into CUDA graphs -- issue no attribute calls.
-static std::mutex g_attr_mu;
-static std::unordered_set<const void*> g_attr_done;
-
+// dynamic shared memory above 48 KB, opted into once per (device, kernel) (launch.cuh)
 template <class K>
 static cudaError_t set_smem(K kernel, int bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    std::lock_guard<std::mutex> lk(g_attr_mu);
-    const void* key = reinterpret_cast<const void*>(kernel);
-    if (g_attr_done.count(key)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) g_attr_done.insert(key);
-    return e;
+    return smem_opt_in(kernel, bytes);
 }
 
 cudaError_t launch_modal(const Geom& g, const Buffers& b, const double2* q, double2* psi, cudaStream_t s) {

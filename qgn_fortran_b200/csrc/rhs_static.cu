@@ -109,6 +109,24 @@ extern "C" int qgn_rhs_static(const qgn_params* p, const double* H, const double
         if (!(H[k] > 0) || !std::isfinite(H[k]) || !std::isfinite(uBar[k]) || !std::isfinite(qyBar[k]) ||
             !std::isfinite(EVals[k]))
             return QGN_ERR_CONFIG;
+    // the same checks qgn_create makes on the mode matrix and the scalar parameters
+    for (int i = 0; i < nz * nz; ++i)
+        if (!std::isfinite(Modes[i])) return QGN_ERR_CONFIG;
+    const double scal[] = {p->Lx, p->Ly, p->Htot, p->beta, p->A2, p->A8, p->r0, p->C_d};
+    for (double v : scal)
+        if (!std::isfinite(v)) return QGN_ERR_CONFIG;
+
+    int ndev = 0, dev = 0, major = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess || major != 10) {
+        cudaGetLastError();
+        return QGN_ERR_NO_DEVICE;
+    }
+    // the constant blocks are copied from this call's stack: a capture would record copies
+    // from a frame that is gone when the graph runs, so the call refuses to be captured
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap) != cudaSuccess) return QGN_ERR_CUDA;
+    if (cap != cudaStreamCaptureStatusNone) return QGN_ERR_CONFIG;
 
     Geom g;
     g.nx = p->nx; g.ny = p->ny; g.nz = nz; g.nxh = p->nx / 2 + 1;

@@ -884,16 +884,10 @@ constexpr bool stage_yinv_built(int ny, int nz) {
     return (ny == 128 && nz <= 16) || (ny == 256 && nz <= 8) || (ny == 512 && nz <= 4);
 }
 
-// the dynamic shared-memory limit of each column kernel, raised once per kernel
+// the dynamic shared-memory limit of each column kernel, raised once per (device, kernel)
 static cudaError_t column_smem(const void* kern, int bytes) {
-    static std::mutex mu;
-    static std::unordered_set<const void*> done;
     if (bytes <= 48 * 1024) return cudaSuccess;
-    std::lock_guard<std::mutex> lk(mu);
-    if (done.count(kern)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    if (e == cudaSuccess) done.insert(kern);
-    return e;
+    return smem_opt_in(kern, 227 * 1024);
 }
 
 template <int NZ, int NY, class Kern, class... Args>

@@ -146,11 +146,17 @@ class QGNModule:
         """TimeStep(q_hat, t, dt): advances q_hat in place; returns the new (t, dt)."""
         q_hat = self._spec(q_hat, writable=True)
         tt, dd = C.c_double(t), C.c_double(dt)
-        # qgn_step writes the whole array with zeros where TimeStep's trailing DeAlias
-        # (QGN_Module.f90:307) zeroes, so no host-side DeAlias pass is needed
+        # qgn_step writes back the kept modes; the entries TimeStep's trailing DeAlias
+        # (QGN_Module.f90:307) zeroes keep their input values, zero for a dealiased q_hat
+        # (set_output("full") writes them as zeros)
         self._check(self.lib.qgn_step(self.ctx, dptr(q_hat), C.byref(tt), C.byref(dd)), "qgn_step")
         self.t, self.dt = tt.value, dd.value
         return tt.value, dd.value
+
+    def set_output(self, mode: str):
+        """What time_step/advance write back: "kept" (the kept modes, default) or "full"."""
+        code = {"kept": _lib.QGN_OUTPUT_KEPT, "full": _lib.QGN_OUTPUT_FULL}[mode]
+        self._check(self.lib.qgn_set_output(self.ctx, code), "qgn_set_output")
 
     def advance(self, q_hat, t: float, dt: float, nsteps: int):
         q_hat = self._spec(q_hat, writable=True)

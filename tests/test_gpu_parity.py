@@ -235,3 +235,28 @@ def test_nonfinite_input_is_reported(cuda_ok):
         with pytest.raises(QGNError) as ei:
             g.time_step(q, 0.0, 500.0)
         assert ei.value.code == QGN_ERR_NONFINITE
+
+
+def test_step_output_modes(cuda_ok):
+    """qgn_step writes back the kept modes by default (TimeStep's trailing DeAlias,
+    QGN_Module.f90:307, zeroes the rest on the host); QGN_OUTPUT_FULL writes zeros there."""
+    w = workload("strat1024x8", nx=64, nz=3)
+    g1 = QGNModule(w.params, w.H, w.S, w.U, scheme="ark43_qgleith")
+    g2 = QGNModule(w.params, w.H, w.S, w.U, scheme="ark43_qgleith")
+    q = g1.initialize(w.qp, 0.0, 5000.0)
+    band = np.zeros(q.shape, dtype=bool)
+    ny, nx = 64, 64
+    band[:, ny // 3:2 * (ny // 3) + 1, :] = True
+    band[:, :, nx // 3:] = True
+    assert np.all(q[band] == 0)
+    qa, qb = q.copy(), q.copy()
+    marker = complex(3.0, -7.0)
+    qa[band] = marker
+    qb[band] = marker
+    ta = g1.time_step(qa, 0.0, 5000.0)
+    g2.set_output("full")
+    tb = g2.time_step(qb, 0.0, 5000.0)
+    assert ta == tb
+    assert np.all(qa[band] == marker)          # kept mode: the band is not written
+    assert np.all(qb[band] == 0)               # full mode: zeros, as after DeAlias
+    assert np.array_equal(qa[~band], qb[~band])

@@ -47,6 +47,17 @@ def test_rhs_static_matches_allocating_entry_point(cuda_ok):
                   r0=1.0e-7, C_d=1.0e-5, TOL=1.0e-12, is_explicit=True)
     g = QGNModule(params, H, S, U, scheme="ark43_qgleith")
     stream = torch.cuda.current_stream().cuda_stream
+    # a call on another geometry first: it leaves data at other offsets of the shared array
+    # (padding columns included), which the calls below must not pick up
+    H8, S8, U8 = exponential_stratification(8)
+    p8 = dict(params, nx=256, ny=256, nz=8, Ly=2.0e6, C_d=0.0)
+    g8 = QGNModule(p8, H8, S8, U8, scheme="ark43_qgleith")
+    q8 = g8.initialize(seeded_random_pv(256, 256, 8, 8.0, 1.0e-6, seed=5))
+    q8_dev = torch.from_numpy(q8).to("cuda")
+    out8_dev = torch.empty_like(q8_dev)
+    assert call_static(g8, q8_dev, out8_dev, stream) == _lib.QGN_OK
+    torch.cuda.synchronize()
+    assert np.all(layer_rel(out8_dev.cpu().numpy(), g8.get_rhs(q8)) <= RHS_TOL)
     for seed in (11, 12):     # two calls in a row: the second must not see the first's scratch
         q = g.initialize(seeded_random_pv(nx, ny, nz, 8.0, 1.0e-6, seed=seed))
         ref = g.get_rhs(q)
@@ -71,3 +82,21 @@ def test_rhs_static_rejects_grids_beyond_the_scratch(cuda_ok):
     out_dev = torch.empty_like(q_dev)
     rc = call_static(g, q_dev, out_dev, torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.QGN_ERR_TOO_LARGE
+
+
+def test_rhs_static_refuses_stream_capture(cuda_ok):
+    """The constants are copied from the call's stack, so a capture is refused, not recorded."""
+    import torch
+
+    nz = 2
+    H, S, U = exponential_stratification(nz)
+    params = dict(nx=64, ny=64, nz=nz, Lx=2.0e6, Ly=2.0e6, Htot=4000.0)
+    g = QGNModule(params, H, S, U)
+    q_dev = torch.zeros((nz, 64, 33), dtype=torch.complex128, device="cuda")
+    out_dev = torch.empty_like(q_dev)
+    s = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s, capture_error_mode="thread_local"):
+        rc = call_static(g, q_dev, out_dev, s.cuda_stream)
+        out_dev.zero_()     # one captured node, so the graph is not empty
+    assert rc == _lib.QGN_ERR_CONFIG
