@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-closure", action="store_true")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 2048^2 x 16 FP64/mixed leg")
+    ap.add_argument("--c3-steps", type=int, default=10)
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=20)
     return ap.parse_args()
@@ -326,6 +328,10 @@ def ours_arm(args):
                  "dtype": "f32 transforms/RHS/stage storage/error spectrum and norm, f64 state/GetPsi/update/controller"}
         gm.cleanup()
 
+    c3 = None
+    if not args.no_c3:
+        c3 = c3_bench(args, ws)
+
     ensemble = None
     if not args.no_ensemble:
         ensemble = ensemble_bench(args, ws)
@@ -377,12 +383,48 @@ def ours_arm(args):
                        "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
                        "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects(),
                        "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the seeded IC"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "ensemble": ensemble, "closure": closure, "gpu_launches": launches,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "mixed_2048x16": c3, "ensemble": ensemble, "closure": closure, "gpu_launches": launches,
             "clocks": clk, "kernels": kernels}
     print(json.dumps(line), flush=True)
     g.cleanup()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def c3_bench(args, ws):
+    """The mixed-precision configuration, 16 layers on 2048^2 (same stratification and mean flow,
+    ARK43_QGLeith with PI.3.4, seed 3): FP64 and mixed on the same window of steps from the
+    seeded IC, state resident in HBM, graph-launched steps, CUDA events on the library's stream."""
+    import torch
+
+    from qgn_fortran_b200 import QGNModule, _lib
+    from qgn_fortran_b200.inputs import workload
+
+    w = workload("strat2048x16")
+    out = {"workload": "strat2048x16", "grid": "2048x2048x16", "scheme": w.scheme, "steps": args.c3_steps,
+           "window": f"steps {args.warmup + 1}..{args.warmup + args.c3_steps} from the seeded IC"}
+    for prec in ("fp64", "mixed"):
+        g = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme, precision=prec)
+        g.initialize(w.qp, 0.0, w.dt0)
+        g.advance_resident(max(args.warmup, 1))
+        sp = _lib.C.c_void_p()
+        g.lib.qgn_stream(g.ctx, _lib.C.byref(sp))
+        st = torch.cuda.ExternalStream(sp.value)
+        t0, _ = g.time()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        g.advance_resident(args.c3_steps)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        t1, dt1 = g.time()
+        ms, days = reduce_over_ranks(ms, (t1 - t0) / DAY, ws)
+        out[prec] = {"ms_per_step": ms / args.c3_steps, "days_per_s": days / (ms / 1000.0), "final_dt_s": dt1}
+        g.cleanup()
+    out["ms_per_step_fp64_vs_mixed"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
 
 
 def ensemble_bench(args, ws):

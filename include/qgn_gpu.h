@@ -133,6 +133,18 @@ int qgn_leith(qgn_ctx* ctx, double* A8L);
 int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins);
 
 /*
+ * FP64 energetics of the resident state per layer k (no counterpart in the reference), each
+ * weighted by H_k/Htot like ke_layer of qgn_diagnostics; any output may be NULL:
+ *   ke_layer[nz]         0.5*mean(u^2+v^2)
+ *   ape_layer[nz]        -0.5*mean(psi_k (L psi)_k) with L the stretching matrix of
+ *                        [Del+L]psi = q (QGN_Module.f90:100-112); the layers sum to the total
+ *                        available potential energy (>= 0), and KE + APE = -0.5 sum_k
+ *                        H_k/Htot mean(psi_k q_k)
+ *   enstrophy_layer[nz]  0.5*mean(q^2)
+ */
+int qgn_energetics(qgn_ctx* ctx, double* ke_layer, double* ape_layer, double* enstrophy_layer);
+
+/*
  * WriteQP's fields (QGN_Module.f90:348-377) in physical space: q_phys = c2r(q_hat)/(nx*ny)
  * and psi_phys = c2r(psi_hat)/(nx*ny) as real(dp)(nx,ny,nz) column-major.  q_hat is a host
  * spectral array, or NULL for the resident state.  Either output pointer may be NULL.

@@ -283,6 +283,42 @@ class QGNOracle:
         v = self.s2g_scaled((1j * self.kx)[None] * psi)
         return 0.5 * np.mean(u ** 2 + v ** 2, axis=(1, 2)) * self.H / p.Htot
 
+    def layer_ape(self, q_hat):
+        """Layer share of the available potential energy, -0.5*mean(psi_k (L psi)_k)*H_k/Htot,
+        with the stretching matrix L of QGN_Module.f90:100-112 applied to the physical psi.
+        The layers sum to sum_i S_i/(Htot (H_i+H_{i+1})) mean((psi_{i+1}-psi_i)^2) >= 0."""
+        p = self.p
+        psi = self.s2g_scaled(self.get_psi(q_hat))
+        Lpsi = np.einsum("kj,jyx->kyx", self.L, psi)
+        return -0.5 * np.mean(psi * Lpsi, axis=(1, 2)) * self.H / p.Htot
+
+    def layer_enstrophy(self, q_hat):
+        """Layer enstrophy 0.5*mean(q^2)*H_k/Htot from the physical PV."""
+        p = self.p
+        q = self.s2g_scaled(q_hat)
+        return 0.5 * np.mean(q ** 2, axis=(1, 2)) * self.H / p.Htot
+
+    def ke_spectrum(self, q_hat, nbins):
+        """Isotropic KE spectrum per layer: shell round(sqrt(i^2 + j^2)) (integer wavenumber
+        indices) of 0.5*k^2|psi_hat|^2/(nx ny)^2 * H_k/Htot over the full FFT plane of the
+        physical psi, so that sum over shells (nbins large enough) equals layer_ke."""
+        p = self.p
+        psi = self.s2g_scaled(self.get_psi(q_hat))
+        full = np.fft.fft2(psi, axes=(-2, -1))
+        i = np.fft.fftfreq(p.nx, d=1.0 / p.nx)
+        j = np.fft.fftfreq(p.ny, d=1.0 / p.ny)
+        kx = (2.0 * math.pi / p.Lx) * i
+        ky = (2.0 * math.pi / p.Ly) * j
+        k2 = kx[None, :] ** 2 + ky[:, None] ** 2
+        shell = np.floor(np.sqrt(i[None, :] ** 2 + j[:, None] ** 2) + 0.5).astype(np.int64)
+        N = float(p.nx * p.ny)
+        out = np.zeros((p.nz, nbins))
+        ok = shell < nbins
+        for k in range(p.nz):
+            dens = 0.5 * k2 * np.abs(full[k]) ** 2 / N / N * self.H[k] / p.Htot
+            out[k] = np.bincount(shell[ok], weights=dens[ok], minlength=nbins)[:nbins]
+        return out
+
     # -- WriteQPmodal (QGN_Module.f90:381-440) -----------------------------------
     def write_qp_modal(self, q_hat):
         """The three physical fields WriteQPmodal writes: q_mode, p_mode, J_mode, each (nz, ny, nx).

@@ -65,6 +65,7 @@ SIGNATURES = {
     "qgn_rhs": (C.c_int, [_ctxp, _dp, _dp]),
     "qgn_psi": (C.c_int, [_ctxp, _dp, _dp]),
     "qgn_leith": (C.c_int, [_ctxp, _dp]),
+    "qgn_energetics": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_diagnostics": (C.c_int, [_ctxp, _dp, _dp, C.c_int]),
     "qgn_physical": (C.c_int, [_ctxp, _dp, _dp, _dp]),
     "qgn_set_state_physical": (C.c_int, [_ctxp, _dp, C.c_double, C.c_double]),

@@ -907,6 +907,26 @@ int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins)
     return QGN_OK;
 }
 
+int qgn_energetics(qgn_ctx* ctx, double* ke_layer, double* ape_layer, double* enstrophy_layer) {
+    if (!ctx) return QGN_ERR_ARG;
+    ProfScope ps_(ctx);
+    if (!ke_layer && !ape_layer && !enstrophy_layer) return set_err(ctx, QGN_ERR_ARG, "all outputs NULL");
+    CK(cudaSetDevice(ctx->device));
+    const Geom& g = ctx->g;
+    Buffers& b = ctx->b;
+    if (b.diag) { cudaFree(b.diag); b.diag = nullptr; }
+    CK(dalloc(&b.diag, (size_t)3 * g.nz));
+    CK(launch_modal(g, b, b.q, b.psi, ctx->stream));
+    CK(launch_energetics(g, b, b.q, b.psi, b.diag, ctx->stream));
+    double* outs[3] = {ke_layer, ape_layer, enstrophy_layer};
+    for (int c = 0; c < 3; ++c)
+        if (outs[c])
+            CK(cudaMemcpyAsync(outs[c], b.diag + (size_t)c * g.nz, sizeof(double) * g.nz, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return QGN_OK;
+}
+
 int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_phys) {
     if (!ctx) return QGN_ERR_ARG;
     ProfScope ps_(ctx);

@@ -288,6 +288,9 @@ cudaError_t launch_zero_scalar_max(DevScalars* sc, cudaStream_t s);
 cudaError_t launch_advance_time(DevScalars* sc, cudaStream_t s);
 cudaError_t launch_set_time(DevScalars* sc, double t, double dt, cudaStream_t s);
 cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const double* Hw, double* ke, cudaStream_t s);
+// per-layer kinetic energy, available potential energy and enstrophy of (q, psi): out[3*nz]
+cudaError_t launch_energetics(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double* out,
+                              cudaStream_t s);
 cudaError_t launch_ke_spectrum(const Geom& g, const double2* psi, const double* Hw, int nbins, double* spec,
                                cudaStream_t s);
 

@@ -56,8 +56,19 @@ __host__ __device__ constexpr int fft_tp() { return (TV == 0 && (N == 512 || N =
 // single-field launches, 16 otherwise.  Half the registers per thread (64, two 512-thread CTAs
 // per SM) doubles the resident warps of these latency-bound kernels at the price of a fourth
 // radix pass at 1024 points: on B200 the 512^2 step ran 11 % and the 1024^2 step 1 % faster.
+// QGN_Y_TP64 (build-time tuning knob, default 8) overrides the FP64 value.
+#ifndef QGN_Y_TP64
+#define QGN_Y_TP64 8
+#endif
 template <class CT, int N, int TV>
-__host__ __device__ constexpr int fft_tp_y() { return (TV == 0 && sizeof(CT) == 16 && N >= 512) ? 8 : 16; }
+__host__ __device__ constexpr int fft_tp_y() { return (TV == 0 && sizeof(CT) == 16 && N >= 512) ? QGN_Y_TP64 : 16; }
+// Row pairs per CTA of the single-field x pass with one warp per transform (a build-time tuning
+// knob).  One row pair (three warps, 96 threads, four CTAs per SM at 168 registers) couples only
+// the three warps of a pair at the barrier between the inverse and forward transforms: the
+// FP64 1024^2 x 8 x pass ran 7 % faster on B200 than with two row pairs per CTA.
+#ifndef QGN_X_ROWPAIRS
+#define QGN_X_ROWPAIRS 1
+#endif
 
 template <int NY, class CT = double2, int TV = 0>
 struct YInvCfg {
@@ -79,7 +90,7 @@ template <int NX, bool DRAG, class CT = double2, int TV = 0>
 struct XCfg {
     static constexpr int TP = fft_tp<CT, NX, TV>();
     static constexpr int G = FFTShape<NX, TP>::G;
-    static constexpr int RP = cmax(1, (TV == 0 ? 64 : TV) / G);   // row pairs per CTA
+    static constexpr int RP = (TV == 0 && G == 32) ? QGN_X_ROWPAIRS : cmax(1, (TV == 0 ? 64 : TV) / G);   // row pairs per CTA
     static constexpr int SP = DRAG ? 4 : 3;             // slots per row pair
     static constexpr int THREADS = SP * RP * G;
     static constexpr int TS = slot_stride(NX, 2, (int)sizeof(CT), TP);

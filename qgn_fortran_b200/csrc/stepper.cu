@@ -513,6 +513,67 @@ __global__ void k_ke_final(Geom g, const double* __restrict__ partial, int nbloc
     if ((threadIdx.x & 31) == 0) ke[l] = 0.5 * ((s / N) / N) * Hw[l];
 }
 
+// Energetics of the state, per layer (block partials, one (block, layer) per CTA): Parseval sums
+// over the full plane of 0: k^2 |psi|^2 (kinetic energy), 1: -Re(conj(psi) (q + k^2 psi)) (the
+// available potential energy: q_hat + k^2 psi_hat is the stretching term (L psi)^ of
+// [Del + L] psi = q, QGN_Module.f90:100-112), 2: |q|^2 (enstrophy).  The kx = 0 column uses the
+// Hermitian projections of both fields, as the reference's c2r does.
+__global__ void __launch_bounds__(256) k_energetics(Geom g, const double2* __restrict__ q,
+                                                    const double2* __restrict__ psi, double* __restrict__ partial) {
+    QGN_PDL_ENTRY();
+    __shared__ double red[3][8];
+    const size_t P = (size_t)g.nkx * g.nky;
+    const int l = blockIdx.y;
+    double a[3] = {0.0, 0.0, 0.0};
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (size_t)gridDim.x * blockDim.x) {
+        int kx, m;
+        double k2;
+        point_k(g, p, kx, m, k2);
+        double2 hp = psi[(size_t)l * P + p], hq = q[(size_t)l * P + p];
+        double w = 2.0;
+        if (kx == 0) {
+            const int j = g.jfull(m);
+            const int jp = (g.ny - j) % g.ny;
+            const bool pk = (jp < g.kylo) || (jp >= g.kylo + g.kyshift);
+            double2 fp = make_double2(0.0, 0.0), fq = make_double2(0.0, 0.0);
+            if (pk) {
+                const size_t pp = (size_t)l * P + (jp < g.kylo ? jp : jp - g.kyshift);
+                fp = psi[pp];
+                fq = q[pp];
+            }
+            hp = make_double2(0.5 * (hp.x + fp.x), 0.5 * (hp.y - fp.y));
+            hq = make_double2(0.5 * (hq.x + fq.x), 0.5 * (hq.y - fq.y));
+            w = pk ? 1.0 : 2.0;
+        }
+        a[0] += w * k2 * (hp.x * hp.x + hp.y * hp.y);
+        a[1] -= w * (hp.x * (hq.x + k2 * hp.x) + hp.y * (hq.y + k2 * hp.y));
+        a[2] += w * (hq.x * hq.x + hq.y * hq.y);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[c] += __shfl_xor_sync(0xffffffffu, a[c], o);
+        if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = a[c];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double t = 0.0;
+        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) t += red[threadIdx.x][w8];
+        partial[((size_t)threadIdx.x * g.nz + l) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// out[c*nz + l] = 0.5 * S_c(l)/(nx ny)^2 * H_l/Htot, one warp per (quantity, layer), fixed order
+__global__ void k_energetics_final(Geom g, const double* __restrict__ partial, int nblocks,
+                                   const double* __restrict__ Hw, double* __restrict__ out) {
+    QGN_PDL_ENTRY();
+    const int cl = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (cl >= 3 * g.nz) return;
+    const double s = layer_sum(partial, cl, nblocks);
+    const double N = (double)g.nx * (double)g.ny;
+    if ((threadIdx.x & 31) == 0) out[cl] = 0.5 * ((s / N) / N) * Hw[cl % g.nz];
+}
+
 // isotropic KE spectrum per layer in integer shells round(sqrt(i^2 + jj^2))
 __global__ void k_ke_spectrum(Geom g, const double2* __restrict__ psi, const double* __restrict__ Hw, int nbins,
                               double* __restrict__ spec) {
@@ -1112,6 +1173,16 @@ cudaError_t launch_ke(const Geom& g, const Buffers& b, const double2* psi, const
     QGN_LAUNCH(KID_PARSEVAL, 16.0 * (double)g.csize(), st,
                ::qgn::launch(k_parseval<1>, dim3(nb, g.nz), 256, 0, st, g, psi, b.red));
     QGN_LAUNCH(KID_SCALAR, 0.0, st, ::qgn::launch(k_ke_final, (g.nz + 7) / 8, 256, 0, st, g, b.red, nb, Hw, ke));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energetics(const Geom& g, const Buffers& b, const double2* q, const double2* psi, double* out,
+                              cudaStream_t st) {
+    const int nb = parseval_blocks(g);
+    QGN_LAUNCH(KID_PARSEVAL, 32.0 * (double)g.csize(), st,
+               ::qgn::launch(k_energetics, dim3(nb, g.nz), 256, 0, st, g, q, psi, b.red));
+    QGN_LAUNCH(KID_SCALAR, 0.0, st,
+               ::qgn::launch(k_energetics_final, (3 * g.nz + 7) / 8, 256, 0, st, g, b.red, nb, b.Hw, out));
     return cudaGetLastError();
 }
 

@@ -178,6 +178,35 @@ class Workload:
     qp: np.ndarray
     scheme: str
     dt0: float
+    t0: float = 0.0
+    ic: str = "seeded"
+
+
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+def spinup_path(name: str) -> str:
+    return os.path.join(DATA, f"{name}_spinup.npz")
+
+
+def spunup_pv(name: str, path: str | None = None):
+    """The spun-up state of a named workload (written by ``qgn_fortran_b200.spinup``) as a physical
+    PV field C-order [nz][ny][nx], with its metadata (simulated time t, last dt, TOL, ...).  The
+    fixture holds the modes DeAlias keeps at bfloat16 precision; the field is their c2r/(nx ny)
+    (MKL_DFTI_Setup.f90 backward transform, QGN_Module.f90:348-377 scaling)."""
+    import json
+    d = np.load(path or spinup_path(name))
+    meta = json.loads(str(d["meta"]))
+    nx, ny, nz = meta["nx"], meta["ny"], meta["nz"]
+
+    def f32(bits):
+        return (np.asarray(bits, dtype=np.uint32) << 16).view(np.float32).astype(np.float64)
+
+    full = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128)
+    rows = np.r_[0:ny // 3, 2 * (ny // 3) + 1:ny]
+    full[:, rows, :nx // 3] = f32(d["re"]) + 1j * f32(d["im"])
+    full[:, 0, 0] = 0.0
+    return np.fft.irfft2(full, s=(ny, nx), axes=(-2, -1)), meta
 
 
 def ensemble_members(n=64, seed0=1000, sizes=(128, 256, 512), layers=(2, 4, 8), Lx=2.0e6, with_ic=True):
@@ -207,7 +236,7 @@ def ensemble_members(n=64, seed0=1000, sizes=(128, 256, 512), layers=(2, 4, 8), 
     return out
 
 
-def workload(name: str, nx=None, nz=None, seed=None, with_ic=True) -> Workload:
+def workload(name: str, nx=None, nz=None, seed=None, with_ic=True, ic: str = "seeded") -> Workload:
     """Named synthetic workloads.
 
     * ``phillips256``: 2-layer Phillips problem, 256^2, L=1000 km, H=[1000,3000] m,
@@ -220,7 +249,16 @@ def workload(name: str, nx=None, nz=None, seed=None, with_ic=True) -> Workload:
       C_d=0.  IC peak wavenumber 16, rms 1e-6, seed 2.
     * ``strat2048x16``: the same stratification on 2048^2 x 16 layers (seed 3).
     ``nx``/``nz`` override the grid for reduced-size parity cases.
+    ``ic="spinup"`` starts from the committed spun-up state of the full-size workload instead
+    (``spunup_pv``): t0 and dt0 are the spin-up's final t and dt, TOL stays the configured one.
     """
+    if ic == "spinup":
+        if nx or nz or seed is not None:
+            raise ValueError("the spun-up state exists for the full-size workload only")
+        w = workload(name, with_ic=False)
+        qp, meta = spunup_pv(name)
+        w.params["TOL"] = meta["TOL"]
+        return Workload(name, w.params, w.H, w.S, w.U, qp, w.scheme, meta["dt"], meta["t"], "spinup")
     if name == "phillips256":
         n = nx or 256
         Lx = 1.0e6

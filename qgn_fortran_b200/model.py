@@ -256,6 +256,12 @@ class QGNModule:
                     "qgn_diagnostics")
         return ke, spec
 
+    def energetics(self):
+        """Per-layer (KE, APE, enstrophy) of the resident state, each weighted by H_k/Htot."""
+        out = [np.empty(self.nz) for _ in range(3)]
+        self._check(self.lib.qgn_energetics(self.ctx, *(dptr(a) for a in out)), "qgn_energetics")
+        return tuple(out)
+
     def rejects(self):
         n = C.c_longlong()
         self._check(self.lib.qgn_rejects(self.ctx, C.byref(n)), "qgn_rejects")

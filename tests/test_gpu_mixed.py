@@ -87,3 +87,16 @@ def test_mixed_rejected_for_other_schemes(cuda_ok):
     with pytest.raises(QGNError) as ei:
         QGNModule(w.params, w.H, w.S, w.U, scheme="rk4", precision="mixed")
     assert ei.value.code == QGN_ERR_CONFIG
+
+
+def test_mixed_error_table_strat2048x16(cuda_ok):
+    """The 2048^2 x 16 workload in the mixed mode against FP64 (both on the GPU, FP64 checked
+    against the oracle in tests/test_gpu_ladder.py): one RHS, 100 fixed-dt ARK43_QGLeith steps
+    (dt = 3600 s), layer KE and the isotropic KE spectrum of the final states."""
+    from qgn_fortran_b200.mixed_error import error_table
+    t = error_table("strat2048x16", steps=100, dt=3600.0)
+    print("strat2048x16 mixed vs FP64:", t)
+    assert t["rhs"] <= 2e-6
+    assert t["fixed_steps"]["state"] <= 1e-5
+    assert t["fixed_steps"]["ke_layer"] <= 1e-6
+    assert t["fixed_steps"]["ke_spectrum"] <= 1e-5

@@ -260,3 +260,25 @@ def test_step_output_modes(cuda_ok):
     assert np.all(qa[band] == marker)          # kept mode: the band is not written
     assert np.all(qb[band] == 0)               # full mode: zeros, as after DeAlias
     assert np.array_equal(qa[~band], qb[~band])
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(64, 128, 3), (256, 256, 8), (128, 64, 2)])
+def test_energetics_and_spectrum(cuda_ok, nx, ny, nz):
+    """Layer KE, APE, enstrophy and the isotropic KE spectrum of the resident state against the
+    oracle's physical-space forms (per-layer 1e-12; spectrum per-layer relative L2 1e-12)."""
+    H, S, U = exponential_stratification(nz)
+    params = strat_params(nx, ny, nz)
+    m, g = pair(params, H, S, U)
+    q = m.initialize_spec(seeded_random_pv(nx, ny, nz, 6.0, 1.0e-6, seed=3 * nx + nz))
+    g.set_state(q, 0.0, 100.0)
+    ke, ape, Z = g.energetics()
+    assert np.allclose(ke, m.layer_ke(q), rtol=RHS_TOL, atol=0)
+    want_ape = m.layer_ape(q)
+    assert np.allclose(ape, want_ape, rtol=0, atol=RHS_TOL * np.abs(want_ape).max())
+    assert np.allclose(Z, m.layer_enstrophy(q), rtol=RHS_TOL, atol=0)
+    nbins = max(nx, ny) // 2
+    ke2, spec = g.diagnostics(nbins)
+    assert np.allclose(ke2, ke, rtol=1e-13, atol=0)     # two reductions in different orders
+    want = m.ke_spectrum(q, nbins)
+    num = np.sqrt(np.sum((spec - want) ** 2, axis=1))
+    assert np.all(num <= RHS_TOL * np.sqrt(np.sum(want ** 2, axis=1)))

@@ -253,6 +253,28 @@ def test_leith_parseval_matches_physical():
     assert LEITH_13 == 1.2999999523162842
 
 
+@pytest.mark.parametrize("nx,ny,nz", [(64, 64, 3), (32, 64, 5), (64, 32, 2)])
+def test_energetics_identities(nx, ny, nz):
+    """KE from the spectrum shells, KE + APE = -0.5 sum_k w_k mean(psi q), APE in its interface
+    form sum_i S_i/(Htot (H_i + H_i+1)) mean((psi_i+1 - psi_i)^2) (from QGN_Module.f90:100-112)."""
+    m = small_model(nx=nx, ny=ny, nz=nz)
+    q = m.initialize_spec(seeded_random_pv(nx, ny, nz, 6.0, 1e-6, seed=nx + nz))
+    ke = m.layer_ke(q)
+    spec = m.ke_spectrum(q, nbins=max(nx, ny))
+    assert np.allclose(spec.sum(axis=1), ke, rtol=1e-12)
+    ape = m.layer_ape(q)
+    psi = m.s2g_scaled(m.get_psi(q))
+    qp = m.s2g_scaled(q)
+    w = m.H / m.p.Htot
+    assert np.sum(ke) + np.sum(ape) == pytest.approx(-0.5 * np.sum(w * np.mean(psi * qp, axis=(1, 2))), rel=1e-12)
+    iface = sum(m.S[i + 1] / (m.p.Htot * (m.H[i] + m.H[i + 1])) * np.mean((psi[i + 1] - psi[i]) ** 2)
+                for i in range(nz - 1))
+    assert np.sum(ape) == pytest.approx(iface, rel=1e-12)
+    assert np.sum(ape) > 0
+    Z = m.layer_enstrophy(q)
+    assert np.allclose(Z, 0.5 * np.mean(qp ** 2, axis=(1, 2)) * w, rtol=1e-14)
+
+
 def test_write_qp_modal_identities():
     """WriteQPmodal: the modes back-project onto q, psi and the full Jacobian; a single
     Fourier mode in one vertical mode gives that mode alone, psi_mode = q_mode/(-k^2+EVals),
