@@ -2,10 +2,12 @@
 
 Workload (default ``strat1024x8``): 8 geometric layers on a 1024^2 doubly periodic grid,
 L = 2000 km, N^2 = (5e-3)^2 exp(z/1000 m), U = 0.1 exp(z/1000 m), ARK43_QGLeith with the
-PI.3.4 controller and TOL = 1e-6 x max|q_IC|, FP64, from a seeded random PV field (seed 2,
-peak wavenumber 16, rms 1e-6 s^-1).  A step is one accepted TimeStep (6 RHS evaluations
-plus any rejected attempts).  Data are synthetic; the spin-up of the named configuration
-(10 model years) is not run -- timing starts from the seeded state after the warm-up steps.
+PI.3.4 controller and TOL = 1e-6 x max|q_IC| of the seeded random PV field (seed 2, peak
+wavenumber 16, rms 1e-6 s^-1), FP64.  A step is one accepted TimeStep (6 RHS evaluations plus
+any rejected attempts).  Data are synthetic.  The window starts from the configuration's
+10-year spun-up state (qgn_fortran_b200/data/strat1024x8_spinup.npz, made on the GPU by
+qgn_fortran_b200.spinup from the seeded IC; kept modes at bfloat16 precision), the regime the
+configuration's statistics year runs in; both arms start there, W untimed steps, K timed.
 
 ``value``: device-resident stepping (qgn_advance_resident, graph-launched steps), CUDA
 events on the library's stream.  ``e2e``: the drop-in path TimeStep (QGNModule.time_step ->
@@ -45,6 +47,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="strat1024x8")
+    ap.add_argument("--ic", choices=["spinup", "seeded"], default=None,
+                    help="window start: the committed 10-year spun-up state (default when the workload "
+                         "has one) or the seeded initial condition")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -154,6 +159,23 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
+def bench_workload(args):
+    """The named workload, starting from its spun-up state when one is committed (or --ic)."""
+    from qgn_fortran_b200.inputs import spinup_path, workload
+    ic = args.ic or ("spinup" if os.path.exists(spinup_path(args.workload)) else "seeded")
+    return workload(args.workload, ic=ic)
+
+
+def bench_config(args, w, ws):
+    """The config keys both arms print (same workload, grid, scheme and step window)."""
+    start = ("the committed state after 10 model years of spin-up (qgn_fortran_b200.spinup; t0 = "
+             f"{w.t0 / 86400.0 / 365.0:.2f} years, dt0 = {w.dt0:.0f} s)" if w.ic == "spinup" else "the seeded IC")
+    return {"workload": args.workload, "grid": f"{w.params['nx']}x{w.params['ny']}x{w.params['nz']}",
+            "scheme": w.scheme, "parallelism": "replicas" if ws > 1 else "single",
+            "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
+            "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from {start}"}
+
+
 def run_oracle(w, warmup, steps):
     """Time the FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c) on the host cores."""
     from oracle.qgn_oracle import Params
@@ -161,7 +183,7 @@ def run_oracle(w, warmup, steps):
 
     c = RefC(Params(**w.params), w.H, w.S, w.U, scheme=w.scheme)
     q = c.initialize_spec(w.qp)
-    t, dt = 0.0, w.dt0
+    t, dt = w.t0, w.dt0
     for _ in range(warmup):
         t, dt = c.step(q, t, dt)
     t0 = t
@@ -174,22 +196,21 @@ def run_oracle(w, warmup, steps):
 
 def reference_arm(args):
     """The reference algorithm on the host cores over the same step window as our arm: from the
-    seeded IC, W untimed steps, then K timed steps, so both arms simulate the same days."""
+    same start state, W untimed steps, then K timed steps, so both arms simulate the same days."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    from qgn_fortran_b200.inputs import workload
-    w = workload(args.workload)
+    w = bench_workload(args)
     warm = max(0, args.warmup)
     steps = max(1, args.steps)
     val, sec, n, nthr = run_oracle(w, warm, steps)
-    sample = (f"steps {warm + 1}..{warm + n} of {w.scheme} on {args.workload} from the seeded IC (the window our "
-              f"arm times), FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c), {nthr} threads, "
-              f"{sec:.1f} s timed")
+    cfg = bench_config(args, w, ws)
+    sample = (f"{cfg['window']} of {w.scheme} on {args.workload} (the window our arm times), FP64 C/OpenMP "
+              f"restatement of the reference (oracle/qgn_ref.c), {nthr} threads, {sec:.1f} s timed")
     line = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": n,
             "warmup": warm, "ms_per_step": 1000.0 * sec / n, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "grid": "1024x1024x8", "scheme": w.scheme},
+            "config": cfg,
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthr, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -208,9 +229,9 @@ def ours_arm(args):
     from qgn_fortran_b200 import QGNModule, _lib
     from qgn_fortran_b200.inputs import workload
 
-    w = workload(args.workload)
+    w = bench_workload(args)
     g = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme)
-    q = g.initialize(w.qp, 0.0, w.dt0)
+    q = g.initialize(w.qp, w.t0, w.dt0)
     sptr = _lib.C.c_void_p()
     g.lib.qgn_stream(g.ctx, _lib.C.byref(sptr))
     stream = torch.cuda.ExternalStream(sptr.value)
@@ -270,13 +291,13 @@ def ours_arm(args):
     e2e = None
     if not args.no_e2e:
         gE = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme)
-        q0 = gE.initialize(w.qp, 0.0, w.dt0)
+        q0 = gE.initialize(w.qp, w.t0, w.dt0)
         qh = torch.empty(q0.shape, dtype=torch.complex128, pin_memory=True).numpy()
         qh[...] = q0
         sE = _lib.C.c_void_p()
         gE.lib.qgn_stream(gE.ctx, _lib.C.byref(sE))
         estream = torch.cuda.ExternalStream(sE.value)
-        t, dt = 0.0, w.dt0
+        t, dt = w.t0, w.dt0
         for _ in range(args.warmup):
             t, dt = gE.time_step(qh, t, dt)
         te0 = t
@@ -297,14 +318,14 @@ def ours_arm(args):
         kept = 16 * (w.params["nx"] // 3) * (w.params["ny"] - w.params["ny"] // 3 - 1) * w.params["nz"]
         e2e = {"value": edays / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": kept,
                "d2h_bytes_per_step": kept, "ms_per_step": ems / args.steps,
-               "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the IC"}
+               "window": bench_config(args, w, ws)["window"]}
         gE.cleanup()
 
     # ---- the same workload in the mixed mode (FP32 transforms/RHS/stages, FP64 state and control)
     mixed = None
     if not args.no_mixed:
         gm = QGNModule(w.params, w.H, w.S, w.U, scheme=w.scheme, precision="mixed")
-        gm.initialize(w.qp, 0.0, w.dt0)
+        gm.initialize(w.qp, w.t0, w.dt0)
         if args.warmup > 0:
             gm.advance_resident(args.warmup)
         smp = _lib.C.c_void_p()
@@ -370,7 +391,7 @@ def ours_arm(args):
         _, sec, n, nthr = run_oracle(w, 1, args.cpu_sample_steps)
         cpu_val = (days_all / args.steps) / (sec / n)
         cpu = {"value": cpu_val, "unit": UNIT, "cores": nthr, "kind": "port", "ms_per_step": 1000.0 * sec / n,
-               "sample": f"{n} {w.scheme} steps of {args.workload} after 1 warm-up step from the seeded IC, "
+               "sample": f"{n} {w.scheme} steps of {args.workload} after 1 warm-up step from the window's start, "
                          f"FP64 C/OpenMP restatement of the reference (oracle/qgn_ref.c), {nthr} threads, "
                          f"{sec:.1f} s; days/s = mean dt of the timed window / CPU s per step"}
 
@@ -378,11 +399,8 @@ def ours_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "grid": f"{w.params['nx']}x{w.params['ny']}x{w.params['nz']}",
-                       "scheme": w.scheme, "parallelism": "replicas" if ws > 1 else "single",
-                       "l2": "working set ~0.7 GB > 126 MB L2 (no flush needed)",
-                       "sim_days": days, "final_dt_s": dt1, "rejects": g.rejects(),
-                       "window": f"steps {args.warmup + 1}..{args.warmup + args.steps} from the seeded IC"},
+            "config": bench_config(args, w, ws),
+            "window_stats": {"sim_days": days, "final_dt_s": dt1, "rejects": g.rejects()},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "mixed_2048x16": c3, "ensemble": ensemble, "closure": closure, "gpu_launches": launches,
             "clocks": clk, "kernels": kernels}
     print(json.dumps(line), flush=True)

@@ -32,6 +32,16 @@ int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
  */
 int qgn_cnn_debug_set_counter(qgn_cnn* net, int tile, unsigned int value);
 
+/*
+ * Bounds-checked build (libqgn_b200_check.so, every source compiled with -DQGN_CHECK): the
+ * right-hand-side transforms and GetPsi test each global index against the length of the
+ * array it addresses and skip, and count, an access out of range instead of making it.
+ * failures receives the count of this context since creation (its kernels are waited for
+ * first), or -1 from the normal build, which compiles no checks.  It stands in for a memory
+ * checker: the checks fault nothing and leave the context usable.
+ */
+int qgn_check_failures(qgn_ctx* ctx, long long* failures);
+
 #ifdef __cplusplus
 }
 #endif

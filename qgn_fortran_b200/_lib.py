@@ -10,6 +10,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqgn_b200.so")
+# the bounds-checked debug build (qgn_fortran_b200.build(check=True)), loaded only by its test
+CHECK_LIB_PATH = os.path.join(HERE, "libqgn_b200_check.so")
 
 QGN_OK = 0
 QGN_ERR_CONFIG = 1
@@ -109,6 +111,7 @@ SIGNATURES = {
     "qgn_kernel_name": (C.c_char_p, [C.c_int]),
     "qgn_stream": (C.c_int, [_ctxp, C.POINTER(C.c_void_p)]),
     "qgn_debug_read": (C.c_int, [_ctxp, C.c_int, _dp, C.c_longlong]),
+    "qgn_check_failures": (C.c_int, [_ctxp, C.POINTER(C.c_longlong)]),
     "qgn_rhs_static": (C.c_int, [C.POINTER(qgn_params), _dp, _dp, _dp, _dp, _dp, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
     "qgn_last_error": (C.c_char_p, [_ctxp]),

@@ -41,18 +41,26 @@ def _headers():
     return hs
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(OBJDIR, exist_ok=True)
+# the bounds-checked debug build (-DQGN_CHECK): same sources, its own objects and library
+CHECK_LIB = os.path.join(HERE, "libqgn_b200_check.so")
+CHECK_OBJDIR = os.path.join(HERE, "_build_check")
+
+
+def build(force: bool = False, verbose: bool = False, check: bool = False) -> str:
+    """Build libqgn_b200.so, or with check=True the bounds-checked libqgn_b200_check.so."""
+    objdir, lib = (CHECK_OBJDIR, CHECK_LIB) if check else (OBJDIR, LIB)
+    extra = ["-DQGN_CHECK"] if check else []
+    os.makedirs(objdir, exist_ok=True)
     cc = nvcc()
     headers = _headers()
     jobs = []
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        o = os.path.join(objdir, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            jobs.append([cc, *ARCH, *NVCC_FLAGS, "-c", s, "-o", o])
+            jobs.append([cc, *ARCH, *NVCC_FLAGS, *extra, "-c", s, "-o", o])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -63,10 +71,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
-    if force or jobs or _stale(LIB, objs):
-        run([cc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
-    return LIB
+    if force or jobs or _stale(lib, objs):
+        run([cc, *ARCH, "-shared", "-o", lib, *objs, "-lcudart"])
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, check="--check" in sys.argv))

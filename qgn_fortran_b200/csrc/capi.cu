@@ -38,7 +38,10 @@ namespace {
 // Makes the context's profiler the current one for the duration of an API call.
 struct ProfScope {
     Prof* prev;
-    explicit ProfScope(qgn_ctx* ctx) : prev(current_prof()) { current_prof() = ctx ? &ctx->prof : nullptr; }
+    NvtxRange range;
+    ProfScope(qgn_ctx* ctx, const char* api) : prev(current_prof()), range(api) {
+        current_prof() = ctx ? &ctx->prof : nullptr;
+    }
     ~ProfScope() { current_prof() = prev; }
 };
 
@@ -196,7 +199,10 @@ bool mixed(const qgn_ctx* ctx) { return ctx->precision == QGN_PREC_MIXED; }
 template <class T>
 float2* f32(T* p) { return reinterpret_cast<float2*>(p); }
 
+static const char* const kStageRange[6] = {"stage 0", "stage 1", "stage 2", "stage 3", "stage 4", "stage 5"};
+
 int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop) {
+    QGN_NVTX("ARK attempt");
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
@@ -212,6 +218,7 @@ int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop
             else CK(launch_rhs_yfwd(g, b, b.Qs[5], b.psi, b.N[5], false, st, extra));
         }
     } else for (int s = 1; s < 6; ++s) {
+        QGN_NVTX(kStageRange[s]);
         if (mixed(ctx)) {
             CK(launch_ark_stage_mixed(g, b, s, st));
             CK(launch_rhs32(g, b, f32(b.Qs[s]), f32(b.psi), f32(b.N[s]), drag_on(ctx), st));
@@ -236,6 +243,7 @@ int ark_attempt(qgn_ctx* ctx, bool leith, const cudaGraphConditionalHandle* loop
 }
 
 int ark_prologue(qgn_ctx* ctx, bool leith) {
+    QGN_NVTX("ARK prologue");
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
     cudaStream_t st = ctx->stream;
@@ -677,6 +685,14 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     AL(b.red, (size_t)512 * kMaxNZ);
     AL(b.Hw, (size_t)kMaxNZ);
     AL(b.lc, 1); AL(b.mc, 1); AL(b.sc, 1);
+#ifdef QGN_CHECK
+    AL(ctx->chk, 1);
+    if (rc == QGN_OK) {
+        cudaError_t e = cudaMemset(ctx->chk, 0, sizeof(unsigned long long));
+        if (e != cudaSuccess) fail("cudaMemset(chk)", e);
+        g.chk = ctx->chk;
+    }
+#endif
 #undef AL
     if (rc == QGN_OK) {
         cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
@@ -766,7 +782,7 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
 
 int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     ++ctx->state_version;
     if (!q_hat) return set_err(ctx, QGN_ERR_ARG, "q_hat is NULL");
     CK(cudaSetDevice(ctx->device));
@@ -779,7 +795,7 @@ int qgn_set_state(qgn_ctx* ctx, const double* q_hat, double t, double dt) {
 
 int qgn_get_time(qgn_ctx* ctx, double* t, double* dt) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     DevScalars s;
     RET(read_scalars(ctx, &s));
     if (t) *t = s.t;
@@ -789,7 +805,7 @@ int qgn_get_time(qgn_ctx* ctx, double* t, double* dt) {
 
 int qgn_get_state(qgn_ctx* ctx, double* q_hat, double* t, double* dt) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     CK(cudaSetDevice(ctx->device));
     if (q_hat) RET(download_full(ctx, ctx->b.q, q_hat));
     return qgn_get_time(ctx, t, dt);
@@ -797,7 +813,7 @@ int qgn_get_state(qgn_ctx* ctx, double* q_hat, double* t, double* dt) {
 
 int qgn_advance_resident(qgn_ctx* ctx, int nsteps) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     ++ctx->state_version;
     if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
     CK(cudaSetDevice(ctx->device));
@@ -809,7 +825,7 @@ int qgn_advance_resident(qgn_ctx* ctx, int nsteps) {
 
 int qgn_advance(qgn_ctx* ctx, double* q_hat, double* t, double* dt, int nsteps) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     ++ctx->state_version;
     if (!q_hat || !t || !dt) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     if (nsteps < 0) return set_err(ctx, QGN_ERR_ARG, "nsteps < 0");
@@ -838,7 +854,7 @@ int qgn_set_output(qgn_ctx* ctx, int mode) {
 
 int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     ++ctx->state_version;
     if (!q_hat || !rhs) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     CK(cudaSetDevice(ctx->device));
@@ -862,7 +878,7 @@ int qgn_rhs(qgn_ctx* ctx, const double* q_hat, double* rhs) {
 
 int qgn_psi(qgn_ctx* ctx, const double* q_hat, double* psi_hat) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     if (!q_hat || !psi_hat) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     CK(cudaSetDevice(ctx->device));
     Buffers& b = ctx->b;
@@ -875,7 +891,7 @@ int qgn_psi(qgn_ctx* ctx, const double* q_hat, double* psi_hat) {
 
 int qgn_leith(qgn_ctx* ctx, double* A8L) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     if (!A8L) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     CK(cudaSetDevice(ctx->device));
     CK(launch_leith(ctx->g, ctx->b, ctx->b.q, leith_c12(ctx->p), ctx->stream));
@@ -887,7 +903,7 @@ int qgn_leith(qgn_ctx* ctx, double* A8L) {
 
 int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     if (!ke_layer) return set_err(ctx, QGN_ERR_ARG, "NULL argument");
     if (spectrum && nbins <= 0) return set_err(ctx, QGN_ERR_ARG, "nbins <= 0");
     CK(cudaSetDevice(ctx->device));
@@ -909,7 +925,7 @@ int qgn_diagnostics(qgn_ctx* ctx, double* ke_layer, double* spectrum, int nbins)
 
 int qgn_energetics(qgn_ctx* ctx, double* ke_layer, double* ape_layer, double* enstrophy_layer) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     if (!ke_layer && !ape_layer && !enstrophy_layer) return set_err(ctx, QGN_ERR_ARG, "all outputs NULL");
     CK(cudaSetDevice(ctx->device));
     const Geom& g = ctx->g;
@@ -929,7 +945,7 @@ int qgn_energetics(qgn_ctx* ctx, double* ke_layer, double* ape_layer, double* en
 
 int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_phys) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     CK(cudaSetDevice(ctx->device));
     const Geom& g = ctx->g;
     Buffers& b = ctx->b;
@@ -955,7 +971,7 @@ int qgn_physical(qgn_ctx* ctx, const double* q_hat, double* q_phys, double* psi_
 
 int qgn_physical_modal(qgn_ctx* ctx, const double* q_hat, double* q_mode, double* p_mode, double* J_mode) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     if (!q_mode || !p_mode || !J_mode) return set_err(ctx, QGN_ERR_ARG, "NULL output");
     CK(cudaSetDevice(ctx->device));
     const Geom& g = ctx->g;
@@ -986,7 +1002,7 @@ int qgn_physical_modal(qgn_ctx* ctx, const double* q_hat, double* q_mode, double
 
 int qgn_set_state_physical(qgn_ctx* ctx, const double* q_phys, double t, double dt) {
     if (!ctx) return QGN_ERR_ARG;
-    ProfScope ps_(ctx);
+    ProfScope ps_(ctx, __func__);
     ++ctx->state_version;
     if (!q_phys) return set_err(ctx, QGN_ERR_ARG, "q_phys is NULL");
     CK(cudaSetDevice(ctx->device));
@@ -1070,6 +1086,20 @@ int qgn_rejects(qgn_ctx* ctx, long long* count) {
 const char* qgn_last_error(const qgn_ctx* ctx) {
     if (!ctx) return "null context";
     return ctx->last_error.c_str();
+}
+
+int qgn_check_failures(qgn_ctx* ctx, long long* failures) {
+    if (!ctx || !failures) return QGN_ERR_ARG;
+#ifdef QGN_CHECK
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long n = 0;
+    CK(cudaMemcpy(&n, ctx->chk, sizeof(n), cudaMemcpyDeviceToHost));
+    *failures = (long long)n;
+#else
+    *failures = -1;
+#endif
+    return QGN_OK;
 }
 
 int qgn_destroy(qgn_ctx* ctx) {

@@ -273,6 +273,7 @@ const double2* closure_tendency(const qgn_ctx* ctx) { return ctx->closure ? ctx-
 // network, the forward transform of its output, the budget kernel.  It writes only the
 // closure's own buffers and, when the check passes, the layers' A8 in the device scalars.
 int closure_eval(qgn_ctx* ctx, const double2* psi, cudaStream_t st) {
+    QGN_NVTX("closure evaluation");
     Closure* c = ctx->closure;
     const Geom& g = ctx->g;
     const Buffers& b = ctx->b;
@@ -348,6 +349,7 @@ int snap_scratch(qgn_ctx* c, double** out) {
 extern "C" {
 
 int qgn_coarse_grain(qgn_ctx* fine, qgn_ctx* coarse) {
+    QGN_NVTX("qgn_coarse_grain");
     if (!fine || !coarse || fine == coarse) return QGN_ERR_ARG;
     if (!compatible(fine, coarse)) return QGN_ERR_CONFIG;
     if (cudaSetDevice(fine->device) != cudaSuccess) return QGN_ERR_CUDA;
@@ -364,6 +366,7 @@ int qgn_coarse_grain(qgn_ctx* fine, qgn_ctx* coarse) {
 
 int qgn_closure_snapshot(qgn_ctx* fine, qgn_ctx* coarse, const float* in_scale, const float* out_scale, void* x_dev,
                          float* y_dev, int cin_p, int cout_p) {
+    QGN_NVTX("qgn_closure_snapshot");
     if (!fine || !coarse || !in_scale || !out_scale || !x_dev || !y_dev) return QGN_ERR_ARG;
     const int nz = coarse->g.nz;
     if (cin_p < 2 * nz || cin_p % 16 || cout_p < nz || cout_p % 16) return QGN_ERR_CONFIG;

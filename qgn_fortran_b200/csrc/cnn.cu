@@ -1362,6 +1362,7 @@ int qgn_cnn_set_weights(qgn_cnn* net, const float* host) {
 // inference: x = BF16 [batch][H][W][cin_p] (device), y = FP32 [batch][H][W][cout_p] (device).
 // Runs on `stream` (NULL: the network's own stream), ordered after the caller's work there.
 int qgn_cnn_forward(qgn_cnn* net, const void* x, float* y, int batch, void* stream) {
+    QGN_NVTX("qgn_cnn_forward");
     if (!net || !x || !y || batch < 1 || batch > net->max_batch) return QGN_ERR_ARG;
     return qgn::cnn::infer(net, x, y, batch, stream ? static_cast<cudaStream_t>(stream) : net->stream, false);
 }
@@ -1396,6 +1397,7 @@ int qgn_cnn_gradients(qgn_cnn* net, const void* x, const float* y, int batch, fl
 // [n][H][W][cin_p], y_all FP32 [n][H][W][cout_p]; loss (before the update) optional
 int qgn_cnn_train_step(qgn_cnn* net, const void* x_all, const float* y_all, const int* idx, int batch, float lr,
                        double* loss) {
+    QGN_NVTX("qgn_cnn_train_step");
     if (!net || !x_all || !y_all || !idx || batch < 1 || batch > net->max_batch || !(lr > 0)) return QGN_ERR_ARG;
     const int L = net->layers;
     const size_t xs = (size_t)net->H * net->W * net->ci[0] * sizeof(__nv_bfloat16);

@@ -707,6 +707,7 @@ int launch_attempt(qgn_ens* e, const cudaGraphConditionalHandle* loop) {
 }
 
 int attempt(qgn_ens* e, const cudaGraphConditionalHandle* loop) {
+    QGN_NVTX("ensemble attempt");
     return fp32(e) ? launch_attempt<float2>(e, loop) : launch_attempt<double2>(e, loop);
 }
 int fsal(qgn_ens* e) { return fp32(e) ? launch_fsal<float2>(e) : launch_fsal<double2>(e); }
@@ -877,6 +878,7 @@ int qgn_ens_create(qgn_ctx* const* members, int nmembers, int precision, qgn_ens
 }
 
 int qgn_ens_advance(qgn_ens* e, int nsteps) {
+    QGN_NVTX("qgn_ens_advance");
     if (!e) return QGN_ERR_ARG;
     if (nsteps < 0) return ens_err(e, QGN_ERR_ARG, "nsteps < 0");
     EnsProfScope ps_(e);

@@ -7,6 +7,7 @@
 // to the caller (qgn_profile_read) without a profiler attached.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <vector>
 
@@ -111,7 +112,22 @@ inline void prof_end(int id, cudaStream_t s, double nbytes) {
     if (Prof* p = current_prof()) p->end(id, s, nbytes);
 }
 
+// An NVTX range (Nsight Systems timelines) for the scope: every C-ABI call opens one named after
+// itself, and the scheme drivers one per prologue, attempt and stage (with graph-launched steps
+// the ranges mark the graph launches).  NVTX3 is header-only: without an attached tool a push or
+// pop is a check of a null function pointer.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 }  // namespace qgn
+
+#define QGN_NVTX_CAT2(a, b) a##b
+#define QGN_NVTX_CAT(a, b) QGN_NVTX_CAT2(a, b)
+#define QGN_NVTX(name) ::qgn::NvtxRange QGN_NVTX_CAT(qgn_nvtx_, __LINE__)(name)
 
 // bracket one kernel launch: QGN_LAUNCH(id, algorithmic_bytes, stream, kernel<<<...>>>(...))
 #define QGN_LAUNCH(id, nbytes, stream, ...)          \

@@ -28,11 +28,29 @@ struct Geom {
     int nx, ny, nz, nxh;
     int nkx, nky, kylo, kyshift, nkxp;
     double dkx, dky, inv_nxny;
+    unsigned long long* chk = nullptr;   // failed-check counter of the bounds-checked build (device)
     __host__ __device__ size_t csize() const { return (size_t)nz * nkx * nky; }
     __host__ __device__ size_t hsize() const { return (size_t)nz * ny * nkxp; }
     __host__ __device__ int jfull(int m) const { return m < kylo ? m : m + kyshift; }
     __host__ __device__ double kyval(int j) const { return dky * (double)(j <= ny / 2 ? j : j - ny); }
 };
+
+// Bounds-checked build (compile every source with -DQGN_CHECK; qgn_fortran_b200.build(check=True)
+// makes libqgn_b200_check.so).  The right-hand-side tile bodies, GetPsi and the stage
+// combinations test each global index against the length of the array it addresses -- compact
+// fields g.csize(), packed row pairs g.hsize(), forward x transforms 2 g.hsize() -- before the
+// access.  An index out of range is not accessed (a load yields zero) and increments the
+// context's counter, which qgn_check_failures reads: no trap, no fault, the context stays
+// usable.  In the normal build in_bounds is the constant true and the checks compile away.
+#ifdef QGN_CHECK
+__device__ __forceinline__ bool in_bounds(const Geom& g, size_t i, size_t n) {
+    if (i < n) return true;
+    if (g.chk) atomicAdd(g.chk, 1ull);
+    return false;
+}
+#else
+__device__ __forceinline__ constexpr bool in_bounds(const Geom&, size_t, size_t) { return true; }
+#endif
 
 // Per-layer physical constants of the RHS (QGN_Module.f90:268-292).
 struct LayerConst {
@@ -187,6 +205,7 @@ struct qgn_ctx {
     // stepper memory (the reference's `save` variables); BSRK3's RHS0 and AB3's history
     // live in b.N[0..1], err0 / r0 in the device scalars
     int output_mode = QGN_OUTPUT_KEPT;   // what qgn_step / qgn_advance write back (qgn_set_output)
+    unsigned long long* chk = nullptr;   // device failed-check counter (bounds-checked build only)
     bool first_call = true;
     int ab_calls = 0;
     bool halted = false;           // a step failed; cleared by the next state upload

@@ -44,11 +44,11 @@ __global__ void __launch_bounds__(256, 2) k_modal(Geom g, const __grid_constant_
     double2 qv[NZC], pv[NZC];
 #pragma unroll
     for (int k = 0; k < NZC; ++k)
-        if (k < nz) qv[k] = q[(size_t)k * P + p];
+        if (k < nz) qv[k] = in_bounds(g, (size_t)k * P + p, g.csize()) ? q[(size_t)k * P + p] : make_double2(0.0, 0.0);
     modal_invert<NZ>(mv.proj, mv.back, mv.ev, mv.Htot, nz, k2, p == 0, qv, pv);
 #pragma unroll
     for (int k = 0; k < NZC; ++k)
-        if (k < nz) psi[(size_t)k * P + p] = pv[k];
+        if (k < nz && in_bounds(g, (size_t)k * P + p, g.csize())) psi[(size_t)k * P + p] = pv[k];
 }
 
 // ------------------------------------------------------------------------------------

@@ -208,7 +208,9 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
         auto ld = [&](int j) -> CT {
             const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
             if (!colok || !kept) return cmk<CT>(0.0, 0.0);
-            CT v = src[colbase + (j < g.kylo ? j : j - g.kyshift)];
+            const size_t ci = colbase + (j < g.kylo ? j : j - g.kyshift);
+            if (!in_bounds(g, ci, g.csize())) return cmk<CT>(0.0, 0.0);
+            CT v = src[ci];
             if (f == 1 && NF == 3) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
                 const RT kyv = (RT)g.kyval(j);
                 v = cmk<CT>(kyv * v.y, -kyv * v.x);
@@ -230,6 +232,8 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
             if (k >= g.nkxp) continue;
             const CT f1 = sm[c * C::TS + p], f2 = sm[c * C::TS + C::HY + p];
             const bool ok = k < g.nkx;
+            const size_t ro = ((size_t)l * (NY / 2) + p) * 2 * g.nkxp;   // row pair p of layer l
+            if (!in_bounds(g, ro + g.nkxp + k, g.hsize())) continue;
             CT* row = dl + (size_t)p * 2 * g.nkxp;
             // Re parts at kx = 0 and at the kx Nyquist column (kept only in the full-spectrum geometry)
             row[k] = ok ? pack_lo(f1, f2, k == 0 || 2 * k == g.nx) : cmk<CT>(0.0, 0.0);
@@ -265,10 +269,11 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
     CT* xs = sm + slot * C::TS;
 
     // ---- inverse: slot 0 = q1+iq2, 1 = u1+iu2, 2 = v1+iv2
-    const CT* F = (s_of == 0 ? pq : (s_of == 1 ? pu : pv)) + ((size_t)l * npairs + rp) * 2 * g.nkxp;
+    const size_t fo = ((size_t)l * npairs + rp) * 2 * g.nkxp;   // row pair rp of layer l
+    const CT* F = (s_of == 0 ? pq : (s_of == 1 ? pu : pv)) + fo;
     auto ld_inv = [&](int k) -> CT {
-        if (k < nkx) return F[k];
-        if (k > NX - nkx) return F[g.nkxp + (NX - k)];
+        if (k < nkx) return in_bounds(g, fo + k, g.hsize()) ? F[k] : cmk<CT>(0.0, 0.0);
+        if (k > NX - nkx) return in_bounds(g, fo + g.nkxp + (NX - k), g.hsize()) ? F[g.nkxp + (NX - k)] : cmk<CT>(0.0, 0.0);
         return cmk<CT>(0.0, 0.0);
     };
     // the last pass stores the two rows apart, as real planes: row 2p at RT offset 0 of the
@@ -296,10 +301,15 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
         return cmk<CT>(m * uv, m * vv);
     };
     const int y = 2 * rp + (s_of & 1);
-    CT* out = (s_of < 2) ? pp + ((size_t)l * g.ny + y) * 2 * g.nkxp : pd + (size_t)y * 2 * g.nkxp;
+    const size_t oo = (s_of < 2) ? ((size_t)l * g.ny + y) * 2 * g.nkxp : (size_t)y * 2 * g.nkxp;
+    const size_t olen = (s_of < 2) ? 2 * g.hsize() : (size_t)g.ny * 2 * g.nkxp;   // pp, or pd (one layer)
+    CT* out = ((s_of < 2) ? pp : pd) + oo;
     auto st_fwd = [&](int k, CT v) {
-        if (k < nkx) out[k] = v;
-        else if (k > NX - nkx) out[g.nkxp + (NX - k)] = v;
+        if (k < nkx) {
+            if (in_bounds(g, oo + k, olen)) out[k] = v;
+        } else if (k > NX - nkx) {
+            if (in_bounds(g, oo + g.nkxp + (NX - k), olen)) out[g.nkxp + (NX - k)] = v;
+        }
     };
     fft_fused<NX, -1, SRC_FN_SMEM, DST_FN, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd,
                                                                    st_fwd);
@@ -358,7 +368,9 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     if (DRAG) {
         // drag_hat = i ky (|u|u)^ - i kx (|u|v)^ on the bottom layer (QGN_Module.f90:284-292)
         auto ldd = [&](int y) -> CT {
-            return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, colok, C::TKX);
+            const size_t ro = (size_t)y * 2 * g.nkxp + (fld == 0 ? 0 : g.nkxp) + kx0 + c;
+            const bool ok = colok && in_bounds(g, ro, (size_t)g.ny * 2 * g.nkxp);
+            return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, ok, C::TKX);
         };
         fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ldd, omap);
         const RT dc = (RT)lc->dragc;
@@ -371,15 +383,18 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
             const CT fu = sm[cc * C::TS + j], fv = sm[(C::TKX + cc) * C::TS + j];
             CT d = cmk<CT>(-kyv * fu.y, kyv * fu.x);        // i ky (|u|u)^
             d = cmk<CT>(d.x + kxv * fv.y, d.y - kxv * fv.x);      // - i kx (|u|v)^
-            out[(colbase + kx) * nky + m] = cmk<CT>(dc * d.x, dc * d.y);
+            if (in_bounds(g, (colbase + kx) * nky + m, g.csize())) out[(colbase + kx) * nky + m] = cmk<CT>(dc * d.x, dc * d.y);
         }
         __syncthreads();
     }
 
     // the (uq)^ and (vq)^ slots of one column load P[k] and P[nx-k] respectively and swap
     // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
-    auto ld = [&](int y) -> CT { return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c,
-                                                         fld, colok, C::TKX); };
+    auto ld = [&](int y) -> CT {
+        const size_t ro = ((size_t)l * NY + y) * 2 * g.nkxp + (fld == 0 ? 0 : g.nkxp) + kx0 + c;
+        const bool ok = colok && in_bounds(g, ro, 2 * g.hsize());
+        return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c, fld, ok, C::TKX);
+    };
     fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
 
     const RT ub = (RT)lc->uBar[l], bq = (RT)lc->betaq[l];
@@ -392,6 +407,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
         const int j = g.jfull(m);
         const RT kxv = (RT)(g.dkx * kx), kyv = (RT)g.kyval(j);
         const size_t idx = (colbase + kx) * nky + m;
+        if (!in_bounds(g, idx, g.csize())) continue;
         const CT fuq = sm[cc * C::TS + j], fvq = sm[(C::TKX + cc) * C::TS + j];
         const CT qv = q[idx], pv = psi[idx];
         // jaco_hat = i kx uq_hat + i ky vq_hat  (QGN_Module.f90:244-247)

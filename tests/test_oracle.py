@@ -275,6 +275,31 @@ def test_energetics_identities(nx, ny, nz):
     assert np.allclose(Z, 0.5 * np.mean(qp ** 2, axis=(1, 2)) * w, rtol=1e-14)
 
 
+def test_notebook_profiles_against_the_reference_notebook():
+    """inputs.notebook_profiles against set_background_profiles.ipynb's own computation (its code
+    cells run by tests/golden/notebook/make_notebook_golden.py, nz = 32, alpha = 1), and the deformation
+    radii of the QGN stretching matrix (QGN_Module.f90:100-112, built from those H and S) against
+    the radii the notebook printed in its stored output (cell 9, 8 decimals, H_tot = 4800 m)."""
+    from oracle.qgn_oracle import stretching_matrix
+    from qgn_fortran_b200.inputs import notebook_profiles
+    d = np.load(os.path.join(GOLDEN, "notebook", "notebook_profiles_nz32.npz"))
+    H, S, U, zc = notebook_profiles(nz=int(d["nz"]), alpha=float(d["alpha"]))
+    assert np.allclose(H, d["H"], rtol=1e-12, atol=0)
+    assert np.allclose(S, d["S"], rtol=1e-12, atol=0)
+    assert np.allclose(U, d["UBar"], rtol=1e-12, atol=1e-15)
+    assert np.allclose(zc, d["zc"], rtol=1e-12, atol=0)
+    L = stretching_matrix(H, S)       # depth 1 (sum(h) = 1), f = 1: the notebook's units
+    from qgn_fortran_b200 import model
+    assert np.array_equal(model.stretching_matrix(H, S), L)     # the GPU host set-up builds the same L
+    vals = np.linalg.eigvals(L).real
+    with np.errstate(invalid="ignore", divide="ignore"):
+        radii = float(d["H_tot"]) * np.sort(1.0 / np.sqrt(-vals)) / 1e3
+    want = d["radii_printed"]
+    n = int(np.sum(np.isfinite(want)))            # the barotropic mode prints as nan
+    assert n == int(d["nz"]) - 1
+    assert np.allclose(radii[:n], want[:n], rtol=0, atol=6e-9)
+
+
 def test_write_qp_modal_identities():
     """WriteQPmodal: the modes back-project onto q, psi and the full Jacobian; a single
     Fourier mode in one vertical mode gives that mode alone, psi_mode = q_mode/(-k^2+EVals),
