@@ -172,6 +172,23 @@ __device__ __forceinline__ CT pack_hi(CT f1, CT f2) {
     return cmk<CT>(f1.x + f2.y, f2.x - f1.y);
 }
 
+// Layout of the forward x transforms P[k] (part 0) and P[nx-k] (part 1) of every row y: the x
+// pass's output, the forward y pass's input.  QGN_P_TILED (default 1): tiles of two kx columns,
+// [nz][nkxp/2][ny][2 parts][2 columns], so that the rows of one column pair are contiguous and a
+// warp of the y-forward pass (8 rows x 2 columns x 2 parts) reads 512 contiguous bytes; the
+// x pass's stores of one row scatter over the tiles instead (stores are not waited for).
+// QGN_P_TILED 0: rows [nz][ny][2 parts][nkxp].  Both hold 2 nz ny nkxp elements.
+#ifndef QGN_P_TILED
+#define QGN_P_TILED 0
+#endif
+__host__ __device__ __forceinline__ size_t p_index(const Geom& g, int l, int y, int part, int k) {
+#if QGN_P_TILED
+    return ((size_t)(l * (g.nkxp >> 1) + (k >> 1)) * g.ny + y) * 4 + part * 2 + (k & 1);
+#else
+    return ((size_t)l * g.ny + y) * 2 * g.nkxp + (size_t)part * g.nkxp + k;
+#endif
+}
+
 // ------------------------------------------------------------------------------------
 // yinv: inverse y transforms of kept columns into packed row pairs.
 // NF = 3: (q -> pq, -i ky psi -> pu, i kx psi -> pv);  NF = 2: (q -> pq, psi -> pu);  NF = 1: (f -> pq).
@@ -301,14 +318,16 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
         return cmk<CT>(m * uv, m * vv);
     };
     const int y = 2 * rp + (s_of & 1);
-    const size_t oo = (s_of < 2) ? ((size_t)l * g.ny + y) * 2 * g.nkxp : (size_t)y * 2 * g.nkxp;
-    const size_t olen = (s_of < 2) ? 2 * g.hsize() : (size_t)g.ny * 2 * g.nkxp;   // pp, or pd (one layer)
-    CT* out = ((s_of < 2) ? pp : pd) + oo;
+    const int ol = (s_of < 2) ? l : 0;                                              // pd holds one layer
+    const size_t olen = (s_of < 2) ? 2 * g.hsize() : (size_t)g.ny * 2 * g.nkxp;   // pp, or pd
+    CT* out = (s_of < 2) ? pp : pd;
     auto st_fwd = [&](int k, CT v) {
         if (k < nkx) {
-            if (in_bounds(g, oo + k, olen)) out[k] = v;
+            const size_t i = p_index(g, ol, y, 0, k);
+            if (in_bounds(g, i, olen)) out[i] = v;
         } else if (k > NX - nkx) {
-            if (in_bounds(g, oo + g.nkxp + (NX - k), olen)) out[g.nkxp + (NX - k)] = v;
+            const size_t i = p_index(g, ol, y, 1, NX - k);
+            if (in_bounds(g, i, olen)) out[i] = v;
         }
     };
     fft_fused<NX, -1, SRC_FN_SMEM, DST_FN, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd,
@@ -321,17 +340,20 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
 // radix pass reads the half-transformed rows straight from HBM.
 // ------------------------------------------------------------------------------------
 // split of the packed forward x transform of row y at kx: fld 0 -> (uq)^, fld 1 -> (vq)^
-__device__ __forceinline__ double2 unpack_p(const double2* __restrict__ row, int nkxp, int kx, int fld) {
-    const double2 X = row[kx];
-    const double2 Y = kx == 0 ? cconj(X) : cconj(row[nkxp + kx]);
+__device__ __forceinline__ double2 unpack_p(const double2* __restrict__ P, const Geom& g, int l, int y, int kx,
+                                            int fld) {
+    const double2 X = P[p_index(g, l, y, 0, kx)];
+    const double2 Y = kx == 0 ? cconj(X) : cconj(P[p_index(g, l, y, 1, kx)]);
     return fld == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
                     : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
 }
 
+// the thread of field fld loads part fld (P[k] for fld 0, P[nx-k] for fld 1) at index i and
+// swaps it with its partner's, so each value is read once
 template <class CT>
-__device__ __forceinline__ CT unpack_pair(const CT* __restrict__ row, int nkxp, int kx, int fld, bool ok, int partner) {
+__device__ __forceinline__ CT unpack_pair(const CT* __restrict__ P, size_t i, int kx, int fld, bool ok, int partner) {
     CT mine = cmk<CT>(0.0, 0.0);
-    if (ok && (fld == 0 || kx > 0)) mine = row[fld == 0 ? kx : nkxp + kx];
+    if (ok && (fld == 0 || kx > 0)) mine = P[i];
     CT other;
     other.x = __shfl_xor_sync(0xffffffffu, mine.x, partner);
     other.y = __shfl_xor_sync(0xffffffffu, mine.y, partner);
@@ -368,9 +390,9 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     if (DRAG) {
         // drag_hat = i ky (|u|u)^ - i kx (|u|v)^ on the bottom layer (QGN_Module.f90:284-292)
         auto ldd = [&](int y) -> CT {
-            const size_t ro = (size_t)y * 2 * g.nkxp + (fld == 0 ? 0 : g.nkxp) + kx0 + c;
-            const bool ok = colok && in_bounds(g, ro, (size_t)g.ny * 2 * g.nkxp);
-            return unpack_pair(pd + (size_t)y * 2 * g.nkxp, g.nkxp, kx0 + c, fld, ok, C::TKX);
+            const size_t i = p_index(g, 0, y, fld, kx0 + c);
+            const bool ok = colok && in_bounds(g, i, (size_t)g.ny * 2 * g.nkxp);
+            return unpack_pair(pd, i, kx0 + c, fld, ok, C::TKX);
         };
         fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ldd, omap);
         const RT dc = (RT)lc->dragc;
@@ -391,9 +413,9 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
     // the (uq)^ and (vq)^ slots of one column load P[k] and P[nx-k] respectively and swap
     // them with a shuffle (partner tid ^ TKX, same warp), so each value is read once
     auto ld = [&](int y) -> CT {
-        const size_t ro = ((size_t)l * NY + y) * 2 * g.nkxp + (fld == 0 ? 0 : g.nkxp) + kx0 + c;
-        const bool ok = colok && in_bounds(g, ro, 2 * g.hsize());
-        return unpack_pair(pp + ((size_t)l * NY + y) * 2 * g.nkxp, g.nkxp, kx0 + c, fld, ok, C::TKX);
+        const size_t i = p_index(g, l, y, fld, kx0 + c);
+        const bool ok = colok && in_bounds(g, i, 2 * g.hsize());
+        return unpack_pair(pp, i, kx0 + c, fld, ok, C::TKX);
     };
     fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
 

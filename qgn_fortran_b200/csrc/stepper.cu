@@ -888,14 +888,7 @@ __global__ void __launch_bounds__(StageYinvCfg<NY, NZ>::THREADS)
         const int f = slot / NZ, l = slot % NZ;
         const bool act = slot < 2 * NZ;
         double2* xs = slots + slot * C::TS;
-        const double2* rows = pp + (size_t)(act ? l : 0) * NY * 2 * g.nkxp;
-        auto ld = [&](int y) -> double2 {
-            const double2* row = rows + (size_t)y * 2 * g.nkxp;
-            const double2 X = row[kx];
-            const double2 Y = kx == 0 ? cconj(X) : cconj(row[g.nkxp + kx]);
-            return f == 0 ? make_double2(0.5 * (X.x + Y.x), 0.5 * (X.y + Y.y))
-                          : make_double2(0.5 * (X.y - Y.y), -0.5 * (X.x - Y.x));
-        };
+        auto ld = [&](int y) -> double2 { return unpack_p(pp, g, act ? l : 0, y, kx, f); };
         auto omap = [](int y) { return y; };
         fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, 16, true>(xs, lane, act, twy, ld, omap);
     }
