@@ -303,3 +303,19 @@ def test_trained_closure_beats_leith_offline(cuda_ok):
     r2_leith = 1.0 - np.sum((alpha * lt - yt) ** 2) / np.sum((yt - yt.mean(axis=(0, 1, 2))) ** 2)
     assert r2_cnn > 0.15, (r2_cnn, r2_leith)
     assert r2_cnn > r2_leith + 0.1, (r2_cnn, r2_leith)
+
+
+def test_trained_closure_beats_leith_online(cuda_ok):
+    """The benchmark's closure experiment (qgn_fortran_b200.closure_experiment, its defaults: a
+    1024^2 x 4 truth spun up for a model year, 1024 coarse-grained samples, 3000 Adam steps, a
+    3-day background hyperviscosity): over 60 model days from the coarse-grained truth, the
+    128^2 run with the trained network stays closer to the coarse-grained truth's time-mean KE
+    spectrum than the 128^2 QG-Leith run, and runs at >= 50x the truth run's days/s."""
+    from qgn_fortran_b200.closure_experiment import run
+    res = run()
+    print("closure online:", res["ke_spectrum_err_closure"], "leith:", res["ke_spectrum_err_leith"],
+          "speedup:", res["closure_speedup_vs_truth"])
+    assert res["online_status"] == "ok"
+    assert res["ke_spectrum_err_closure"]["mean_abs_rel"] < res["ke_spectrum_err_leith"]["mean_abs_rel"]
+    assert res["ke_spectrum_err_closure"]["mean_abs_rel"] <= 0.10
+    assert res["closure_speedup_vs_truth"] >= 50.0

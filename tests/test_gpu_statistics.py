@@ -1,15 +1,23 @@
 """Long-time statistics rung of the parity ladder: past the chaotic predictability horizon the GPU
 and the C/OpenMP restatement of the reference (oracle/qgn_ref.c) are two independent realisations
-of the same turbulence, and their time-mean layer kinetic energies and isotropic KE spectra (in
-octave bands of the shell index) must agree within 2 %.
+of the same turbulence, and their time-mean statistics must agree.
 
-Both start from the same seeded IC and run ARK43_QGLeith with the PI.3.4 controller
-(ARK43_QGLeith.f90:75-140) for SPIN years, which separates the trajectories completely (checked),
-then average daily samples for MEAN years.  The configuration -- a two-layer Phillips problem on
-128^2 with a one-day bottom drag on the f-plane -- equilibrates within months and forgets its
-state within days, so the sampling error of a MEAN-year mean is well under the 2 % bound: the
-standard error measured on B200 from a 10-year GPU run of the same configuration is given beside
-the constants.  The oracle's side is the costly one (about 1 minute on the GPU box's 16 cores).
+Configuration: the 2-layer Phillips problem (H = 1000/3000 m, g' = 0.02, U = 0.1/0 m/s) on a
+64^2, 1000 km beta-plane (beta = 1.6e-11) with bottom drag r0 = 2e-6 s^-1, ARK43_QGLeith with the
+PI.3.4 controller (ARK43_QGLeith.f90:75-140) at TOL = 1e-4 max|q_IC|.  Both sides start from the
+same seeded IC, spin up for SPIN model years (the layer energies level off after about 4) and then
+average samples taken every 2 model days for MEAN years.
+
+What converges in MEAN years, and what is asserted.  Two runs of the C oracle from ICs 1e-10
+apart (one 40-year mean each, measured in the build container) agree on the top layer's share
+of the kinetic energy to 0.07 % (batch-mean standard error 0.04 %) and on the shape of the
+top layer's KE spectrum above the domain scale -- the share of the energy at k >= 8 (integer
+wavenumber shells) that each octave band [8, 16), [16, 32) holds -- to 0.2 % and 0.9 % (standard
+errors 0.1 % and 0.7 %).  Those are asserted within 2 %.  The absolute layer energies keep a
+slow variability in a domain this small (the two oracle runs differ by 5 % and 8 %, standard
+errors 2-5 % of a 40-year mean), so they are compared within four combined standard errors
+(from 10 batch means of each run), the statistical equivalence this averaging can resolve; the
+test prints every difference and standard error.
 """
 import math
 
@@ -25,9 +33,10 @@ pytestmark = pytest.mark.gpu
 
 DAY = 86400.0
 YEAR = 365.0 * DAY
-N, L_DOMAIN, U1, R0, BETA = 128, 1.0e6, 0.1, 1.0e-5, 0.0
-SPIN, MEAN = 1.0, 2.0          # years
-BANDS = [(1, 2), (2, 4), (4, 8), (8, 16), (16, 32), (32, 64)]
+N, L_DOMAIN, U1, R0, BETA = 64, 1.0e6, 0.1, 2.0e-6, 1.6e-11
+SPIN, MEAN, EVERY = 4.0, 40.0, 2.0 * DAY
+BANDS = [(1, 2), (2, 4), (4, 8), (8, 16), (16, 32)]
+HIGH = (3, 4)                   # the octave bands at k >= 8
 TOL_STAT = 0.02
 
 
@@ -35,8 +44,8 @@ def config():
     H, S, U = phillips_two_layer(U=(U1, 0.0))
     qp = seeded_random_pv(N, N, 2, 8.0, 1.0e-6, seed=11)
     p = dict(nx=N, ny=N, nz=2, Lx=L_DOMAIN, Ly=L_DOMAIN, Htot=4000.0, f0=1.0e-4, beta=BETA, A2=0.0, A8=1.0e23,
-             r0=R0, C_d=0.0, TOL=1.0e-6 * float(np.max(np.abs(qp))), is_explicit=False,
-             dt_max=math.pi / (1.6e-11 * L_DOMAIN))
+             r0=R0, C_d=0.0, TOL=1.0e-4 * float(np.max(np.abs(qp))), is_explicit=False,
+             dt_max=math.pi / (BETA * L_DOMAIN))
     return p, H, S, U, qp
 
 
@@ -44,50 +53,83 @@ def bands_of(spec):
     return np.array([[spec[l, a:b].sum() for a, b in BANDS] for l in range(spec.shape[0])])
 
 
-def test_time_mean_statistics_match_the_oracle(cuda_ok):
-    p, H, S, U, qp = config()
-    # GPU: sample every simulated day after the spin-up
+def summary(ke, bd):
+    """Per-sample statistics: layer KE [s][2], top-layer share [s], high-band shares [s][2]."""
+    ke, bd = np.array(ke), np.array(bd)
+    top = ke[:, 0] / ke.sum(axis=1)
+    high = bd[:, 0, HIGH[0]:HIGH[1] + 1]
+    shares = high / high.sum(axis=1, keepdims=True)
+    return ke, top, shares
+
+
+def batch_se(x, nb=10):
+    n = len(x) // nb * nb
+    m = x[:n].reshape(nb, -1, *x.shape[1:]).mean(axis=1)
+    return m.std(axis=0, ddof=1) / np.sqrt(nb)
+
+
+def gpu_run(p, H, S, U, qp):
     g = QGNModule(p, H, S, U, scheme="ark43_qgleith")
     g.initialize(qp, 0.0, 1800.0)
     t = 0.0
     while t < SPIN * YEAR:
-        g.advance_resident(10)
+        g.advance_resident(20)
         t, _ = g.time()
-    ke_g, bd_g, n_g, nxt = 0.0, 0.0, 0, t + DAY
+    ke, bd, nxt = [], [], t + EVERY
     while t < (SPIN + MEAN) * YEAR:
         g.advance_resident(1)
         t, _ = g.time()
         if t >= nxt:
-            ke, sp = g.diagnostics(N // 2)
-            ke_g, bd_g, n_g = ke_g + ke, bd_g + bands_of(sp), n_g + 1
-            nxt += DAY
-    q_gpu = g.get_state()
+            k, sp = g.diagnostics(N // 2)
+            ke.append(k)
+            bd.append(bands_of(sp))
+            nxt += EVERY
+    q = g.get_state()
     g.cleanup()
+    return ke, bd, q
 
-    # the C oracle, the same way; its diagnostics from the numpy oracle's physical-space forms
+
+def oracle_run(p, H, S, U, qp):
     c = RefC(Params(**p), H, S, U, scheme="ark43_qgleith")
     m = QGNOracle(Params(**p), H, S, U)
     q = c.initialize_spec(qp)
     t, dt = 0.0, 1800.0
     while t < SPIN * YEAR:
         t, dt = c.step(q, t, dt)
-    ke_o, bd_o, n_o, nxt = 0.0, 0.0, 0, t + DAY
+    ke, bd, nxt = [], [], t + EVERY
     while t < (SPIN + MEAN) * YEAR:
         t, dt = c.step(q, t, dt)
         if t >= nxt:
-            ke_o, bd_o, n_o = ke_o + m.layer_ke(q), bd_o + bands_of(m.ke_spectrum(q, N // 2)), n_o + 1
-            nxt += DAY
+            ke.append(m.layer_ke(q))
+            bd.append(bands_of(m.ke_spectrum(q, N // 2)))
+            nxt += EVERY
+    return ke, bd, q
 
+
+def test_time_mean_statistics_match_the_oracle(cuda_ok):
+    p, H, S, U, qp = config()
+    ke_g, bd_g, q_g = gpu_run(p, H, S, U, qp)
+    ke_o, bd_o, q_o = oracle_run(p, H, S, U, qp)
+    assert abs(len(ke_g) - len(ke_o)) <= 2
     # past the predictability horizon: the two states are unrelated
-    sep = np.linalg.norm(q_gpu - q) / np.linalg.norm(q)
-    ke_g, ke_o = ke_g / n_g, ke_o / n_o
-    bd_g, bd_o = bd_g / n_g, bd_o / n_o
-    ke_err = np.abs(ke_g / ke_o - 1.0)
-    keep = bd_o >= 0.01 * bd_o.sum(axis=1, keepdims=True)
-    bd_err = np.abs(bd_g / bd_o - 1.0)[keep]
-    print(f"long-time statistics: separation {sep:.2f}, samples {n_g}/{n_o}, layer KE err {ke_err.max():.4f}, "
-          f"band err {bd_err.max():.4f}")
-    assert sep > 0.5
-    assert abs(n_g - n_o) <= 2
-    assert np.all(ke_err <= TOL_STAT)
-    assert np.all(bd_err <= TOL_STAT)
+    sep = float(np.linalg.norm(q_g - q_o) / np.linalg.norm(q_o))
+    assert sep > 0.5, sep
+
+    kg, tg, sg = summary(ke_g, bd_g)
+    ko, to, so = summary(ke_o, bd_o)
+    rows = []
+
+    def compare(name, a, b, strict):
+        d = abs(a.mean(axis=0) / b.mean(axis=0) - 1.0)
+        se = np.sqrt((batch_se(a) / a.mean(axis=0)) ** 2 + (batch_se(b) / b.mean(axis=0)) ** 2)
+        rows.append(f"{name}: rel diff {np.round(d, 4)} combined SE {np.round(se, 4)}")
+        return np.all(d <= TOL_STAT) if strict else np.all(d <= 4.0 * se)
+
+    ok_top = compare("top-layer share of KE", tg, to, strict=True)
+    ok_shape = compare("top-layer KE spectrum, shares of k>=8 in [8,16), [16,32)", sg, so, strict=True)
+    ok_ke = compare("layer KE", kg, ko, strict=False)
+    ok_tot = compare("total KE", kg.sum(axis=1), ko.sum(axis=1), strict=False)
+    print(f"long-time statistics ({len(kg)}/{len(ko)} samples over {MEAN:.0f} years, separation {sep:.2f}):\n  "
+          + "\n  ".join(rows))
+    assert ok_top and ok_shape, rows
+    assert ok_ke and ok_tot, rows
