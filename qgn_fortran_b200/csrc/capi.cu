@@ -170,6 +170,7 @@ const char* status_text(int st) {
     switch (st) {
         case QGN_ERR_NONFINITE: return "non-finite embedded error estimate";
         case QGN_ERR_REJECT_LIMIT: return "adaptive step rejected max_rejects times in a row";
+        case QGN_ERR_CUDA: return "a bounded device wait ran out";
         default: return "step failed";
     }
 }
@@ -543,6 +544,7 @@ int check_state(qgn_ctx* ctx) {
     DevScalars s;
     CK(launch_nonfinite_check(ctx->g, ctx->b.q, ctx->b.sc, ctx->stream));
     RET(read_scalars(ctx, &s));
+    if (s.wait_timeout) return set_err(ctx, QGN_ERR_CUDA, "a bounded device wait ran out");
     if (s.nonfinite) return set_err(ctx, QGN_ERR_NONFINITE, "non-finite values in the state q_hat");
     return QGN_OK;
 }
@@ -685,6 +687,8 @@ int qgn_create(const qgn_params* p, const double* H, const double* S, const doub
     AL(b.red, (size_t)512 * kMaxNZ);
     AL(b.Hw, (size_t)kMaxNZ);
     AL(b.lc, 1); AL(b.mc, 1); AL(b.sc, 1);
+    if (rc == QGN_OK)   // the sticky flag a bounded device wait sets when it runs out
+        g.wait_err = reinterpret_cast<int*>(reinterpret_cast<char*>(b.sc) + offsetof(DevScalars, wait_timeout));
 #ifdef QGN_CHECK
     AL(ctx->chk, 1);
     if (rc == QGN_OK) {

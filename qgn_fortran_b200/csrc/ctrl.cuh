@@ -21,7 +21,11 @@ __device__ __forceinline__ unsigned ctrl_decide(int kind, double inv_n, double T
     sc->err1 = err1;
     sc->attempts += 1;
     unsigned again = 0;
-    if (!(err1 == err1) || isinf(err1)) {
+    if (sc->wait_timeout) {   // a transform of this attempt ran on data it never received
+        sc->accept = 0;
+        sc->halt = 1;
+        sc->status = QGN_ERR_CUDA;
+    } else if (!(err1 == err1) || isinf(err1)) {
         sc->nonfinite = 1;
         sc->accept = 0;
         sc->halt = 1;

@@ -29,6 +29,8 @@ struct Geom {
     int nkx, nky, kylo, kyshift, nkxp;
     double dkx, dky, inv_nxny;
     unsigned long long* chk = nullptr;   // failed-check counter of the bounds-checked build (device)
+    int* wait_err = nullptr;             // set to 1 when a bounded device wait runs out (device);
+                                         // null: the kernels take no path that waits
     __host__ __device__ size_t csize() const { return (size_t)nz * nkx * nky; }
     __host__ __device__ size_t hsize() const { return (size_t)nz * ny * nkxp; }
     __host__ __device__ int jfull(int m) const { return m < kylo ? m : m + kyshift; }
@@ -148,6 +150,7 @@ struct DevScalars {
     long long accepted;           // accepted steps since creation
     long long attempts;           // attempts (accepted + rejected) since creation
     long long rejected;           // rejected attempts since creation
+    int wait_timeout;             // a bounded device wait (bulk-copy completion) ran out; sticky
     double A8L[kMaxNZ];
 };
 

@@ -190,11 +190,62 @@ __host__ __device__ __forceinline__ size_t p_index(const Geom& g, int l, int y, 
 }
 
 // ------------------------------------------------------------------------------------
+// Bulk-copy staging (cp.async.bulk, the untiled TMA copy) of contiguous global spans into shared
+// memory, completing on an mbarrier.  Source and destination are 16-byte aligned and the sizes
+// multiples of 16 bytes; a CTA copies from this GPU's own memory only, with no multicast.
+// QGN_Y_BULK (build-time knob, default 1): the FP64 y-inverse stages its compact columns this way.
+// ------------------------------------------------------------------------------------
+#ifndef QGN_Y_BULK
+#define QGN_Y_BULK 1
+#endif
+constexpr long long kBulkWaitLimit = 1LL << 22;   // polls of the mbarrier before the wait gives up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+    // the initialised barrier becomes visible to the async (bulk-copy) proxy
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void bar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+// bounded wait for phase `parity` of the barrier; false when it ran out
+__device__ __forceinline__ bool bar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kBulkWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------------------------
 // yinv: inverse y transforms of kept columns into packed row pairs.
 // NF = 3: (q -> pq, -i ky psi -> pu, i kx psi -> pv);  NF = 2: (q -> pq, psi -> pu);  NF = 1: (f -> pq).
-// The first radix pass reads the compact column straight from HBM (zeros in the dealiased
-// band); the transformed column stays in shared memory, where a packing loop pairs rows
-// y and y+1 and writes the two packed arrays with TKX-wide coalesced stores.
+// The first radix pass reads the compact column (zeros in the dealiased band) straight from HBM,
+// or, in FP64 with a wait-flag in the geometry (QGN_Y_BULK), from the column's own shared-memory
+// slot, where one bulk copy per column has staged it; the transformed column stays in shared
+// memory, where a packing loop pairs rows y and y+1 and writes the two packed arrays with
+// TKX-wide coalesced stores.
 // ------------------------------------------------------------------------------------
 template <int NY, int NF, class CT, int TV = 0>
 // f_begin/f_end: the fields this CTA transforms (all NF by default; one each when a launch
@@ -222,17 +273,13 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
         if (f < f_begin || f >= f_end) continue;
         const CT* src = (f == 0) ? q : psi;
         CT* dst = (f == 0) ? pq : (f == 1 ? pu : pv);
-        auto ld = [&](int j) -> CT {
-            const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
-            if (!colok || !kept) return cmk<CT>(0.0, 0.0);
-            const size_t ci = colbase + (j < g.kylo ? j : j - g.kyshift);
-            if (!in_bounds(g, ci, g.csize())) return cmk<CT>(0.0, 0.0);
-            CT v = src[ci];
-            if (f == 1 && NF == 3) {   // u_hat = -i ky psi_hat  (QGN_Module.f90:223)
+        // the spectral derivative of field f at ky index j (QGN_Module.f90:223-224)
+        auto deriv = [&](CT v, int j) -> CT {
+            if (f == 1 && NF == 3) {   // u_hat = -i ky psi_hat
                 const RT kyv = (RT)g.kyval(j);
-                v = cmk<CT>(kyv * v.y, -kyv * v.x);
-            } else if (f == 2) {   // v_hat = i kx psi_hat  (QGN_Module.f90:224)
-                v = cmk<CT>(-kxv * v.y, kxv * v.x);
+                return cmk<CT>(kyv * v.y, -kyv * v.x);
+            } else if (f == 2) {   // v_hat = i kx psi_hat
+                return cmk<CT>(-kxv * v.y, kxv * v.x);
             }
             return v;
         };
@@ -240,7 +287,50 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
         // packing loop below reads consecutive offsets (free of bank-group conflicts; HY
         // offsets the odd half so that the last pass's stores are conflict-free too)
         auto omap = [](int y) { return (y & 1) * C::HY + (y >> 1); };
-        fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
+        bool staged = false;
+        if constexpr (QGN_Y_BULK && sizeof(CT) == 16) {
+            const int ncol = cmin(C::TKX, g.nkx - kx0);   // kept columns of this tile (>= 1)
+            const size_t last = ((size_t)l * g.nkx + kx0 + ncol - 1) * g.nky + g.nky - 1;
+            if (g.wait_err && in_bounds(g, last, g.csize())) {
+                // one bulk copy per kept column into its slot (nky <= TS elements), thread 0 issues
+                __shared__ __align__(8) uint64_t ybar;
+                // this thread's earlier accesses to the slots are ordered before the copies' writes
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                if (tid == 0) bar_init(&ybar);
+                __syncthreads();   // the barrier is initialised before anyone waits on it
+                if (tid == 0) {
+                    bar_expect_tx(&ybar, (uint32_t)(ncol * g.nky * (int)sizeof(CT)));
+                    for (int c = 0; c < ncol; ++c)
+                        bulk_g2s(sm + c * C::TS, src + ((size_t)l * g.nkx + kx0 + c) * g.nky,
+                                 (uint32_t)(g.nky * (int)sizeof(CT)), &ybar);
+                }
+                if (!bar_wait_bounded(&ybar, 0)) {
+                    atomicExch(g.wait_err, 1);            // the controller halts the run on it
+                    bar_wait_bounded(&ybar, 0);           // once more for the copies still in flight
+                }
+                const CT* stage = xs;
+                auto lds = [&](int j) -> CT {
+                    const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
+                    if (!colok || !kept) return cmk<CT>(0.0, 0.0);
+                    return deriv(stage[j < g.kylo ? j : j - g.kyshift], j);
+                };
+                // SRC_FN_SMEM: every thread has read the staged column before the first pass
+                // overwrites the slot (block-wide barrier inside the pass)
+                fft_fused<NY, +1, SRC_FN_SMEM, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, lds, omap);
+                if (tid == 0) bar_inval(&ybar);           // every waiter has passed the barrier
+                staged = true;
+            }
+        }
+        if (!staged) {
+            auto ld = [&](int j) -> CT {
+                const bool kept = (j < g.kylo) || (j >= g.kylo + g.kyshift);
+                if (!colok || !kept) return cmk<CT>(0.0, 0.0);
+                const size_t ci = colbase + (j < g.kylo ? j : j - g.kyshift);
+                if (!in_bounds(g, ci, g.csize())) return cmk<CT>(0.0, 0.0);
+                return deriv(src[ci], j);
+            };
+            fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
+        }
         // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
         CT* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
         for (int e = tid; e < (NY / 2) * C::TKX; e += C::THREADS) {

@@ -645,6 +645,7 @@ __global__ void k_set_time(DevScalars* sc, double t, double dt) {
     sc->halt = 0;
     sc->status = 0;
     sc->rejects_step = 0;
+    sc->wait_timeout = 0;
 }
 
 // ------------------------------------------------------------------------------------------

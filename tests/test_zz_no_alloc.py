@@ -100,3 +100,31 @@ def test_rhs_static_refuses_stream_capture(cuda_ok):
         rc = call_static(g, q_dev, out_dev, s.cuda_stream)
         out_dev.zero_()     # one captured node, so the graph is not empty
     assert rc == _lib.QGN_ERR_CONFIG
+
+
+def test_rhs_static_on_a_second_device(cuda_ok):
+    """The scratch array's device address and the kernels' shared-memory opt-in are per device:
+    after calls on device 0, calls on device 1 (qgn_rhs_static, then a context there) must give
+    the same right-hand side.  Needs two GPUs."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one visible GPU")
+    nx, ny, nz = 128, 256, 4
+    H, S, U = exponential_stratification(nz)
+    params = dict(nx=nx, ny=ny, nz=nz, Lx=2.0e6, Ly=4.0e6, Htot=4000.0, beta=2.0e-11, A8=1.0e20, r0=1.0e-7,
+                  TOL=1.0e-12)
+    outs = []
+    for dev in (0, 1):
+        with torch.cuda.device(dev):
+            g = QGNModule(params, H, S, U, scheme="ark43_qgleith")
+            q = g.initialize(seeded_random_pv(nx, ny, nz, 8.0, 1.0e-6, seed=31))
+            q_dev = torch.from_numpy(q).to(f"cuda:{dev}")
+            out_dev = torch.empty_like(q_dev)
+            assert call_static(g, q_dev, out_dev, torch.cuda.current_stream(dev).cuda_stream) == _lib.QGN_OK
+            torch.cuda.synchronize(dev)
+            out = out_dev.cpu().numpy()
+            assert np.all(layer_rel(out, g.get_rhs(q)) <= RHS_TOL)
+            outs.append(out)
+            g.cleanup()
+    assert np.all(layer_rel(outs[1], outs[0]) <= RHS_TOL)
