@@ -420,6 +420,39 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
             if (in_bounds(g, i, olen)) out[i] = v;
         }
     };
+#if QGN_P_TILED
+    // Tiled layout: the last radix pass leaves the kept outputs in the transform's own slot
+    // (P[k] at k, P[nx-k] at nkxp + k; the dealiased band's outputs on the slot's last element),
+    // and the whole CTA then writes each kx column pair's values of its rows as one contiguous
+    // run: with one row pair per CTA, rows 2p and 2p+1 of a tile are adjacent, 8 values = 128 B.
+    if (2 * g.nkxp < C::TS - 1) {   // the kept outputs fit below the spare element (uniform)
+        auto omap = [&](int k) -> int {
+            if (k < nkx) return k;
+            if (k > NX - nkx) return g.nkxp + (NX - k);
+            return C::TS - 1;
+        };
+        fft_fused<NX, -1, SRC_FN_SMEM, DST_SMEM_MAP, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2),
+                                                                             twx, ld_fwd, omap);
+        // fft_fused ended with a block-wide barrier: every slot holds its row's outputs
+        const int T = g.nkxp >> 1;
+        for (int dr = 0; dr < (DRAG ? 2 : 1); ++dr) {   // dr 0: uq + i vq into pp; 1: drag fields into pd
+            CT* o = dr == 0 ? pp : pd;
+            const int ol2 = dr == 0 ? l : 0;
+            const size_t olen2 = dr == 0 ? 2 * g.hsize() : (size_t)g.ny * 2 * g.nkxp;
+            for (int e = tid; e < C::RP * T * 8; e += C::THREADS) {
+                const int r = e / (T * 8), rem = e % (T * 8);
+                const int t = rem >> 3, w = rem & 7;
+                const int rr = w >> 2, part = (w >> 1) & 1, k = 2 * t + (w & 1);
+                const int rpp = bx * C::RP + r;
+                if (rpp >= npairs || k >= nkx || (part == 1 && k == 0)) continue;
+                const CT* src = sm + (r * C::SP + 2 * dr + rr) * C::TS;
+                const size_t i = p_index(g, ol2, 2 * rpp + rr, part, k);
+                if (in_bounds(g, i, olen2)) o[i] = src[part * g.nkxp + k];
+            }
+        }
+        return;
+    }
+#endif
     fft_fused<NX, -1, SRC_FN_SMEM, DST_FN, C::TP, (C::G <= 32)>(xs, lane, pair_ok && s_of < (DRAG ? 4 : 2), twx, ld_fwd,
                                                                    st_fwd);
 }

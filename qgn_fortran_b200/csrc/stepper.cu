@@ -728,8 +728,14 @@ __global__ void __launch_bounds__(256, 2) k_ark_stage_small(Geom g, CombPtrs<dou
         if (l < nz) psi[(size_t)l * P + p] = pv[l];
 }
 
-// grids of at most this many kept mode-layers take the fused stage kernel
+// grids of at most this many kept mode-layers take the fused stage kernel and the column kernels
 constexpr size_t kSmallStage = (size_t)1 << 17;
+// the fused stage kernel (combination and GetPsi of all layers per mode) up to this many kept
+// mode-layers (build-time tuning knob; beyond it the stage is a streaming combination per
+// element followed by GetPsi)
+#ifndef QGN_FUSED_STAGE_MAX
+#define QGN_FUSED_STAGE_MAX kSmallStage
+#endif
 
 template <int NZ>
 static cudaError_t launch_stage_small_nz(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
@@ -1057,7 +1063,7 @@ cudaError_t launch_modal_f32(const Geom& g, const Buffers& b, const float2* q, f
 
 // stage s of ARK4(3)6L[2]SA: q_s (streaming combination), then psi_s = GetPsi(q_s)
 cudaError_t launch_ark_stage(const Geom& g, const Buffers& b, int s, cudaStream_t st) {
-    if (g.csize() <= kSmallStage && b.mc_h) {
+    if (g.csize() <= (size_t)(QGN_FUSED_STAGE_MAX) && b.mc_h) {
         switch (g.nz) {
             case 2: return launch_stage_small_nz<2>(g, b, s, st);
             case 4: return launch_stage_small_nz<4>(g, b, s, st);
@@ -1145,10 +1151,12 @@ cudaError_t launch_lincomb(const Geom& g, const Combo& cb, double2* out, cudaStr
     return cudaGetLastError();
 }
 
-// blocks per layer of the Parseval reductions (the partial buffer holds 512*kMaxNZ doubles)
+// blocks per layer of the Parseval reductions: about 8 per SM over all layers, so each thread
+// streams only a few dozen modes (with 2 per SM the Leith reduction of 1024^2 x 8 read its
+// 29.8 MB at 1.1 TB/s); the partials buffer holds 512 x kMaxNZ doubles, 3 x nz x nb at most here
 static int parseval_blocks(const Geom& g) {
     const size_t P = (size_t)g.nkx * g.nky;
-    const size_t want = (size_t)(2 * 148 + g.nz - 1) / g.nz;   // ~2 blocks per SM over all layers
+    const size_t want = (size_t)(8 * 148 + g.nz - 1) / g.nz;
     size_t nb = (P + 255) / 256;
     if (nb > want) nb = want;
     if (nb > 512) nb = 512;
