@@ -22,6 +22,7 @@ Multi-GPU (torchrun): the path does not shard -- each rank advances an independe
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -382,6 +383,7 @@ def ours_arm(args):
                 "ms_per_launch": top[0] / top[2] if top[2] else None,
                 "share_of_kernel_time": top[0] / roof_ms if roof_ms else None,
                 "timed_steps": nroof}
+    roofline["fp64"] = fp64_roofline(g, w, fam, ms_all / args.steps)
     kernels = {f[4]: {"ms": round(f[0], 4), "launches": f[3]} for f in fam if f[3]}
 
     cpu = None
@@ -518,6 +520,42 @@ def read_traffic(workload, kernel):
             except ValueError:
                 return None
     return None
+
+
+def fp64_roofline(g, w, fam, ms_step):
+    """FLOP fraction of the x pass and of the step against the FP64 FMA peak measured here.
+
+    Algorithmic FLOPs: 5 N log2 N per complex N-point FFT, i.e. 2.5 nx ny log2(nx) for the x part
+    of one real 2-D transform (five per layer: q, u, v inverse and uq, vq forward; two more on
+    the bottom layer with quadratic drag) plus 5 nx ny per layer for the scalings and products;
+    per RHS 2.5 nx ny log2(nx ny) per real 2-D transform plus 4 nz^2 per kept spectral mode for
+    GetPsi (to modes and back); six RHS per ARK43_QGLeith step (stage combinations, update, error
+    norm and controller not counted)."""
+    tf, pms = ctypes.c_double(), ctypes.c_double()
+    rc = g.lib.qgn_probe_fp64_fma(5, ctypes.byref(tf), ctypes.byref(pms))
+    if rc != 0:
+        return {"unavailable": f"FP64 probe returned {rc}"}
+    p = w.params
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    nkx = nx // 3
+    nky = ny - ny // 3 - 1
+    drag = p.get("C_d", 0.0) != 0.0
+    ntr = 5 * nz + (2 if drag else 0)
+    x_flops_layer = 2.5 * nx * ny * math.log2(nx) * 5 + 5.0 * nx * ny
+    x_bytes_layer = 5 * ny * nkx * 16
+    peak = tf.value
+    out = {"unit": "TFLOP/s", "peak": peak, "peak_source": "FP64 FMA probe (qgn_probe_fp64_fma: 32 chains per "
+           "thread, 8 CTAs of 256 per SM, best of 5 launches) on this GPU", "probe_ms": pms.value}
+    xp = [f for f in fam if f[4] == "xpass" and f[2]]
+    if xp and not drag:
+        f = xp[0]
+        flops = (f[1] / f[2]) / x_bytes_layer * x_flops_layer   # layers per launch x FLOPs per layer
+        ach = flops / ((f[0] / f[2]) / 1000.0) / 1e12
+        out.update({"kernel": "xpass", "flops_per_launch": flops, "achieved": ach, "frac": ach / peak})
+    rhs = 2.5 * nx * ny * math.log2(nx * ny) * ntr + 4.0 * nz * nz * nkx * nky
+    step_ach = 6 * rhs / (ms_step / 1000.0) / 1e12
+    out.update({"step_flops": 6 * rhs, "step_achieved": step_ach, "step_frac": step_ach / peak})
+    return out
 
 
 def main():

@@ -20,8 +20,9 @@ extern "C" {
  * doubles).  which: 0 state q (compact [nz][nx/3][nky]), 1 psi of the last evaluation
  * (compact), 2..6 the half-transformed fields [nz][ny][nkxp] of the last RHS as packed row
  * pairs [nz][ny/2][2][nkxp]: 2 q, 3 v = i kx psi, 4 u = -i ky psi; 5 the forward x transforms
- * of u*q + i v*q in tiles of two kx columns, [nz][nkxp/2][ny][2][2] (P[k] then P[nx-k] of
- * columns k = 2c, 2c+1, for k < nkx).  nkxp = nx/3 rounded up to a multiple of 4.
+ * P of u*q + i v*q row by row, [nz][ny][2][nkxp] (P[k] at k and P[nx-k] at nkxp + k, for
+ * k < nkx; a build with -DQGN_P_TILED=1 stores them in tiles of two kx columns instead,
+ * [nz][nkxp/2][ny][2][2]).  nkxp = nx/3 rounded up to a multiple of 4.
  */
 int qgn_debug_read(qgn_ctx* ctx, int which, double* out, long long count);
 

@@ -112,6 +112,7 @@ SIGNATURES = {
     "qgn_stream": (C.c_int, [_ctxp, C.POINTER(C.c_void_p)]),
     "qgn_debug_read": (C.c_int, [_ctxp, C.c_int, _dp, C.c_longlong]),
     "qgn_check_failures": (C.c_int, [_ctxp, C.POINTER(C.c_longlong)]),
+    "qgn_probe_fp64_fma": (C.c_int, [C.c_int, _dp, _dp]),
     "qgn_rhs_static": (C.c_int, [C.POINTER(qgn_params), _dp, _dp, _dp, _dp, _dp, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
     "qgn_last_error": (C.c_char_p, [_ctxp]),

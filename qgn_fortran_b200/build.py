@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqgn_b200.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["rhs_kernels.cu", "layout.cu", "stepper.cu", "capi.cu", "rhs_static.cu", "ensemble.cu", "cnn.cu", "closure.cu"]
+SOURCES = ["rhs_kernels.cu", "layout.cu", "stepper.cu", "capi.cu", "rhs_static.cu", "ensemble.cu", "cnn.cu", "closure.cu",
+           "probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

@@ -68,4 +68,5 @@ def test_argument_validation_without_device(lib):
                           _lib.dptr(H), 9, 0, C.byref(ctx)) == _lib.QGN_ERR_CONFIG     # scheme
     assert lib.qgn_step(None, None, None, None) == _lib.QGN_ERR_ARG
     assert lib.qgn_destroy(None) == 0
+    assert lib.qgn_probe_fp64_fma(0, None, None) == _lib.QGN_ERR_ARG
     assert lib.qgn_last_error(None) == b"null context"
