@@ -5,8 +5,8 @@
 // the channel count padded to a multiple of 16; weights are FP32 masters with BF16 copies in
 // two layouts (forward: [tap][cout][cin], backward-data: [tap'][cin][cout] with the taps
 // mirrored); products run on the BF16 tensor cores with FP32 accumulation: tcgen05.mma with
-// the accumulator tile in TMEM (default), or the warp-level mma.m16n8k16 path (selectable with
-// qgn_cnn_set_engine or QGN_CNN_MMA=sync; the weight gradients always use it).  An inference
+// the accumulator tile in TMEM (default; forward, backward-data and weight gradients), or the
+// warp-level mma.m16n8k16 path (selectable with qgn_cnn_set_engine or QGN_CNN_MMA=sync).  An inference
 // whose tiles fit one CTA each runs all layers in one cooperative launch (k_cnn_fused);
 // QGN_CNN_MMA=layers keeps one tcgen05 launch per layer.
 //
@@ -20,6 +20,7 @@
 //   k_mse                 loss and dL/dY = 2 (Y - T)/count, as BF16 G of the last layer
 //   k_adam                Adam on the FP32 masters, refreshing both BF16 layouts
 //   k_conv_tc<CIN,COUT,EPI>  the implicit GEMM on tcgen05 (TMEM accumulators)
+//   k_wgrad_tc<CIN,COUT>  the weight-gradient partials on tcgen05 (M = 64, MN-major operands)
 //   k_cnn_fused           every layer of a small-batch inference, rows exchanged through L2
 #include "qgn_internal.cuh"
 #include "cnn.cuh"
@@ -949,6 +950,200 @@ __global__ void __launch_bounds__(kThreads, 1) k_cnn_fused(FusedArgs a) {
     }
 }
 
+// ---- weight gradient on tcgen05 -------------------------------------------------------------
+// dW[tap][n][k] = sum_p G[p][n] X[p + tap][k] as MMAs with M = 64 (the 64-channel side: G when
+// COUT = 64, else X, whose channels are then padded to 64 with zero rows), N = the other side's
+// channels and K = 16 pixels.  Both operands are read MN-major (channels contiguous), straight
+// from the NHWC rows staged in the [channel group][pixel][16 B] layout of the forward pass, so a
+// tap's horizontal shift is a 16-byte offset of the descriptor's start address.  One CTA covers
+// a chunk of image rows for one tap row dh and keeps the three taps dw in TMEM; each stage (one
+// image row segment of 128 pixels: X row h + dh with its periodic halo, G row h) is fetched into
+// a three-buffer ring while the previous stage's 24 MMAs run.  On B200 an M = 64 accumulator
+// holds row m in TMEM lane 32 (m / 16) + m % 16, and an MN-major no-swizzle descriptor takes the
+// stride between 8-pixel (K) groups as its leading byte offset and the stride between 8-channel
+// groups as its stride byte offset (both measured with known operands).
+namespace tc {
+template <int CIN, int COUT>
+struct WgLay {
+    static constexpr bool A_IS_G = COUT == 64;
+    static constexpr int N = A_IS_G ? CIN : COUT;           // MMA N
+    static constexpr int XG = A_IS_G ? CIN / 8 : 8;        // channel groups of an X slot
+    static constexpr int GG = A_IS_G ? 8 : COUT / 8;       // channel groups of a G slot
+    static constexpr int X_BYTES = XG * kPixS * 16;
+    static constexpr int G_BYTES = GG * kTileP * 16;
+    static constexpr int STAGE = (X_BYTES + G_BYTES + 1023) / 1024 * 1024;
+    static constexpr int NST = 3;                          // ring buffers
+    static constexpr int BAR_OFF = NST * STAGE;
+    static constexpr int SMEM = BAR_OFF + 64;
+    static constexpr int TMEM_COLS = 3 * N <= 64 ? 64 : (3 * N <= 128 ? 128 : 256);
+    // every byte an MMA reads lies inside its stage, under either reading of LBO/SBO: the
+    // furthest is the last pixel group of the last channel group at the largest start offset
+    static_assert((16 * 7 + 2) * 16 + (XG - 1) * kPixS * 16 + 2 * 128 <= X_BYTES, "X reads stay in the slot");
+    static_assert(16 * 7 * 16 + (GG - 1) * kTileP * 16 + 2 * 128 <= G_BYTES, "G reads stay in the slot");
+};
+
+// M = 64, N, BF16 x BF16 -> F32, both operands MN-major
+template <int N>
+__host__ __device__ constexpr uint32_t idesc_mn() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(64 >> 4) << 24);
+}
+
+// one G row segment (image b, row h, pixels w0 .. w0+127) into a slot [C/8][128][16 B]
+template <int C>
+__device__ __forceinline__ void fetch_grow(const __nv_bfloat16* __restrict__ g, int b, int h, int H, int W, int w0,
+                                          uint32_t slot_addr) {
+    const size_t row = ((size_t)b * H + h) * W + w0;
+    for (int i = threadIdx.x; i < kTileP * (C / 8); i += kThreads) {
+        const int c8 = i % (C / 8), px = i / (C / 8);
+        cp16(slot_addr + (uint32_t)((c8 * kTileP + px) * 16), g + (row + px) * C + c8 * 8);
+    }
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+}  // namespace tc
+
+// partial[chunk][tap][n][k] over the chunk's rows for taps 3 dh' + 0..2 (dh' = blockIdx.y)
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_wgrad_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ gr, int B, int H, int W,
+               float* __restrict__ part, int* __restrict__ err) {
+    QGN_PDL_ENTRY();
+    using L = tc::WgLay<CIN, COUT>;
+    constexpr int N = L::N;
+    extern __shared__ __align__(1024) unsigned char smw[];
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(smw + L::BAR_OFF + 32);
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t base_a = smem_u32(smw), bar_a = smem_u32(smw + L::BAR_OFF);
+    const int dhi = blockIdx.y, dh = dhi - 1;
+    const int chunk = blockIdx.x;
+    const int segs = W / kTileP;
+    const int r0 = chunk * kWChunkRows, r1 = min(B * H, r0 + kWChunkRows);
+    const int S = (r1 - r0) * segs;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "r"((uint32_t)L::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < L::NST; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a + 8u * i));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if constexpr (!L::A_IS_G && CIN < 64) {   // X as M: channel groups CIN/8 .. 7 are zero rows
+        constexpr int P = tc::kPixS;
+        for (int i = threadIdx.x; i < L::NST * (8 - CIN / 8) * P; i += kThreads) {
+            const int st = i / ((8 - CIN / 8) * P), r = i % ((8 - CIN / 8) * P);
+            *reinterpret_cast<uint4*>(smw + st * L::STAGE + (CIN / 8) * P * 16 + r * 16) = make_uint4(0, 0, 0, 0);
+        }
+    }
+    auto fetch = [&](int s, int buf) {
+        const int row = r0 + s / segs, w0 = (s % segs) * kTileP;
+        const int b = row / H, h = row % H;
+        const uint32_t xs = base_a + (uint32_t)(buf * L::STAGE), gs = xs + (uint32_t)L::X_BYTES;
+        tc::fetch_row<CIN>(x, b, (h + dh + H) % H, H, W, w0, xs);
+        tc::fetch_grow<COUT>(gr, b, h, H, W, w0, gs);
+        tc::cp_commit();
+    };
+    fetch(0, 0);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tslot;
+
+    bool failed = false;
+    int issued = 0;   // stages whose MMAs were issued
+    for (int s = 0; s < S; ++s) {
+        const int buf = s % L::NST;
+        if (s + 1 < S) {
+            const int nb = (s + 1) % L::NST;
+            if (s + 1 >= L::NST) {   // the MMAs of stage s+1-NST read buffer nb
+                const bool ok = tc::bar_wait(bar_a + 8u * (uint32_t)nb, (uint32_t)(((s + 1 - L::NST) / L::NST) & 1));
+                if (__syncthreads_or(!ok)) {
+                    failed = true;
+                    break;
+                }
+            }
+            fetch(s + 1, nb);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");   // stage s has landed
+        } else {
+            tc::cp_wait_all();
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t xs = base_a + (uint32_t)(buf * L::STAGE), gs = xs + (uint32_t)L::X_BYTES;
+#pragma unroll
+            for (int dw = 0; dw < 3; ++dw) {
+#pragma unroll
+                for (int kc = 0; kc < kTileP / 16; ++kc) {
+                    const uint32_t xa = xs + (uint32_t)((16 * kc + dw) * 16);   // slot pixel 0 is w0 - 1
+                    const uint32_t ga = gs + (uint32_t)(16 * kc * 16);
+                    const uint64_t xd = tc::sdesc(xa, 128, tc::kPixS * 16), gd = tc::sdesc(ga, 128, kTileP * 16);
+                    tc::mma(tmem + (uint32_t)(dw * N), L::A_IS_G ? gd : xd, L::A_IS_G ? xd : gd, tc::idesc_mn<N>(),
+                            (s > 0 || kc > 0) ? 1u : 0u);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             bar_a + 8u * (uint32_t)buf)
+                         : "memory");
+        }
+        issued = s + 1;
+    }
+    // the last issued stage's commit covers every earlier MMA of this thread
+    bool ok = true;
+    if (issued > 0) {
+        const int ls = issued - 1;
+        ok = tc::bar_wait(bar_a + 8u * (uint32_t)(ls % L::NST), (uint32_t)((ls / L::NST) & 1));
+    }
+    if (__syncthreads_or(!ok) || failed) {
+        if (threadIdx.x == 0) atomicOr(err, 4);
+        failed = true;
+    }
+    if (!failed) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        // warp w reads TMEM lanes 32 (w % 4) ..; its threads 0..15 hold rows m = 16 (w % 4) + lane,
+        // and the two warps of a sub-partition split the N columns
+        const int m = 16 * (warp % 4) + lane;
+        const int c0 = (warp / 4) * (N / 2);
+#pragma unroll
+        for (int dw = 0; dw < 3; ++dw) {
+            const int tap = 3 * dhi + dw;
+            float* out = part + ((size_t)chunk * 9 + tap) * COUT * CIN;
+#pragma unroll
+            for (int c = 0; c < N / 2; c += 8) {
+                float v[8];
+                tc::tmem_ld8(tmem + ((uint32_t)(32 * (warp % 4)) << 16) + (uint32_t)(dw * N + c0 + c), v);
+                if (lane < 16) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int col = c0 + c + j;
+                        if constexpr (L::A_IS_G) out[(size_t)m * CIN + col] = v[j];          // D[n][k]
+                        else if (m < CIN) out[(size_t)col * CIN + m] = v[j];                 // D[k][n]
+                    }
+                }
+            }
+        }
+    }
+    tc::cp_wait_all();
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)L::TMEM_COLS));
+    }
+}
+
 template <int CIN, int COUT>
 constexpr int conv_smem() {
     return (9 * COUT + 3 * (kTileP + 2)) * RowPad<CIN>::LD * 2;
@@ -1055,10 +1250,17 @@ cudaError_t launch_conv(qgn_cnn* n, int cin, int cout, const __nv_bfloat16* x, c
 template <int CIN, int COUT>
 cudaError_t launch_wgrad_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat16* g, int batch, float* part,
                            int* nchunks) {
-    constexpr int SM = wgrad_smem<CIN, COUT>();
-    if (cudaError_t e = smem_opt_in(k_wgrad<CIN, COUT>, SM); e != cudaSuccess) return e;
     const int chunks = (batch * n->H + kWChunkRows - 1) / kWChunkRows;
     *nchunks = chunks;
+    if (n->engine != 1) {   // tcgen05: one CTA per (row chunk, tap row), the three taps in TMEM
+        constexpr int SM = tc::WgLay<CIN, COUT>::SMEM;
+        if (cudaError_t e = smem_opt_in(k_wgrad_tc<CIN, COUT>, SM); e != cudaSuccess) return e;
+        ::qgn::launch(k_wgrad_tc<CIN, COUT>, dim3(chunks, 3), kThreads, SM, n->stream, x, g, batch, n->H, n->W, part,
+                      n->d_err);
+        return cudaGetLastError();
+    }
+    constexpr int SM = wgrad_smem<CIN, COUT>();
+    if (cudaError_t e = smem_opt_in(k_wgrad<CIN, COUT>, SM); e != cudaSuccess) return e;
     ::qgn::launch(k_wgrad<CIN, COUT>, dim3(chunks, 9), kThreads, SM, n->stream, x, g, batch, n->H, n->W, part);
     return cudaGetLastError();
 }
@@ -1136,8 +1338,9 @@ int check_err(qgn_cnn* net) {
         net->fused_tiles = -1;   // the layer counters may be uneven: the next fused launch clears them
         NCK(cudaMemsetAsync(net->d_err, 0, sizeof(int), net->stream));   // reported once
         return cnn_err(net, QGN_ERR_CUDA,
-                       (h & 2) ? "the fused inference timed out waiting for a neighbouring row"
-                               : "a tensor-core convolution timed out waiting for its MMAs");
+                       (h & 2)   ? "the fused inference timed out waiting for a neighbouring row"
+                       : (h & 4) ? "a tensor-core weight gradient timed out waiting for its MMAs"
+                                 : "a tensor-core convolution timed out waiting for its MMAs");
     }
     return QGN_OK;
 }
