@@ -237,6 +237,15 @@ int qgn_ens_advance(qgn_ens* ens, int nsteps);
 /* autotuner's choice for pass 0 (y-inverse), 1 (x pass), 2 (y-forward): CTA threads,
  * CTAs per SM of the persistent grid (0 = one CTA per tile) and the timed ms per launch */
 int qgn_ens_tuning(qgn_ens* ens, int pass, int* threads, int* ctas_per_sm, float* ms);
+/* the autotuner's FFT radix for the pass: elements per thread of its transforms (8, 16 or 32;
+ * a transform of n points runs on n / that many threads, in radix passes of that size) */
+int qgn_ens_fft_radix(qgn_ens* ens, int pass, int* elements_per_thread);
+/* pin a pass to one tile variant instead of tuning it: CTA threads (as qgn_ens_tuning reports
+ * them), elements per thread and CTAs per SM (0 = one CTA per tile).  Variants: y-inverse
+ * 64/128/256 threads at 16 or 8 elements, x pass 96/192/384 at 16 and 192/384 at 8, y-forward
+ * 64/128/256 at 16 and 128/256 at 8; QGN_PREC_MIXED adds 32 elements (y-inverse 64/128/256,
+ * x pass 96/192/384, y-forward 64/128).  QGN_ERR_CONFIG for any other combination. */
+int qgn_ens_set_tiles(qgn_ens* ens, int pass, int threads, int elements_per_thread, int ctas_per_sm);
 int qgn_ens_profile_enable(qgn_ens* ens, int enable);
 int qgn_ens_profile_read(qgn_ens* ens, int kernel, double* total_ms, double* bytes,
                          long long* timed_launches, long long* launches);

@@ -99,6 +99,8 @@ SIGNATURES = {
     "qgn_ens_advance": (C.c_int, [C.c_void_p, C.c_int]),
     "qgn_ens_tuning": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                  C.POINTER(C.c_float)]),
+    "qgn_ens_fft_radix": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "qgn_ens_set_tiles": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "qgn_ens_profile_enable": (C.c_int, [C.c_void_p, C.c_int]),
     "qgn_ens_profile_read": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_longlong),
                                        C.POINTER(C.c_longlong)]),

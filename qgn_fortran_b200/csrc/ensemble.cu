@@ -29,6 +29,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <unordered_set>
 #include <vector>
@@ -68,8 +69,49 @@ struct EnsMember {
 enum { EP_POINT = 0, EP_ELEM, EP_YINV, EP_XPASS, EP_YFWD, EP_YINV1, EP_XINV1, EP_COUNT };
 // passes the autotuner chooses for
 enum { TP_YINV = 0, TP_XPASS, TP_YFWD, TP_COUNT };
-constexpr int kTileVariants[TP_COUNT][3] = {{64, 128, 256}, {32, 64, 128}, {64, 128, 256}};
+// Tile variants the autotuner searches per pass: CTA width (threads of a y pass, threads per
+// slot group of the x pass) and elements per thread of the transforms (tv_make, rhs_tiles.cuh).
+// Every listed pair gives whole tiles for 128-, 256- and 512-point transforms (the y-forward
+// needs a width of at least two transforms, the others one); 32 elements per thread only in
+// FP32, where they take 64 registers (FP64 would spill under the 128-register cap).  Index 1 is
+// the default before tuning (16 elements per thread).
+template <class CT>
+struct EnsVariants;
+template <>
+struct EnsVariants<double2> {
+    static constexpr int yinv[] = {tv_make(64, 16), tv_make(128, 16), tv_make(256, 16),
+                                   tv_make(64, 8),  tv_make(128, 8),  tv_make(256, 8)};
+    static constexpr int xpass[] = {tv_make(32, 16), tv_make(64, 16), tv_make(128, 16), tv_make(64, 8),
+                                    tv_make(128, 8)};
+    static constexpr int yfwd[] = {tv_make(64, 16), tv_make(128, 16), tv_make(256, 16), tv_make(128, 8),
+                                   tv_make(256, 8)};
+};
+template <>
+struct EnsVariants<float2> {
+    static constexpr int yinv[] = {tv_make(64, 16), tv_make(128, 16), tv_make(256, 16), tv_make(64, 8),
+                                   tv_make(128, 8),  tv_make(256, 8),  tv_make(64, 32),  tv_make(128, 32),
+                                   tv_make(256, 32)};
+    static constexpr int xpass[] = {tv_make(32, 16), tv_make(64, 16), tv_make(128, 16), tv_make(64, 8),
+                                    tv_make(128, 8), tv_make(32, 32), tv_make(64, 32),  tv_make(128, 32)};
+    static constexpr int yfwd[] = {tv_make(64, 16), tv_make(128, 16), tv_make(256, 16), tv_make(128, 8),
+                                   tv_make(256, 8), tv_make(64, 32),  tv_make(128, 32)};
+};
+template <class CT>
+constexpr int ens_variant_count(int tp) {
+    return tp == 0 ? (int)(sizeof(EnsVariants<CT>::yinv) / sizeof(int))
+                   : tp == 1 ? (int)(sizeof(EnsVariants<CT>::xpass) / sizeof(int))
+                             : (int)(sizeof(EnsVariants<CT>::yfwd) / sizeof(int));
+}
+template <class CT>
+constexpr int ens_variant(int tp, int v) {
+    return tp == 0 ? EnsVariants<CT>::yinv[v] : tp == 1 ? EnsVariants<CT>::xpass[v] : EnsVariants<CT>::yfwd[v];
+}
 constexpr int kDefaultVariant = 1;
+// register cap of an ensemble transform kernel: 32 FP32 elements per thread need 64 for data
+template <class CT, int TV>
+__host__ __device__ constexpr int ens_regcap() {
+    return tv_radix(TV) == 32 ? 128 : regcap<CT>(128, 96);
+}
 constexpr int kPointTile = 256;
 
 __device__ __forceinline__ int ens_find(const int* __restrict__ start, int nm, int t) {
@@ -192,7 +234,7 @@ __global__ void __launch_bounds__(256, 2) k_ens_stage(const EnsMember* __restric
 template <int N, class CT, int TV>
 __device__ __noinline__ void ens_yinv_one(const EnsMember& M, const Geom& g, int local, int s) {
     using C = YInvCfg<N, CT, TV>;
-    static_assert(C::THREADS == TV, "y-inverse tile width must give TV threads");
+    static_assert(C::THREADS == tv_width(TV), "y-inverse tile width must give TV threads");
     const int nbx = (g.nkx + C::TKX - 1) / C::TKX;
     yinv_tile<N, 3, CT, TV>(g, local % nbx, local / nbx, stage_input<CT>(M, s), static_cast<const CT*>(M.psi),
                             static_cast<CT*>(M.hq), static_cast<CT*>(M.hp), static_cast<CT*>(M.hu),
@@ -200,7 +242,7 @@ __device__ __noinline__ void ens_yinv_one(const EnsMember& M, const Geom& g, int
 }
 
 template <class CT, int TV>
-__global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
+__global__ void __launch_bounds__(tv_width(TV), minb(tv_width(TV), ens_regcap<CT, TV>()))
     k_ens_yinv(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
     QGN_PDL_ENTRY();
     const int total = start[nm];
@@ -223,7 +265,7 @@ __global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
 template <int N, class CT, int TV>
 __device__ __noinline__ void ens_xpass_one(const EnsMember& M, const Geom& g, int local) {
     using C = XCfg<N, false, CT, TV>;
-    static_assert(C::THREADS == 3 * TV, "x-pass tile width must give 3 TV threads");
+    static_assert(C::THREADS == 3 * tv_width(TV), "x-pass tile width must give 3 TV threads");
     const int nbx = (g.ny / 2 + C::RP - 1) / C::RP;
     xpass_tile<N, false, CT, TV>(g, local % nbx, local / nbx, static_cast<const CT*>(M.hq),
                                  static_cast<const CT*>(M.hp), static_cast<const CT*>(M.hu), static_cast<CT*>(M.hpp),
@@ -231,7 +273,7 @@ __device__ __noinline__ void ens_xpass_one(const EnsMember& M, const Geom& g, in
 }
 
 template <class CT, int TV>
-__global__ void __launch_bounds__(3 * TV, minb(3 * TV, regcap<CT>(128, 96)))
+__global__ void __launch_bounds__(3 * tv_width(TV), minb(3 * tv_width(TV), ens_regcap<CT, TV>()))
     k_ens_xpass(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
     QGN_PDL_ENTRY();
     const int total = start[nm];
@@ -254,7 +296,7 @@ __global__ void __launch_bounds__(3 * TV, minb(3 * TV, regcap<CT>(128, 96)))
 template <int N, class CT, int TV>
 __device__ __noinline__ void ens_yfwd_one(const EnsMember& M, const Geom& g, int local, int s) {
     using C = YFwdCfg<N, false, CT, TV>;
-    static_assert(C::THREADS == TV, "y-forward tile width must give TV threads");
+    static_assert(C::THREADS == tv_width(TV), "y-forward tile width must give TV threads");
     const int nbx = (g.nkx + C::TKX - 1) / C::TKX;
     yfwd_tile<N, false, CT, TV>(g, local % nbx, local / nbx, M.lc, stage_input<CT>(M, s),
                                 static_cast<const CT*>(M.psi), static_cast<const CT*>(M.hpp),
@@ -263,7 +305,7 @@ __device__ __noinline__ void ens_yfwd_one(const EnsMember& M, const Geom& g, int
 }
 
 template <class CT, int TV>
-__global__ void __launch_bounds__(TV, minb(TV, regcap<CT>(128, 96)))
+__global__ void __launch_bounds__(tv_width(TV), minb(tv_width(TV), ens_regcap<CT, TV>()))
     k_ens_yfwd(const EnsMember* __restrict__ mem, const int* __restrict__ start, int nm, int s) {
     QGN_PDL_ENTRY();
     const int total = start[nm];
@@ -449,17 +491,22 @@ constexpr int xinv1_smem() {
 
 int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// tiles of one member for a pass and tile-width variant
+// threads per transform of n points at t elements per thread (FFTShape)
+int fft_threads(int n, int t) { return n / std::min(n, t); }
+
+// tiles of one member for a pass and tile variant (the tile shapes of YInvCfg, XCfg, YFwdCfg)
 int member_tiles(const Geom& g, int pass, int tv) {
-    const int Gx = g.nx / 16, Gy = g.ny / 16;
+    const int w = tv_width(tv), r = tv_radix(tv) ? tv_radix(tv) : 16;
+    const int Gx = fft_threads(g.nx, r), Gy = fft_threads(g.ny, r);
+    const int G1x = g.nx / 16, G1y = g.ny / 16;   // the error transforms: 16 elements per thread
     switch (pass) {
         case EP_POINT: return ceil_div((long long)g.nkx * g.nky, kPointTile);
         case EP_ELEM: return ceil_div((long long)g.csize(), kPointTile);
-        case EP_YINV: return ceil_div(g.nkx, std::max(1, tv / Gy)) * g.nz;
-        case EP_XPASS: return ceil_div(g.ny / 2, std::max(1, tv / Gx)) * g.nz;
-        case EP_YFWD: return ceil_div(g.nkx, std::min(std::max(1, tv / (2 * Gy)), 16)) * g.nz;
-        case EP_YINV1: return ceil_div(g.nkx, 128 / Gy) * g.nz;
-        case EP_XINV1: return ceil_div(g.ny / 2, 128 / Gx) * g.nz;
+        case EP_YINV: return ceil_div(g.nkx, std::max(1, w / Gy)) * g.nz;
+        case EP_XPASS: return ceil_div(g.ny / 2, std::max(1, w / Gx)) * g.nz;
+        case EP_YFWD: return ceil_div(g.nkx, std::min(std::max(1, w / (2 * Gy)), 16)) * g.nz;
+        case EP_YINV1: return ceil_div(g.nkx, 128 / G1y) * g.nz;
+        case EP_XINV1: return ceil_div(g.ny / 2, 128 / G1x) * g.nz;
         default: return 0;
     }
 }
@@ -484,6 +531,7 @@ struct qgn_ens {
     int variant[TP_COUNT] = {kDefaultVariant, kDefaultVariant, kDefaultVariant};
     int grid_mode[TP_COUNT] = {0, 0, 0};   // 0: one CTA per tile; k > 0: k CTAs per SM, persistent
     float tuned_ms[TP_COUNT] = {0.f, 0.f, 0.f};
+    bool pinned[TP_COUNT] = {false, false, false};   // set by qgn_ens_set_tiles: not tuned
     bool tuned = false;
     bool graphs_off = false;
     cudaGraphExec_t gexec = nullptr;
@@ -519,7 +567,12 @@ int ens_err(qgn_ens* e, int code, const std::string& msg) {
 
 bool fp32(const qgn_ens* e) { return e->precision == QGN_PREC_MIXED; }
 
-int tv_of(const qgn_ens* e, int tp) { return kTileVariants[tp][e->variant[tp]]; }
+int tv_of(const qgn_ens* e, int tp) {
+    return fp32(e) ? ens_variant<float2>(tp, e->variant[tp]) : ens_variant<double2>(tp, e->variant[tp]);
+}
+int variant_count(const qgn_ens* e, int tp) {
+    return fp32(e) ? ens_variant_count<float2>(tp) : ens_variant_count<double2>(tp);
+}
 
 const int* start_of(const qgn_ens* e, int pass) { return e->d_start + (size_t)pass * (e->mem.size() + 1); }
 
@@ -603,7 +656,8 @@ int launch_yinv_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += sizeof(CT) * (2.0 * c->g.csize() + 3.0 * c->g.nz * c->g.ny * c->g.nkx);
     QGN_LAUNCH(KID_YINV, bytes, e->stream,
-               ::qgn::launch(k_ens_yinv<CT, TV>, grid, TV, SM, e->stream, e->d_mem, start_of(e, EP_YINV), (int)e->mem.size(), s));
+               ::qgn::launch(k_ens_yinv<CT, TV>, grid, tv_width(TV), SM, e->stream, e->d_mem, start_of(e, EP_YINV),
+                             (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
 }
@@ -615,7 +669,7 @@ int launch_xpass_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += 5.0 * sizeof(CT) * c->g.nz * c->g.ny * c->g.nkx;
     QGN_LAUNCH(KID_XPASS, bytes, e->stream,
-               ::qgn::launch(k_ens_xpass<CT, TV>, grid, 3 * TV, SM, e->stream, e->d_mem, start_of(e, EP_XPASS),
+               ::qgn::launch(k_ens_xpass<CT, TV>, grid, 3 * tv_width(TV), SM, e->stream, e->d_mem, start_of(e, EP_XPASS),
                                                                    (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
@@ -628,30 +682,41 @@ int launch_yfwd_tv(qgn_ens* e, int s, int grid) {
     double bytes = 0.0;
     for (qgn_ctx* c : e->mem) bytes += sizeof(CT) * c->g.nz * c->g.nkx * (2.0 * c->g.ny + 3.0 * c->g.nky);
     QGN_LAUNCH(KID_YFWD, bytes, e->stream,
-               ::qgn::launch(k_ens_yfwd<CT, TV>, grid, TV, SM, e->stream, e->d_mem, start_of(e, EP_YFWD), (int)e->mem.size(), s));
+               ::qgn::launch(k_ens_yfwd<CT, TV>, grid, tv_width(TV), SM, e->stream, e->d_mem, start_of(e, EP_YFWD),
+                             (int)e->mem.size(), s));
     ECK(cudaGetLastError());
     return QGN_OK;
+}
+
+// variant v of a pass: the I-th instantiation of the pass's list for I == v
+template <class CT, size_t... I>
+int launch_yinv_v(qgn_ens* e, int v, int s, std::index_sequence<I...>) {
+    int r = QGN_ERR_CONFIG;
+    const int grid = grid_for(e, EP_YINV, TP_YINV);
+    (void)((v == (int)I ? (r = launch_yinv_tv<CT, ens_variant<CT>(TP_YINV, (int)I)>(e, s, grid), true) : false) || ...);
+    return r;
+}
+template <class CT, size_t... I>
+int launch_xpass_v(qgn_ens* e, int v, int s, std::index_sequence<I...>) {
+    int r = QGN_ERR_CONFIG;
+    const int grid = grid_for(e, EP_XPASS, TP_XPASS);
+    (void)((v == (int)I ? (r = launch_xpass_tv<CT, ens_variant<CT>(TP_XPASS, (int)I)>(e, s, grid), true) : false) || ...);
+    return r;
+}
+template <class CT, size_t... I>
+int launch_yfwd_v(qgn_ens* e, int v, int s, std::index_sequence<I...>) {
+    int r = QGN_ERR_CONFIG;
+    const int grid = grid_for(e, EP_YFWD, TP_YFWD);
+    (void)((v == (int)I ? (r = launch_yfwd_tv<CT, ens_variant<CT>(TP_YFWD, (int)I)>(e, s, grid), true) : false) || ...);
+    return r;
 }
 
 template <class CT>
 int launch_pass(qgn_ens* e, int tp, int s) {
     const int v = e->variant[tp];
-    if (tp == TP_YINV) {
-        const int grid = grid_for(e, EP_YINV, tp);
-        if (v == 0) return launch_yinv_tv<CT, 64>(e, s, grid);
-        if (v == 1) return launch_yinv_tv<CT, 128>(e, s, grid);
-        return launch_yinv_tv<CT, 256>(e, s, grid);
-    }
-    if (tp == TP_XPASS) {
-        const int grid = grid_for(e, EP_XPASS, tp);
-        if (v == 0) return launch_xpass_tv<CT, 32>(e, s, grid);
-        if (v == 1) return launch_xpass_tv<CT, 64>(e, s, grid);
-        return launch_xpass_tv<CT, 128>(e, s, grid);
-    }
-    const int grid = grid_for(e, EP_YFWD, tp);
-    if (v == 0) return launch_yfwd_tv<CT, 64>(e, s, grid);
-    if (v == 1) return launch_yfwd_tv<CT, 128>(e, s, grid);
-    return launch_yfwd_tv<CT, 256>(e, s, grid);
+    if (tp == TP_YINV) return launch_yinv_v<CT>(e, v, s, std::make_index_sequence<ens_variant_count<CT>(TP_YINV)>{});
+    if (tp == TP_XPASS) return launch_xpass_v<CT>(e, v, s, std::make_index_sequence<ens_variant_count<CT>(TP_XPASS)>{});
+    return launch_yfwd_v<CT>(e, v, s, std::make_index_sequence<ens_variant_count<CT>(TP_YFWD)>{});
 }
 
 template <class CT>
@@ -726,9 +791,10 @@ int autotune(qgn_ens* e) {
     int rc = QGN_OK;
     const int grid_modes[4] = {0, 2, 4, 8};
     for (int tp = 0; tp < TP_COUNT && rc == QGN_OK; ++tp) {
+        if (e->pinned[tp]) continue;
         float best = 1e30f;
         int bv = kDefaultVariant, bg = 0;
-        for (int v = 0; v < 3 && rc == QGN_OK; ++v) {
+        for (int v = 0; v < variant_count(e, tp) && rc == QGN_OK; ++v) {
             e->variant[tp] = v;
             build_tables(e);
             rc = upload_tables(e);
@@ -978,11 +1044,41 @@ int qgn_ens_advance(qgn_ens* e, int nsteps) {
 
 int qgn_ens_tuning(qgn_ens* e, int pass, int* threads, int* ctas_per_sm, float* ms) {
     if (!e || pass < 0 || pass >= TP_COUNT) return QGN_ERR_ARG;
-    const int tv = tv_of(e, pass);
-    if (threads) *threads = pass == TP_XPASS ? 3 * tv : tv;
+    const int w = tv_width(tv_of(e, pass));
+    if (threads) *threads = pass == TP_XPASS ? 3 * w : w;
     if (ctas_per_sm) *ctas_per_sm = e->grid_mode[pass];
     if (ms) *ms = e->tuned_ms[pass];
     return QGN_OK;
+}
+
+int qgn_ens_fft_radix(qgn_ens* e, int pass, int* elements_per_thread) {
+    if (!e || !elements_per_thread || pass < 0 || pass >= TP_COUNT) return QGN_ERR_ARG;
+    const int r = tv_radix(tv_of(e, pass));
+    *elements_per_thread = r ? r : 16;
+    return QGN_OK;
+}
+
+int qgn_ens_set_tiles(qgn_ens* e, int pass, int threads, int elements_per_thread, int ctas_per_sm) {
+    if (!e || pass < 0 || pass >= TP_COUNT || ctas_per_sm < 0 || ctas_per_sm > 64) return QGN_ERR_ARG;
+    const int w = pass == TP_XPASS ? threads / 3 : threads;
+    if (pass == TP_XPASS && threads % 3 != 0) return ens_err(e, QGN_ERR_CONFIG, "x-pass threads: three slot groups");
+    for (int v = 0; v < variant_count(e, pass); ++v) {
+        const int tv = fp32(e) ? ens_variant<float2>(pass, v) : ens_variant<double2>(pass, v);
+        if (tv_width(tv) == w && (tv_radix(tv) ? tv_radix(tv) : 16) == elements_per_thread) {
+            e->variant[pass] = v;
+            e->grid_mode[pass] = ctas_per_sm;
+            e->pinned[pass] = true;
+            e->tuned_ms[pass] = 0.f;
+            build_tables(e);
+            if (e->gexec) {   // the captured graph holds the old launches
+                ECK(cudaStreamSynchronize(e->stream));
+                cudaGraphExecDestroy(e->gexec);
+                e->gexec = nullptr;
+            }
+            return QGN_OK;
+        }
+    }
+    return ens_err(e, QGN_ERR_CONFIG, "no tile variant with these threads and elements per thread");
 }
 
 int qgn_ens_profile_enable(qgn_ens* e, int on) {

@@ -3,6 +3,7 @@
 
 #include "../../include/qgn_gpu.h"
 #include "../../include/qgn_probe.h"
+#include "launch.cuh"
 
 namespace {
 
@@ -14,6 +15,7 @@ constexpr int kIters = 2048;     // iterations of kChains FMAs: ~40 GFLOP per la
 // a <- a*b + c on kChains registers; b and c are launch arguments, so nothing folds, and every
 // thread stores its sum, so no chain is dead.  With b < 1 the chains converge to c/(1-b).
 __global__ void __launch_bounds__(kThreads) k_fp64_fma(double* __restrict__ out, int iters, double b, double c) {
+    QGN_PDL_ENTRY();
     double a[kChains];
 #pragma unroll
     for (int i = 0; i < kChains; ++i) a[i] = 1.0e-3 * threadIdx.x + i;
@@ -59,8 +61,7 @@ extern "C" int qgn_probe_fp64_fma(int reps, double* tflops, double* ms) {
     float best = -1.0f;
     for (int r = 0; r < reps + 2; ++r) {
         if (cudaEventRecord(c.e0, c.st) != cudaSuccess) return QGN_ERR_CUDA;
-        k_fp64_fma<<<grid, kThreads, 0, c.st>>>(c.out, kIters, b, cc);
-        if (cudaGetLastError() != cudaSuccess) return QGN_ERR_CUDA;
+        if (::qgn::launch(k_fp64_fma, grid, kThreads, 0, c.st, c.out, kIters, b, cc) != cudaSuccess) return QGN_ERR_CUDA;
         if (cudaEventRecord(c.e1, c.st) != cudaSuccess) return QGN_ERR_CUDA;
         if (cudaEventSynchronize(c.e1) != cudaSuccess) return QGN_ERR_CUDA;
         float t = 0.0f;

@@ -50,8 +50,16 @@ __host__ __device__ constexpr int regcap(int fp64 = 128, int fp32 = 64) { return
 // registers), 16 otherwise.  The y passes keep 16 in FP32: their CTAs interleave columns
 // across warps, and at 32 elements they had half the threads per column and ran 1.3-1.7x
 // slower on B200.
+// A non-zero tile-variant code carries the CTA width in its low 16 bits and, above them, the
+// elements per thread of its transforms (8, 16 or 32; 0 there means 16): the ensemble's
+// autotuner searches both.
+__host__ __device__ constexpr int tv_width(int tv) { return tv & 0xFFFF; }
+__host__ __device__ constexpr int tv_radix(int tv) { return tv >> 16; }
+__host__ __device__ constexpr int tv_make(int width, int radix) { return width | (radix << 16); }
 template <class CT, int N, int TV>
-__host__ __device__ constexpr int fft_tp() { return (TV == 0 && (N == 512 || N == 1024)) ? 32 : 16; }
+__host__ __device__ constexpr int fft_tp() {
+    return TV == 0 ? ((N == 512 || N == 1024) ? 32 : 16) : (tv_radix(TV) ? tv_radix(TV) : 16);
+}
 // elements per thread of a y transform: 8 for the FP64 512- and 1024-point columns of the
 // single-field launches, 16 otherwise.  Half the registers per thread (64, two 512-thread CTAs
 // per SM) doubles the resident warps of these latency-bound kernels at the price of a fourth
@@ -61,7 +69,9 @@ __host__ __device__ constexpr int fft_tp() { return (TV == 0 && (N == 512 || N =
 #define QGN_Y_TP64 8
 #endif
 template <class CT, int N, int TV>
-__host__ __device__ constexpr int fft_tp_y() { return (TV == 0 && sizeof(CT) == 16 && N >= 512) ? QGN_Y_TP64 : 16; }
+__host__ __device__ constexpr int fft_tp_y() {
+    return TV == 0 ? ((sizeof(CT) == 16 && N >= 512) ? QGN_Y_TP64 : 16) : (tv_radix(TV) ? tv_radix(TV) : 16);
+}
 // Row pairs per CTA of the single-field x pass with one warp per transform (a build-time tuning
 // knob).  One row pair (three warps, 96 threads, four CTAs per SM at 168 registers) couples only
 // the three warps of a pair at the barrier between the inverse and forward transforms: the
@@ -74,7 +84,7 @@ template <int NY, class CT = double2, int TV = 0>
 struct YInvCfg {
     static constexpr int TP = fft_tp_y<CT, NY, TV>();
     static constexpr int G = FFTShape<NY, TP>::G;
-    static constexpr int TKX = TV == 0 ? cmin(cmax(4, 128 / G), 16) : cmax(1, TV / G);
+    static constexpr int TKX = TV == 0 ? cmin(cmax(4, 128 / G), 16) : cmax(1, tv_width(TV) / G);
     static constexpr int THREADS = TKX * G;
     static constexpr int TS = slot_stride(NY, interleave_target(TKX, (int)sizeof(CT)), (int)sizeof(CT), TP);
     static constexpr int SMEM = TKX * TS * (int)sizeof(CT);
@@ -90,7 +100,7 @@ template <int NX, bool DRAG, class CT = double2, int TV = 0>
 struct XCfg {
     static constexpr int TP = fft_tp<CT, NX, TV>();
     static constexpr int G = FFTShape<NX, TP>::G;
-    static constexpr int RP = (TV == 0 && G == 32) ? QGN_X_ROWPAIRS : cmax(1, (TV == 0 ? 64 : TV) / G);   // row pairs per CTA
+    static constexpr int RP = (TV == 0 && G == 32) ? QGN_X_ROWPAIRS : cmax(1, (TV == 0 ? 64 : tv_width(TV)) / G);   // row pairs per CTA
     static constexpr int SP = DRAG ? 4 : 3;             // slots per row pair
     static constexpr int THREADS = SP * RP * G;
     static constexpr int TS = slot_stride(NX, 2, (int)sizeof(CT), TP);
@@ -102,7 +112,7 @@ struct YFwdCfg {
     static constexpr int TP = fft_tp_y<CT, NY, TV>();
     static constexpr int G = FFTShape<NY, TP>::G;
     // tid ^ TKX stays in the warp
-    static constexpr int TKX = TV == 0 ? cmin(cmax(2, 64 / G), 16) : cmin(cmax(1, TV / (2 * G)), 16);
+    static constexpr int TKX = TV == 0 ? cmin(cmax(2, 64 / G), 16) : cmin(cmax(1, tv_width(TV) / (2 * G)), 16);
     static constexpr int SLOTS = 2 * TKX;
     static constexpr int THREADS = SLOTS * G;
     static constexpr int TS = slot_stride(NY, interleave_target(SLOTS, (int)sizeof(CT)), (int)sizeof(CT), TP);

@@ -314,8 +314,17 @@ class QGNEnsemble:
             th, cps, ms = C.c_int(), C.c_int(), C.c_float()
             self._check(self.lib.qgn_ens_tuning(self.ens, i, C.byref(th), C.byref(cps), C.byref(ms)),
                         "qgn_ens_tuning")
-            out[name] = {"threads": th.value, "ctas_per_sm": cps.value, "ms": ms.value}
+            rad = C.c_int()
+            self._check(self.lib.qgn_ens_fft_radix(self.ens, i, C.byref(rad)), "qgn_ens_fft_radix")
+            out[name] = {"threads": th.value, "ctas_per_sm": cps.value, "ms": ms.value,
+                         "elements_per_thread": rad.value}
         return out
+
+    def set_tiles(self, pass_name: str, threads: int, elements_per_thread: int, ctas_per_sm: int = 0):
+        """Pin a right-hand-side pass to one tile variant (the autotuner then leaves it alone)."""
+        i = self.PASSES.index(pass_name)
+        self._check(self.lib.qgn_ens_set_tiles(self.ens, i, int(threads), int(elements_per_thread),
+                                               int(ctas_per_sm)), "qgn_ens_set_tiles")
 
     def profile_enable(self, on: bool = True):
         self._check(self.lib.qgn_ens_profile_enable(self.ens, int(bool(on))), "qgn_ens_profile_enable")

@@ -69,17 +69,22 @@ def test_fp64_ensemble_equals_single_contexts(cuda_ok):
     ens = QGNEnsemble(gs, precision="fp64")
     ens.advance(4)
     ens.advance(3)      # the FSAL RHS0 and the captured graph carry over between calls
+    tune = ens.tuning()
+    radix16 = all(v["elements_per_thread"] == 16 for v in tune.values())
     for w, g, q in zip(ws, gs, q0):
         got = g.get_state()
         t, dt = g.time()
         ref, tr, dr = single_run(w, q, 7)
         # a single context transforms 512- and 1024-point y columns with 8 elements per thread
-        # and rows with 32, the ensemble's tiles with 16: same transform, different roundoff,
-        # which the adaptive dt carries along (the adaptive tolerance of the oracle comparisons)
-        tol = 1e-9 if max(w.params["nx"], w.params["ny"]) >= 512 else 1e-13
+        # and rows with 32, the ensemble's tiles with 16 unless the autotuner chose 8 or 32: the
+        # same transform with another radix schedule, whose roundoff the adaptive dt carries
+        # along (the adaptive tolerance of the oracle comparisons)
+        if max(w.params["nx"], w.params["ny"]) >= 512:
+            tol = 1e-9
+        else:
+            tol = 1e-13 if radix16 else 1e-11
         assert np.all(layer_rel(got, ref) <= tol), w.name
         assert t == pytest.approx(tr, rel=tol) and dt == pytest.approx(dr, rel=tol), w.name
-    tune = ens.tuning()
     assert tune["yinv"]["threads"] in (64, 128, 256)
     assert tune["xpass"]["threads"] in (96, 192, 384)
     assert tune["yfwd"]["threads"] in (64, 128, 256)
@@ -175,3 +180,60 @@ def test_create_rejects_unsupported_members(cuda_ok):
     with pytest.raises(QGNError) as ei:
         QGNEnsemble([g, g])
     assert ei.value.code == QGN_ERR_ARG
+
+
+# every tile variant the autotuner can choose (qgn_ens_set_tiles): CTA threads, elements per thread
+VARIANTS = {
+    "fp64": {"yinv": [(64, 16), (128, 16), (256, 16), (64, 8), (128, 8), (256, 8)],
+             "xpass": [(96, 16), (192, 16), (384, 16), (192, 8), (384, 8)],
+             "yfwd": [(64, 16), (128, 16), (256, 16), (128, 8), (256, 8)]},
+    "mixed": {"yinv": [(64, 16), (128, 16), (256, 16), (64, 8), (128, 8), (256, 8), (64, 32), (128, 32),
+                       (256, 32)],
+              "xpass": [(96, 16), (192, 16), (384, 16), (192, 8), (384, 8), (96, 32), (192, 32), (384, 32)],
+              "yfwd": [(64, 16), (128, 16), (256, 16), (128, 8), (256, 8), (64, 32), (128, 32)]},
+}
+
+
+def variant_set():
+    """128-, 256- and 512-point transforms along both x and y, fixed dt."""
+    ws = [rect_member(128, 128, 2, 81), rect_member(512, 128, 2, 82), rect_member(128, 512, 3, 83),
+          rect_member(256, 256, 2, 84)]
+    for w in ws:
+        w.params["TOL"] = 1.0e30
+        w.params["dt_max"] = 1800.0
+    return ws
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_tile_variant_matches(cuda_ok, monkeypatch, precision):
+    """Each pass pinned to each of its tile variants (the others at their defaults, no tuning):
+    FP64 equals single-context runs within the roundoff of another radix schedule, and the mixed
+    ensemble its own default variant within FP32 roundoff; the pinned choice is reported back."""
+    monkeypatch.setenv("QGN_NO_AUTOTUNE", "1")
+    ws = variant_set()
+    nsteps = 2
+    if precision == "fp64":
+        _, q0 = contexts(ws)
+        refs = [single_run(w, q, nsteps)[0] for w, q in zip(ws, q0)]
+        tol = 1e-12
+    else:
+        gs, _ = contexts(ws)
+        QGNEnsemble(gs, precision="mixed").advance(nsteps)
+        refs = [g.get_state() for g in gs]
+        tol = 1e-5
+    for pname, variants in VARIANTS[precision].items():
+        for threads, ept in variants:
+            gs, _ = contexts(ws)
+            ens = QGNEnsemble(gs, precision=precision)
+            ens.set_tiles(pname, threads, ept)
+            ens.advance(nsteps)
+            tune = ens.tuning()[pname]
+            assert (tune["threads"], tune["elements_per_thread"]) == (threads, ept)
+            for w, g, ref in zip(ws, gs, refs):
+                err = layer_rel(g.get_state(), ref)
+                assert np.all(err <= tol), (pname, threads, ept, w.name, err)
+    gs, _ = contexts(ws)
+    ens = QGNEnsemble(gs, precision=precision)
+    with pytest.raises(QGNError) as ei:
+        ens.set_tiles("yfwd", 64, 8)          # two 512-point transforms need 128 threads
+    assert ei.value.code == QGN_ERR_CONFIG
