@@ -118,6 +118,60 @@ __device__ __forceinline__ CT rot_root(CT a, int k) {
     else return rot16<DIR>(a, k * (16 / R));
 }
 
+// cos and sin of 2 pi k / R for the non-trivial roots of the radix-2 butterflies
+// (R = 8, 16, 32; 0 < k < R/2, k != R/4), from the first-octant constants
+__host__ __device__ constexpr double root_cos(int R, int k) {
+    const int m = k * (32 / R);   // angle in units of pi/16, 0 < m < 16, m != 8
+    constexpr double c[9] = {1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+                             0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+                             0.19509032201612826785, 0.0};
+    return m <= 8 ? c[m] : -c[16 - m];
+}
+__host__ __device__ constexpr double root_sin(int R, int k) {
+    const int m = k * (32 / R);
+    constexpr double c[9] = {1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+                             0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+                             0.19509032201612826785, 0.0};
+    return m <= 8 ? c[8 - m] : c[m - 8];
+}
+
+// Radix-2 butterfly (e + w o, e - w o), w = exp(DIR 2 pi i k / R), k a compile-time constant
+// after unrolling.  Trivial roots (k = 0: w = 1; k = R/4: w = DIR i) are additions; the others
+// use the tangent form: with |c| >= |s|, w o = c (o.x - t o.y, o.y + t o.x), t = s/c, and with
+// |s| > |c|, w o = s (r o.x - o.y, o.x + r o.y), r = c/s -- two FMAs for the scaled product and
+// one per output component, six in all against eight for product then sum and difference, and
+// at most two roundings per output (|t|, |r| <= 1).
+template <int R, int DIR, class CT>
+__device__ __forceinline__ void bfly(CT& a, CT& b, int k) {
+    using T = typename CTraits<CT>::R;
+    const CT e = a, o = b;
+    if (k == 0) {
+        a = cadd(e, o);
+        b = csub(e, o);
+        return;
+    }
+    if (4 * k == R) {   // w o = DIR i o
+        const CT t = DIR > 0 ? cmk<CT>(-o.y, o.x) : cmk<CT>(o.y, -o.x);
+        a = cadd(e, t);
+        b = csub(e, t);
+        return;
+    }
+    const double c = root_cos(R, k), s = DIR * root_sin(R, k);
+    const bool cdom = (c < 0 ? -c : c) >= (s < 0 ? -s : s);
+    const T f = (T)(cdom ? c : s);                 // common factor
+    const T t = (T)(cdom ? s / c : c / s);         // tangent or cotangent
+    T u, w;
+    if (cdom) {
+        u = fma(-t, o.y, o.x);
+        w = fma(t, o.x, o.y);
+    } else {
+        u = fma(t, o.x, -o.y);
+        w = fma(t, o.y, o.x);
+    }
+    a = cmk<CT>(fma(f, u, e.x), fma(f, w, e.y));
+    b = cmk<CT>(fma(-f, u, e.x), fma(-f, w, e.y));
+}
+
 // In-register DFT of length R (1,2,4,8,16,32), natural order in and out, sign DIR.
 template <int R, int DIR>
 struct RegDFT {
@@ -130,9 +184,10 @@ struct RegDFT {
         RegDFT<R / 2, DIR>::run(o);
 #pragma unroll
         for (int k = 0; k < R / 2; ++k) {
-            CT t = rot_root<R, DIR>(o[k], k);
-            v[k] = cadd(e[k], t);
-            v[k + R / 2] = csub(e[k], t);
+            CT x = e[k], y = o[k];
+            bfly<R, DIR>(x, y, k);
+            v[k] = x;
+            v[k + R / 2] = y;
         }
     }
 };
