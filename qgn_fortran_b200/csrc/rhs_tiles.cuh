@@ -407,13 +407,16 @@ __device__ __forceinline__ void xpass_tile(const Geom g, int bx, int l, const CT
     // ---- forward: slot 0 = u1 q1 + i v1 q1, 1 = u2 q2 + i v2 q2 (grid/(nx*ny) scaling as in
     //      QGN_Module.f90:229-235); with drag 2 = |u1|u1 + i|u1|v1, 3 = |u2|u2 + i|u2|v2
     const RT sc = (RT)g.inv_nxny;
+    const RT sc2 = sc * sc;   // nx, ny are powers of two: u (q sc^2) == (u sc)(q sc) exactly
     // this slot's row in the planes of the q, u, v slots (RT offsets 0, 2 TS, 4 TS)
     const RT* rows = reinterpret_cast<const RT*>(base) + ((s_of & 1) ? C::TS : 0);
     auto ld_fwd = [&](int x) -> CT {
-        const RT qv = rows[x] * sc;
+        if (s_of < 2) {
+            const RT qs = rows[x] * sc2;
+            return cmk<CT>(rows[2 * C::TS + x] * qs, rows[4 * C::TS + x] * qs);
+        }
         const RT uv = rows[2 * C::TS + x] * sc;
         const RT vv = rows[4 * C::TS + x] * sc;
-        if (s_of < 2) return cmk<CT>(uv * qv, vv * qv);
         const RT m = sqrt(uv * uv + vv * vv);   // URMS, QGN_Module.f90:285
         return cmk<CT>(m * uv, m * vv);
     };
