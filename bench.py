@@ -358,8 +358,9 @@ def ours_arm(args):
     if not args.no_ensemble:
         ensemble = ensemble_bench(args, ws)
 
-    # learned closure: 1024^2 x 4 truth -> 128^2 training data -> trained network -> 128^2 runs
-    # with QG-Leith and with the closure against the coarse-grained truth (KE spectrum, days/s)
+    # learned closure: a 1024^2 x 4 truth run -> 128^2 training data -> trained network -> 128^2
+    # runs with QG-Leith and with the closure against the coarse-grained truth of a second 1024^2
+    # x 4 run the network never saw (KE spectrum, days/s)
     closure = None
     if not args.no_closure:
         from qgn_fortran_b200.closure_experiment import run as run_closure

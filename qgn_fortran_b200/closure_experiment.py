@@ -4,11 +4,15 @@ closure compared against the coarse-grained truth on the KE spectrum and on days
 
 Inputs are synthetic: the exponential stratification restricted to 4 layers on a 2000 km
 square, the seeded random PV initial condition (peak wavenumber 16, rms 1e-6, seed 5),
-ARK43_QGLeith with PI.3.4 adaptive dt.  The truth is spun up for a model year before any
-sample is taken: while the initial condition decays, the subgrid statistics drift and a
-network trained on earlier samples does not carry to later ones.  Sizes (spin-up, samples,
-training steps, evaluation window) are arguments so the experiment can run at benchmark
-length or at full length (the named configuration: 10-year spin-up, 20k samples).
+ARK43_QGLeith with PI.3.4 adaptive dt.  Every truth run is spun up for a model year before
+any sample is taken: while the initial condition decays, the subgrid statistics drift and a
+network trained on earlier samples does not carry to later ones.  The training samples come
+from separate truth runs (other seeds of the same initial-condition generator), the 60-day
+evaluation from the seed-5 truth: the network is scored on a trajectory it never saw.  Sizes
+(spin-up, samples, training steps, evaluation window) are arguments, so the experiment runs at
+benchmark length (1024 samples from one run, 3000 Adam steps) or with the named
+configuration's 20 000 samples (five runs, 6000 Adam steps, a 12-day background:
+``--samples 20000 --every 2 --iters 6000 --train-seeds 6,7,8,9,10 --background-days 12``).
 
 ``python -m qgn_fortran_b200.closure_experiment`` prints the result as one JSON line.
 """
@@ -96,7 +100,16 @@ def _conv_tflops(net, batch):
 
 
 def run(truth_n=1024, coarse_n=128, nz=4, spinup_days=365.0, nsnap=1024, every=8, iters=3000, batch=32,
-        lr=1e-3, eval_days=60.0, sample_days=1.0, A8_background=None, energy_limit=1.0, seed=5, log=None):
+        lr=1e-3, eval_days=60.0, sample_days=1.0, A8_background=None, energy_limit=1.0, seed=5, log=None,
+        train_seed=(6,), window_samples=1024, window_every=8, background_days=3.0):
+    """By default the network trains on samples of a separate truth run (train_seed: the
+    initial condition of seed 6, the same spin-up; several seeds split the samples evenly), and
+    the evaluated truth (seed) takes the steps of the default sampling (window_samples every
+    window_every steps, discarded): the 60-day window is the same whatever the size of the
+    training set, and it lies on a trajectory the network never saw.  With train_seed None the
+    network trains on the evaluated truth itself, and the window starts where the sampling ends.
+    background_days: grid-scale e-folding time of the hyperviscosity kept under the network
+    (A8_background overrides it)."""
     import torch
 
     from . import QGNModule
@@ -112,7 +125,8 @@ def run(truth_n=1024, coarse_n=128, nz=4, spinup_days=365.0, nsnap=1024, every=8
     tol = 1.0e-6 * float(np.max(np.abs(qp)))
     out = {"truth": f"{truth_n}^2x{nz}", "coarse": f"{coarse_n}^2x{nz}", "scheme": "ark43_qgleith",
            "samples": nsnap, "every_steps": every, "train_iters": iters, "batch": batch,
-           "spinup_days": spinup_days, "eval_days": eval_days}
+           "spinup_days": spinup_days, "eval_days": eval_days, "background_days": background_days,
+           "training_truth": "the evaluated truth"}
     truth = QGNModule(_params(truth_n, nz, tol), H, S, U)
     truth.initialize(qp, 0.0, 750.0)
     t_wall = time.perf_counter()
@@ -126,7 +140,26 @@ def run(truth_n=1024, coarse_n=128, nz=4, spinup_days=365.0, nsnap=1024, every=8
     helper = QGNModule(pc, H, S, U)
     net = cl.ClosureNet(nz=nz, H=coarse_n, W=coarse_n, layers=6, max_batch=batch, seed=seed)
     t_wall = time.perf_counter()
-    x, y, isc, osc = cl.make_dataset(truth, helper, nsnap, every, net.cin_p, net.cout_p)
+    if train_seed is None:
+        x, y, isc, osc = cl.make_dataset(truth, helper, nsnap, every, net.cin_p, net.cout_p)
+    else:
+        seeds = [train_seed] if isinstance(train_seed, int) else list(train_seed)
+        out["training_truth"] = f"separate truth runs, seeds {seeds}"
+        xs, ys, isc, osc = [], [], None, None
+        for i, sd in enumerate(seeds):   # nsnap samples split evenly over the training runs
+            ni = nsnap // len(seeds) + (1 if i < nsnap % len(seeds) else 0)
+            src = QGNModule(_params(truth_n, nz, tol), H, S, U)
+            src.initialize(seeded_random_pv(truth_n, truth_n, nz, 16.0, 1.0e-6, sd), 0.0, 750.0)
+            _advance_to(src, spinup_days * DAY, chunk=100)
+            _timed_days_per_s(src, 200)      # the same path as the evaluated truth's
+            xi, yi, isc, osc = cl.make_dataset(src, helper, ni, every, net.cin_p, net.cout_p, isc, osc)
+            src.cleanup()
+            xs.append(xi)
+            ys.append(yi)
+        x, y = (xs[0], ys[0]) if len(xs) == 1 else (torch.cat(xs), torch.cat(ys))
+        del xs, ys
+        xw, yw, _, _ = cl.make_dataset(truth, helper, window_samples, window_every, net.cin_p, net.cout_p)
+        del xw, yw
     out["dataset_s"] = time.perf_counter() - t_wall
     ntr = int(0.9 * nsnap)
     t_wall = time.perf_counter()
@@ -156,10 +189,11 @@ def run(truth_n=1024, coarse_n=128, nz=4, spinup_days=365.0, nsnap=1024, every=8
     cl.coarse_grain(truth, leith)
     cl.coarse_grain(truth, learned)
     if A8_background is None:
-        # background hyperviscosity under the network: grid-scale e-folding of 3 days on the coarse
-        # grid.  Measured on B200 (same data and network): 10 days left 6.9 % mean spectrum error
-        # (QG-Leith 4.4 %), 3 days 3.0 %, 1 day 5.9 %
-        A8_background = 1.0 / (3.0 * DAY * (math.pi * coarse_n / pc["Lx"]) ** 8)
+        # background hyperviscosity under the network, a grid-scale e-folding time on the coarse
+        # grid.  The better the network, the less it needs (B200, the same 60-day window, QG-Leith
+        # 4.4 % mean spectrum error): 1024 samples, 3 / 5 / 8 days -> 2.7 / 4.1 / 5.5 %; 20 000
+        # samples from five runs, 3 / 8 / 12 / 20 days -> 5.0 / 2.6 / 2.3 / 2.3 %
+        A8_background = 1.0 / (background_days * DAY * (math.pi * coarse_n / pc["Lx"]) ** 8)
     cl.attach(learned, net, isc, osc, A8_background=A8_background, energy_limit=energy_limit)
     nbins = coarse_n // 3
     t0 = truth.time()[0]
@@ -211,10 +245,19 @@ def main():
     ap.add_argument("--iters", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--eval-days", type=float, default=60.0)
+    ap.add_argument("--train-seeds", type=str, default="6",
+                    help="comma-separated seeds: train on separate truth runs from these initial conditions "
+                         "(the samples split evenly); evaluate on the default window; 'none': train on the "
+                         "evaluated truth")
+    ap.add_argument("--background-days", type=float, default=3.0,
+                    help="grid-scale e-folding time of the background hyperviscosity under the network")
     args = ap.parse_args()
     import sys
     res = run(args.truth, args.coarse, args.nz, args.spinup_days, args.samples, args.every, args.iters, args.batch,
-              eval_days=args.eval_days, log=sys.stderr)
+              eval_days=args.eval_days, log=sys.stderr,
+              train_seed=None if args.train_seeds == "none" else [int(v) for v in args.train_seeds.split(",")],
+              background_days=args.background_days)
+    res.pop("ke_spectra", None)
     print(json.dumps(res))
 
 

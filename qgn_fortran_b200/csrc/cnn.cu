@@ -43,6 +43,16 @@ namespace cnn {
 constexpr int kTileP = 128;          // pixels per CTA tile (one row segment)
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
+// Warps of the tcgen05 convolutions (one CTA per SM either way: shared memory).  The fused
+// small-batch inference has one tile per CTA and per layer, with nothing to overlap its epilogue
+// (TMEM loads, bias, GELU, BF16 packing, staged stores), so 16 warps each drain 16 accumulator
+// columns: the 128^2 batch-1 inference ran 58.2 -> 53.7 us on B200.  The persistent layer kernel
+// overlaps each tile's epilogue with the next tile's MMAs and stays at 8 warps (16 made the
+// batch-32 forward 231 -> 228 TFLOP/s and a training step 3.92 -> 4.06 ms).
+constexpr int kTcWarps = 8;
+constexpr int kTcThreads = kTcWarps * 32;
+constexpr int kFusedWarps = 16;
+constexpr int kFusedThreads = kFusedWarps * 32;
 constexpr int kWChunkRows = 16;      // image rows per weight-gradient partial
 
 // EPI_PLANAR: as EPI_LINEAR but the FP32 output is planar, out[n][pixel] (the closure's input
@@ -503,21 +513,22 @@ __device__ __forceinline__ void issue_tile(uint32_t dacc, const uint32_t* ra, ui
 
 // a layer's weights [9][COUT][CIN] (BF16) into the K-major operand layout [9][CIN/8][COUT][8];
 // cin and cout are powers of two (16 or 64), so the index split is shifts and masks
+template <int NT>
 __device__ __forceinline__ void fetch_weights(const __nv_bfloat16* __restrict__ wt, int cin, int cout, uint32_t w) {
     const int c8n = cin >> 3;
     const int lc8 = __ffs(c8n) - 1, lco = __ffs(cout) - 1;
-    for (int i = threadIdx.x; i < 9 * cout * c8n; i += kThreads) {
+    for (int i = threadIdx.x; i < 9 * cout * c8n; i += NT) {
         const int c8 = i & (c8n - 1), n = (i >> lc8) & (cout - 1), tap = i >> (lc8 + lco);
         cp16(w + (uint32_t)(((tap * c8n + c8) * cout + n) * 16), wt + ((size_t)tap * cout + n) * cin + c8 * 8);
     }
 }
 
 // one input row (image b, row hh, pixels w0-1 .. w0+128 periodic) into a ring slot, asynchronously
-template <int CIN>
+template <int CIN, int NT>
 __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, int b, int hh, int H, int W, int w0,
                                          uint32_t slot_addr) {
     const size_t row = ((size_t)b * H + hh) * W;
-    for (int i = threadIdx.x; i < kPixS * (CIN / 8); i += kThreads) {
+    for (int i = threadIdx.x; i < kPixS * (CIN / 8); i += NT) {
         const int c8 = i % (CIN / 8), px = i / (CIN / 8);
         int ww = w0 - 1 + px;   // in [-1, W]: one periodic wrap at either end
         ww = ww < 0 ? ww + W : (ww >= W ? ww - W : ww);
@@ -531,20 +542,28 @@ __device__ __forceinline__ void fetch_row(const __nv_bfloat16* __restrict__ x, i
 // of columns, applies bias + GELU (or GELU' for the backward pass), and writes the tile through
 // XOR-swizzled shared-memory staging so that the global stores are contiguous 16-byte pieces.
 // The tile's outputs are contiguous in global memory: pixels p0 .. p0+127, COUT channels each.
-template <int CIN, int COUT, int EPI>
+// Columns of the accumulator each epilogue thread drains (NW warps: four TMEM sub-partitions,
+// NW/4 column blocks each when COUT = 64; four warps when COUT = 16) and the first of them.
+template <int COUT, int NW>
+__host__ __device__ constexpr int epi_ncol() { return COUT == 64 ? 64 / (NW / 4) : 16; }
+template <int COUT, int NW>
+__device__ __forceinline__ int epi_n0(int warp) { return COUT == 64 ? epi_ncol<COUT, NW>() * (warp / 4) : 0; }
+
+template <int CIN, int COUT, int EPI, int NW>
 __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const float* breg,
                                                  float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
                                                  const float* __restrict__ zin, unsigned char* stf, unsigned char* stb,
                                                  size_t npix) {
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    constexpr int NCOL = COUT == 64 ? 32 : 16;
+    constexpr int NCOL = epi_ncol<COUT, NW>();
+    constexpr int NT = NW * 32;
     constexpr int CF = COUT / 4;        // 16-byte pieces per staged FP32 row
     constexpr int CB = COUT / 8;        // 16-byte pieces per staged BF16 row
     const bool reads = COUT == 64 || warp < 4;
     const int px = 32 * (warp % 4) + lane;
-    const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+    const int n0 = epi_n0<COUT, NW>(warp);
     if (EPI == EPI_GELU_GRAD) {   // the tile's pre-activations, read contiguously
-        for (int i = threadIdx.x; i < kTileP * CF; i += kThreads) {
+        for (int i = threadIdx.x; i < kTileP * CF; i += NT) {
             const int r = i / CF, c = i % CF;
             *reinterpret_cast<float4*>(stf + (r * CF + (c ^ (r % CF))) * 16) =
                 *reinterpret_cast<const float4*>(zin + (p0 + r) * COUT + c * 4);
@@ -578,14 +597,14 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
     }
     __syncthreads();
     if (EPI == EPI_GELU || EPI == EPI_LINEAR) {
-        for (int i = threadIdx.x; i < kTileP * CF; i += kThreads) {
+        for (int i = threadIdx.x; i < kTileP * CF; i += NT) {
             const int r = i / CF, c = i % CF;
             *reinterpret_cast<float4*>(outf + (p0 + r) * COUT + c * 4) =
                 *reinterpret_cast<const float4*>(stf + (r * CF + (c ^ (r % CF))) * 16);
         }
     }
     if (EPI == EPI_PLANAR) {   // out[n][p0 + r]: each channel's 128 pixels are contiguous
-        for (int i = threadIdx.x; i < COUT * kTileP; i += kThreads) {
+        for (int i = threadIdx.x; i < COUT * kTileP; i += NT) {
             const int n = i / kTileP, r = i % kTileP;
             const int c = n / 4;
             outf[(size_t)n * npix + p0 + r] =
@@ -593,7 +612,7 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
         }
     }
     if (EPI == EPI_GELU || EPI == EPI_GELU_GRAD || EPI == EPI_GELU_ACT) {
-        for (int i = threadIdx.x; i < kTileP * CB; i += kThreads) {
+        for (int i = threadIdx.x; i < kTileP * CB; i += NT) {
             const int r = i / CB, c = i % CB;
             *reinterpret_cast<uint4*>(outb + (p0 + r) * COUT + c * 8) =
                 *reinterpret_cast<const uint4*>(stb + (r * CB + (c ^ (r % CB))) * 16);
@@ -605,7 +624,7 @@ __device__ __forceinline__ void conv_tc_epilogue(uint32_t tacc, size_t p0, const
 // epilogue drains tile t-1 from the other buffer, and the next tile's new input row is fetched
 // meanwhile.  Input rows live in a 6-slot ring.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kTcThreads, 1)
     k_conv_tc(const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ wt, const float* __restrict__ bias,
               int B, int H, int W, float* __restrict__ outf, __nv_bfloat16* __restrict__ outb,
               const float* __restrict__ zin, int* __restrict__ err) {
@@ -635,7 +654,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_a + 8));
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    tc::fetch_weights(wt, CIN, COUT, w_a);
+    tc::fetch_weights<kTcThreads>(wt, CIN, COUT, w_a);
     tc::cp_commit();
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -644,10 +663,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     unsigned char* stf = smtc + L::STF_OFF;
     unsigned char* stb = smtc + L::STB_OFF;
     // this thread's bias values (its columns are the same in every tile)
-    float breg[COUT == 64 ? 32 : 16];
+    constexpr int NCOL = epi_ncol<COUT, kTcWarps>();
+    float breg[NCOL];
     {
-        constexpr int NCOL = COUT == 64 ? 32 : 16;
-        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+        const int n0 = epi_n0<COUT, kTcWarps>(warp);
 #pragma unroll
         for (int j = 0; j < NCOL; ++j) breg[j] = (EPI == EPI_GELU_GRAD) ? 0.f : bias[n0 + j];
     }
@@ -676,14 +695,14 @@ __global__ void __launch_bounds__(kThreads, 1)
             } else {
                 sl[2] = next_slot;
                 next_slot = (next_slot + 1) % tc::kSlots;
-                tc::fetch_row<CIN>(x, b, (h + 1) % H, H, W, w0, in_a + (uint32_t)(sl[2] * L::SLOT_BYTES));
+                tc::fetch_row<CIN, kTcThreads>(x, b, (h + 1) % H, H, W, w0, in_a + (uint32_t)(sl[2] * L::SLOT_BYTES));
             }
         } else {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 sl[k] = next_slot;
                 next_slot = (next_slot + 1) % tc::kSlots;
-                tc::fetch_row<CIN>(x, b, (h + k - 1 + H) % H, H, W, w0, in_a + (uint32_t)(sl[k] * L::SLOT_BYTES));
+                tc::fetch_row<CIN, kTcThreads>(x, b, (h + k - 1 + H) % H, H, W, w0, in_a + (uint32_t)(sl[k] * L::SLOT_BYTES));
             }
         }
         pre_slot = -1;
@@ -704,7 +723,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if ((cont || t == t0) && t + 1 < t1 && (t + 1) / H == bs && h + 1 < H && H >= 3) {
             pre_slot = next_slot;
             next_slot = (next_slot + 1) % tc::kSlots;
-            tc::fetch_row<CIN>(x, b, (h + 2) % H, H, W, w0, in_a + (uint32_t)(pre_slot * L::SLOT_BYTES));
+            tc::fetch_row<CIN, kTcThreads>(x, b, (h + 2) % H, H, W, w0, in_a + (uint32_t)(pre_slot * L::SLOT_BYTES));
             tc::cp_commit();
         }
         // drain the previous tile while this one's MMAs run
@@ -717,7 +736,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 failed = true;
             } else {
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(pbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
+                conv_tc_epilogue<CIN, COUT, EPI, kTcWarps>(tmem + (uint32_t)(pbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
                                                  outf, outb, zin, stf, stb, (size_t)B * H * W);
             }
         }
@@ -738,7 +757,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             failed = true;
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            conv_tc_epilogue<CIN, COUT, EPI>(tmem + (uint32_t)(lbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
+            conv_tc_epilogue<CIN, COUT, EPI, kTcWarps>(tmem + (uint32_t)(lbuf * NACC), ((size_t)pb * H + ph) * W + pw0, breg,
                                              outf, outb, zin, stf, stb, (size_t)B * H * W);
         }
     }
@@ -823,14 +842,14 @@ __device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, in
     const int H = a.H, W = a.W;
     const __nv_bfloat16* src = l == 0 ? a.x : a.act[l];
     // the own row needs no wait: it is this CTA's previous output (or the input)
-    tc::fetch_row<CIN>(src, b, h, H, W, w0, in_a + (uint32_t)FL::SLOT_BYTES);
+    tc::fetch_row<CIN, kFusedThreads>(src, b, h, H, W, w0, in_a + (uint32_t)FL::SLOT_BYTES);
     tc::cp_commit();
     // the epilogue's bias columns, loaded while the rows and the MMAs are in flight
     const int warp = threadIdx.x / 32;
-    float breg[COUT == 64 ? 32 : 16];
+    constexpr int NCOL = epi_ncol<COUT, kFusedWarps>();
+    float breg[NCOL];
     {
-        constexpr int NCOL = COUT == 64 ? 32 : 16;
-        const int n0 = COUT == 64 ? 32 * (warp / 4) : 0;
+        const int n0 = epi_n0<COUT, kFusedWarps>(warp);
 #pragma unroll
         for (int j = 0; j < NCOL; ++j) breg[j] = a.bias[l][n0 + j];
     }
@@ -842,8 +861,8 @@ __device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, in
         tc::cp_wait_all();
         return false;
     }
-    tc::fetch_row<CIN>(src, b, (h - 1 + H) % H, H, W, w0, in_a);
-    tc::fetch_row<CIN>(src, b, (h + 1) % H, H, W, w0, in_a + 2u * (uint32_t)FL::SLOT_BYTES);
+    tc::fetch_row<CIN, kFusedThreads>(src, b, (h - 1 + H) % H, H, W, w0, in_a);
+    tc::fetch_row<CIN, kFusedThreads>(src, b, (h + 1) % H, H, W, w0, in_a + 2u * (uint32_t)FL::SLOT_BYTES);
     tc::cp_commit();
     tc::cp_wait_all();   // the rows and this layer's weights
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -863,12 +882,12 @@ __device__ __forceinline__ bool fused_layer(const FusedArgs& a, int l, int t, in
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     // the MMAs have read the weights: fetch the next layer's while the accumulator drains
     if (l + 1 < a.L) {
-        tc::fetch_weights(a.wt[l + 1], a.ci[l + 1], a.co[l + 1], w_a);
+        tc::fetch_weights<kFusedThreads>(a.wt[l + 1], a.ci[l + 1], a.co[l + 1], w_a);
         tc::cp_commit();
     }
     const size_t p0 = ((size_t)b * H + h) * W + w0;
-    conv_tc_epilogue<CIN, COUT, EPI>(tmem, p0, breg, a.y, EPI == EPI_GELU_ACT ? a.act[l + 1] : nullptr, nullptr, stf,
-                                     stb, (size_t)a.B * H * W);
+    conv_tc_epilogue<CIN, COUT, EPI, kFusedWarps>(tmem, p0, breg, a.y, EPI == EPI_GELU_ACT ? a.act[l + 1] : nullptr,
+                                               nullptr, stf, stb, (size_t)a.B * H * W);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     if (l + 1 < a.L) {   // publish the row
         __threadfence();
@@ -894,7 +913,7 @@ __device__ __forceinline__ bool fused_dispatch(const FusedArgs& a, int l, int t,
     return fused_layer<16, 16, EPI>(a, l, t, tup, tdn, b, h, w0, base, in_a, w_a, bar_a, phase, tmem, stf, stb);
 }
 
-__global__ void __launch_bounds__(kThreads, 1) k_cnn_fused(FusedArgs a) {
+__global__ void __launch_bounds__(kFusedThreads, 1) k_cnn_fused(FusedArgs a) {
     QGN_PDL_ENTRY();
     using FL = tc::FusedLay;
     extern __shared__ __align__(1024) unsigned char smtc[];
@@ -921,7 +940,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_cnn_fused(FusedArgs a) {
         asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(a.flags + t) : "memory");
         *sbase = v;
     }
-    tc::fetch_weights(a.wt[0], a.ci[0], a.co[0], w_a);
+    tc::fetch_weights<kFusedThreads>(a.wt[0], a.ci[0], a.co[0], w_a);
     tc::cp_commit();
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -990,11 +1009,11 @@ __host__ __device__ constexpr uint32_t idesc_mn() {
 }
 
 // one G row segment (image b, row h, pixels w0 .. w0+127) into a slot [C/8][128][16 B]
-template <int C>
+template <int C, int NT>
 __device__ __forceinline__ void fetch_grow(const __nv_bfloat16* __restrict__ g, int b, int h, int H, int W, int w0,
                                           uint32_t slot_addr) {
     const size_t row = ((size_t)b * H + h) * W + w0;
-    for (int i = threadIdx.x; i < kTileP * (C / 8); i += kThreads) {
+    for (int i = threadIdx.x; i < kTileP * (C / 8); i += NT) {
         const int c8 = i % (C / 8), px = i / (C / 8);
         cp16(slot_addr + (uint32_t)((c8 * kTileP + px) * 16), g + (row + px) * C + c8 * 8);
     }
@@ -1049,8 +1068,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int row = r0 + s / segs, w0 = (s % segs) * kTileP;
         const int b = row / H, h = row % H;
         const uint32_t xs = base_a + (uint32_t)(buf * L::STAGE), gs = xs + (uint32_t)L::X_BYTES;
-        tc::fetch_row<CIN>(x, b, (h + dh + H) % H, H, W, w0, xs);
-        tc::fetch_grow<COUT>(gr, b, h, H, W, w0, gs);
+        tc::fetch_row<CIN, kThreads>(x, b, (h + dh + H) % H, H, W, w0, xs);
+        tc::fetch_grow<COUT, kThreads>(gr, b, h, H, W, w0, gs);
         tc::cp_commit();
     };
     fetch(0, 0);
@@ -1226,7 +1245,7 @@ cudaError_t launch_conv_t(qgn_cnn* n, const __nv_bfloat16* x, const __nv_bfloat1
     if (n->engine == 0) {
         constexpr int SM = tc::Lay<CIN, COUT>::SMEM;
         if (cudaError_t e = smem_opt_in(k_conv_tc<CIN, COUT, EPI>, SM); e != cudaSuccess) return e;
-        ::qgn::launch(k_conv_tc<CIN, COUT, EPI>, conv_grid(n, batch), kThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W,
+        ::qgn::launch(k_conv_tc<CIN, COUT, EPI>, conv_grid(n, batch), kTcThreads, SM, n->stream, x, wt, bias, batch, n->H, n->W,
                                                                                     outf, outb, zin, n->d_err);
         return cudaGetLastError();
     }
@@ -1354,7 +1373,7 @@ bool fused_ok(qgn_cnn* net, int batch) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (smem_opt_in(k_cnn_fused, tc::FusedLay::SMEM) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cnn_fused, kThreads, tc::FusedLay::SMEM) !=
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cnn_fused, kFusedThreads, tc::FusedLay::SMEM) !=
                 cudaSuccess)
             per = 0;
         net->fused_max_tiles = per > 0 ? sms * per : -1;
@@ -1389,7 +1408,7 @@ int forward_fused(qgn_cnn* net, int batch, const __nv_bfloat16* x, float* y, boo
     // cooperative: every CTA is resident at once, which the waits on neighbouring rows need
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(tiles);
-    cfg.blockDim = dim3(kThreads);
+    cfg.blockDim = dim3(kFusedThreads);
     cfg.dynamicSmemBytes = tc::FusedLay::SMEM;
     cfg.stream = net->stream;
     cudaLaunchAttribute attr[1];

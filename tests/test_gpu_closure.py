@@ -306,11 +306,12 @@ def test_trained_closure_beats_leith_offline(cuda_ok):
 
 
 def test_trained_closure_beats_leith_online(cuda_ok):
-    """The benchmark's closure experiment (qgn_fortran_b200.closure_experiment, its defaults: a
-    1024^2 x 4 truth spun up for a model year, 1024 coarse-grained samples, 3000 Adam steps, a
-    3-day background hyperviscosity): over 60 model days from the coarse-grained truth, the
-    128^2 run with the trained network stays closer to the coarse-grained truth's time-mean KE
-    spectrum than the 128^2 QG-Leith run, and runs at >= 50x the truth run's days/s."""
+    """The benchmark's closure experiment (qgn_fortran_b200.closure_experiment, its defaults:
+    1024 coarse-grained samples from a 1024^2 x 4 truth run (seed 6) spun up for a model year,
+    3000 Adam steps, a 3-day background hyperviscosity; evaluated on the seed-5 truth, which the
+    network never saw): over 60 model days from the coarse-grained truth, the 128^2 run with
+    the trained network stays closer to the coarse-grained truth's time-mean KE spectrum than
+    the 128^2 QG-Leith run, and runs at >= 50x the truth run's days/s."""
     from qgn_fortran_b200.closure_experiment import run
     res = run()
     print("closure online:", res["ke_spectrum_err_closure"], "leith:", res["ke_spectrum_err_leith"],
