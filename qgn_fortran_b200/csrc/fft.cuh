@@ -4,7 +4,7 @@
 // (T = TP elements per thread, TP = 16 or 32, fewer for N < TP) as a sequence of Stockham
 // decimation-in-time radix passes: radix TP for every pass except the last, which
 // takes the remaining factor.  Each pass reads T values from shared memory into
-// registers, applies the inter-pass twiddles, performs register-resident radix-R
+// registers, applies the inter-pass twiddles (folded into the first radix-2 stage), performs register-resident radix-R
 // DFTs and writes the results back in place (the load and store halves of a pass
 // are separated by a barrier).  Indices are padded by one element per TP
 // (p -> p + p/TP) so that both the strided stores of the first pass and the
@@ -52,71 +52,6 @@ __device__ __forceinline__ int fpad(int p) { return p + p / TP; }
 // padded length of one transform of length N
 template <int TP = 16>
 __host__ __device__ constexpr int fpadlen(int N) { return N + N / TP; }
-
-// Multiply by exp(DIR * 2*pi*i * m/16); m is a compile-time constant after unrolling.
-template <int DIR, class CT>
-__device__ __forceinline__ CT rot16(CT a, int m) {
-    using R = typename CTraits<CT>::R;
-    constexpr R C1 = (R)0.92387953251128675613;  // cos(pi/8)
-    constexpr R S1 = (R)0.38268343236508977173;  // sin(pi/8)
-    constexpr R HH = (R)0.70710678118654752440;  // sqrt(2)/2
-    switch (m & 15) {
-        case 0: return a;
-        case 4: return DIR > 0 ? cmk<CT>(-a.y, a.x) : cmk<CT>(a.y, -a.x);
-        case 8: return cmk<CT>(-a.x, -a.y);
-        case 12: return DIR > 0 ? cmk<CT>(a.y, -a.x) : cmk<CT>(-a.y, a.x);
-        case 2: { R s = DIR * HH; return cmk<CT>(HH * a.x - s * a.y, s * a.x + HH * a.y); }
-        case 6: { R s = DIR * HH; return cmk<CT>(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
-        case 10: { R s = -DIR * HH; return cmk<CT>(-HH * a.x - s * a.y, s * a.x - HH * a.y); }
-        case 14: { R s = -DIR * HH; return cmk<CT>(HH * a.x - s * a.y, s * a.x + HH * a.y); }
-        default: break;
-    }
-    R c, s;
-    switch (m & 15) {
-        case 1: c = C1; s = S1; break;
-        case 3: c = S1; s = C1; break;
-        case 5: c = -S1; s = C1; break;
-        case 7: c = -C1; s = S1; break;
-        case 9: c = -C1; s = -S1; break;
-        case 11: c = -S1; s = -C1; break;
-        case 13: c = S1; s = -C1; break;
-        default: c = C1; s = -S1; break;  // 15
-    }
-    s = DIR * s;
-    return cmk<CT>(a.x * c - a.y * s, a.x * s + a.y * c);
-}
-
-// Multiply by exp(DIR * 2*pi*i * m/32) for 0 <= m < 16; m is a compile-time constant after
-// unrolling.  Even m reduce to rot16; odd m use cos and sin of pi/16 and 3*pi/16.
-template <int DIR, class CT>
-__device__ __forceinline__ CT rot32(CT a, int m) {
-    using R = typename CTraits<CT>::R;
-    if ((m & 1) == 0) return rot16<DIR>(a, m >> 1);
-    constexpr R A = (R)0.98078528040323044913;  // cos(pi/16)
-    constexpr R B = (R)0.19509032201612826785;  // sin(pi/16)
-    constexpr R E = (R)0.83146961230254523708;  // cos(3 pi/16)
-    constexpr R F = (R)0.55557023301960222474;  // sin(3 pi/16)
-    R c, s;
-    switch (m & 15) {
-        case 1: c = A; s = B; break;
-        case 3: c = E; s = F; break;
-        case 5: c = F; s = E; break;
-        case 7: c = B; s = A; break;
-        case 9: c = -B; s = A; break;
-        case 11: c = -F; s = E; break;
-        case 13: c = -E; s = F; break;
-        default: c = -A; s = B; break;  // 15
-    }
-    s = DIR * s;
-    return cmk<CT>(a.x * c - a.y * s, a.x * s + a.y * c);
-}
-
-// Multiply by exp(DIR * 2*pi*i * k/R), 0 <= k < R/2.
-template <int R, int DIR, class CT>
-__device__ __forceinline__ CT rot_root(CT a, int k) {
-    if constexpr (R == 32) return rot32<DIR>(a, k);
-    else return rot16<DIR>(a, k * (16 / R));
-}
 
 // cos and sin of 2 pi k / R for the non-trivial roots of the radix-2 butterflies
 // (R = 8, 16, 32; 0 < k < R/2, k != R/4), from the first-octant constants
@@ -172,16 +107,18 @@ __device__ __forceinline__ void bfly(CT& a, CT& b, int k) {
     b = cmk<CT>(fma(-f, u, e.x), fma(-f, w, e.y));
 }
 
-// In-register DFT of length R (1,2,4,8,16,32), natural order in and out, sign DIR.
-template <int R, int DIR>
+// In-register DFT of length R (1,2,4,8,16,32), natural order in and out, sign DIR.  With S1 the
+// first radix-2 stage -- the sums and differences of elements i and i + R/2 -- has been done
+// by the caller (twiddled_dft): the recursion's length-2 base cases are then the identity.
+template <int R, int DIR, bool S1 = false>
 struct RegDFT {
     template <class CT>
     __device__ __forceinline__ static void run(CT* v) {
         CT e[R / 2], o[R / 2];
 #pragma unroll
         for (int i = 0; i < R / 2; ++i) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
-        RegDFT<R / 2, DIR>::run(e);
-        RegDFT<R / 2, DIR>::run(o);
+        RegDFT<R / 2, DIR, S1>::run(e);
+        RegDFT<R / 2, DIR, S1>::run(o);
 #pragma unroll
         for (int k = 0; k < R / 2; ++k) {
             CT x = e[k], y = o[k];
@@ -191,18 +128,20 @@ struct RegDFT {
         }
     }
 };
-template <int DIR>
-struct RegDFT<1, DIR> {
+template <int DIR, bool S1>
+struct RegDFT<1, DIR, S1> {
     template <class CT>
     __device__ __forceinline__ static void run(CT*) {}
 };
-template <int DIR>
-struct RegDFT<2, DIR> {
+template <int DIR, bool S1>
+struct RegDFT<2, DIR, S1> {
     template <class CT>
     __device__ __forceinline__ static void run(CT* v) {
-        CT a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
+        if constexpr (!S1) {
+            CT a = v[0], b = v[1];
+            v[0] = cadd(a, b);
+            v[1] = csub(a, b);
+        }
     }
 };
 
@@ -212,56 +151,78 @@ struct FFTShape {
     static constexpr int G = N / T;             // threads per transform
 };
 
-// Inter-pass twiddles of one radix-R butterfly: v[r] *= w^r, w = exp(DIR 2 pi i k/(NS R)).
-// w^(2^q) come from the table tw[m] = exp(-2 pi i m/N) (conjugated for DIR=+1); the other
-// powers are products of at most three table values, formed just before use.
+// First radix-2 stage with the inter-pass twiddle of its second element folded in: given a
+// (already multiplied by its own twiddle), (a + W b, a - W b) as a + W b by four FMAs and
+// a - W b = 2 a - (a + W b) by two, against a complex product and four additions.
+template <class CT>
+__device__ __forceinline__ void fold2(CT& a, CT& b, CT W) {
+    using T = typename CTraits<CT>::R;
+    const CT y0 = cmk<CT>(fma(b.x, W.x, fma(-b.y, W.y, a.x)), fma(b.x, W.y, fma(b.y, W.x, a.y)));
+    b = cmk<CT>(fma((T)2, a.x, -y0.x), fma((T)2, a.y, -y0.y));
+    a = y0;
+}
+
+// The radix-R DFT of v[r] w^r, w = exp(DIR 2 pi i k/(NS R)): the twiddle powers are formed as in
+// apply_twiddles (table values w^(2^q), the others products of at most three of them), pair by
+// pair (j, j + R/2) of the first radix-2 stage, which fold2 performs; RegDFT does the rest.
 template <int N, int NS, int R, int DIR, class CT>
-__device__ __forceinline__ void apply_twiddles(CT* v, int k, const CT* __restrict__ tw) {
-    if constexpr (NS > 1) {
+__device__ __forceinline__ void twiddled_dft(CT* v, int k, const CT* __restrict__ tw) {
+    if constexpr (NS == 1 || R < 2) {
+        RegDFT<R, DIR>::run(v);
+    } else {
         constexpr int S = N / (NS * R);
         const int kS = k * S;
         auto ldw = [&](int r) {
             const CT t = __ldg(&tw[r * kS]);
             return DIR > 0 ? cconj(t) : t;
         };
+        constexpr int H = R / 2;
+        const CT wH = ldw(H);                   // w^(R/2), the second element's extra factor
         const CT w1 = ldw(1);
-        v[1] = cmul(v[1], w1);
-        if constexpr (R > 2) {
-            const CT w2 = ldw(2);
-            const CT w3 = cmul(w2, w1);
-            v[2] = cmul(v[2], w2);
-            v[3] = cmul(v[3], w3);
-            if constexpr (R > 4) {
-                const CT w4 = ldw(4);
-                const CT w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
-                v[4] = cmul(v[4], w4);
-                v[5] = cmul(v[5], w5);
-                v[6] = cmul(v[6], w6);
-                v[7] = cmul(v[7], w7);
-                if constexpr (R > 8) {
-                    const CT w8 = ldw(8);
-                    v[8] = cmul(v[8], w8);
-                    v[9] = cmul(v[9], cmul(w8, w1));
-                    v[10] = cmul(v[10], cmul(w8, w2));
-                    v[11] = cmul(v[11], cmul(w8, w3));
-                    v[12] = cmul(v[12], cmul(w8, w4));
-                    v[13] = cmul(v[13], cmul(w8, w5));
-                    v[14] = cmul(v[14], cmul(w8, w6));
-                    v[15] = cmul(v[15], cmul(w8, w7));
-                    if constexpr (R > 16) {
-                        // w^(16+r) = w16 * w^r; the low powers are formed again from the table
-                        const CT w16 = ldw(16);
-                        const CT u[8] = {w16, cmul(w16, w1), cmul(w16, w2), cmul(w16, w3),
-                                         cmul(w16, w4), cmul(w16, w5), cmul(w16, w6), cmul(w16, w7)};
+        CT w2 = w1, w3 = w1, w4 = w1;
+        if constexpr (R >= 8) w2 = ldw(2);
+        if constexpr (R >= 8) w3 = cmul(w2, w1);
+        if constexpr (R >= 16) w4 = ldw(4);
+        // w^j for 0 < j < 8 (j < R/2): one product at most beyond the loads
+        auto lowpow = [&](int j) -> CT {
+            switch (j) {
+                case 1: return w1;
+                case 2: return w2;
+                case 3: return w3;
+                case 4: return w4;
+                case 5: return cmul(w4, w1);
+                case 6: return cmul(w4, w2);
+                default: return cmul(w4, w3);   // 7
+            }
+        };
+        if constexpr (R <= 16) {
 #pragma unroll
-                        for (int r = 0; r < 8; ++r) {
-                            v[16 + r] = cmul(v[16 + r], u[r]);
-                            v[24 + r] = cmul(v[24 + r], cmul(u[r], w8));
-                        }
-                    }
+            for (int j = 0; j < H; ++j) {
+                if (j == 0) {
+                    fold2(v[0], v[H], wH);
+                } else {
+                    const CT Wj = lowpow(j);
+                    v[j] = cmul(v[j], Wj);
+                    fold2(v[j], v[j + H], cmul(wH, Wj));
                 }
             }
+        } else {   // R = 32: j and j + 8 share w^j; w^(j+8) = w8 w^j, and w^16 is wH
+            const CT w8 = ldw(8);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const CT Wj = j == 0 ? w8 : lowpow(j);   // (w8 unused as Wj when j == 0)
+                if (j == 0) {
+                    fold2(v[0], v[16], wH);
+                } else {
+                    v[j] = cmul(v[j], Wj);
+                    fold2(v[j], v[j + 16], cmul(wH, Wj));
+                }
+                const CT W8 = j == 0 ? w8 : cmul(w8, Wj);
+                v[j + 8] = cmul(v[j + 8], W8);
+                fold2(v[j + 8], v[j + 24], cmul(W8, wH));
+            }
         }
+        RegDFT<R, DIR, true>::run(v);
     }
 }
 
@@ -318,8 +279,7 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
         for (int b = 0; b < BPT; ++b) {
             const int j = lane + b * G;
             const int k = j & (NS - 1);
-            apply_twiddles<N, NS, R, DIR>(&v[b * R], k, tw);
-            RegDFT<R, DIR>::run(&v[b * R]);
+            twiddled_dft<N, NS, R, DIR>(&v[b * R], k, tw);
             const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
