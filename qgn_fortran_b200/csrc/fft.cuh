@@ -162,9 +162,10 @@ __device__ __forceinline__ void fold2(CT& a, CT& b, CT W) {
     a = y0;
 }
 
-// The radix-R DFT of v[r] w^r, w = exp(DIR 2 pi i k/(NS R)): the twiddle powers are formed as in
-// apply_twiddles (table values w^(2^q), the others products of at most three of them), pair by
-// pair (j, j + R/2) of the first radix-2 stage, which fold2 performs; RegDFT does the rest.
+// The radix-R DFT of v[r] w^r, w = exp(DIR 2 pi i k/(NS R)) (the inter-pass twiddles of a
+// Stockham pass): the powers w^(2^q) come from the table, the others are products of at most
+// three of them, formed pair by pair (j, j + R/2) of the first radix-2 stage, which fold2
+// performs; RegDFT does the rest.
 template <int N, int NS, int R, int DIR, class CT>
 __device__ __forceinline__ void twiddled_dft(CT* v, int k, const CT* __restrict__ tw) {
     if constexpr (NS == 1 || R < 2) {
@@ -293,15 +294,96 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
     if constexpr (TO_SMEM) fft_sync<LAST, WS>();
 }
 
-template <int N, int NS, int DIR, int SRC0, int DSTL, int TP, bool WS, class CT, class Ld, class St>
+// The last two passes of an N = 2 TP NS point transform (a radix-TP pass at sub-length NS, then
+// the final radix-2 pass), fused, with the exchange between them done by warp shuffles
+// instead of shared memory.  Radix-2 butterfly j' (< N/2) pairs element j' + NS r of the first
+// with element N/2 + j' + NS r: outputs r of the first pass's butterflies j and j + NS.  The
+// first pass assigns its butterflies to the transform's threads so that j and j + NS are 16
+// threads of the block apart in one warp: the transform's thread l has block thread
+// l IL + slot (IL threads of other transforms interleaved, IL * LPW = 32 with LPW of its
+// threads in each warp), and takes butterfly
+//   j(l) = H (l / LPW) + l % H + NS ((l % LPW) / H),  H = LPW / 2,
+// whose partner l ^ H is block thread ^ 16.  The lower thread of a pair keeps its outputs
+// r < TP/2 and the partner's r < TP/2, the upper one the outputs r >= TP/2 of both; each
+// then does TP/2 radix-2 butterflies.  One read of shared memory, one write and two barriers
+// in place of two of each and four.  Every thread of the warp executes the shuffles (a
+// transform's threads share `active`, and inactive ones exchange unused registers).
+template <int N, int NS, int DIR, int SRC, int DST, int TP, bool WS, int IL, class CT, class Ld, class St>
+__device__ __forceinline__ void fft_pass_tail2(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
+    constexpr int R = TP;
+    constexpr int LPW = 32 / IL, H = LPW / 2;
+    constexpr int STRIDE = N / R;
+    static_assert(2 * R * NS == N && IL >= 1 && IL <= 16 && 32 % IL == 0, "fused radix-2 tail");
+    static_assert(FFTShape<N, TP>::T == R && FFTShape<N, TP>::G % LPW == 0, "whole warps per transform");
+    const int j = H * (lane / LPW) + lane % H + NS * ((lane % LPW) / H);
+    const bool upper = j >= NS;
+    const int jl = upper ? j - NS : j;
+    CT v[R];
+    if (active) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int idx = j + r * STRIDE;
+            if constexpr (SRC == SRC_SMEM) v[r] = x[fpad<TP>(idx)];
+            else v[r] = ld(idx);
+        }
+    }
+    constexpr bool TO_SMEM = (DST == DST_SMEM || DST == DST_SMEM_MAP || DST == DST_SMEM_STORE);
+    if constexpr (TO_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
+    if (active) twiddled_dft<N, NS, R, DIR>(v, j & (NS - 1), tw);
+#pragma unroll
+    for (int r = 0; r < R / 2; ++r) {
+        // the upper thread sends its outputs r < R/2, the lower one its outputs r >= R/2
+        const CT send = upper ? v[r] : v[r + R / 2];
+        CT recv;
+        recv.x = __shfl_xor_sync(0xffffffffu, send.x, 16);
+        recv.y = __shfl_xor_sync(0xffffffffu, send.y, 16);
+        if (active) {
+            const int rr = upper ? r + R / 2 : r;
+            CT a = upper ? recv : v[r];
+            CT b = upper ? v[r + R / 2] : recv;
+            const int jp = jl + NS * rr;   // radix-2 butterfly: twiddle w^jp, outputs jp and jp + N/2
+            const CT t = __ldg(&tw[jp]);
+            fold2(a, b, DIR > 0 ? cconj(t) : t);
+            if constexpr (DST == DST_SMEM) {
+                x[fpad<TP>(jp)] = a;
+                x[fpad<TP>(jp + N / 2)] = b;
+            } else if constexpr (DST == DST_SMEM_MAP) {
+                x[st(jp)] = a;
+                x[st(jp + N / 2)] = b;
+            } else {
+                st(jp, a);
+                st(jp + N / 2, b);
+            }
+        }
+    }
+    if constexpr (TO_SMEM) fft_sync<true, WS>();
+}
+
+// whether fft_pass_tail2 takes the pass at sub-length NS and the last one
+template <int N, int NS, int TP, int IL>
+__host__ __device__ constexpr bool tail2_applies() {
+    if (IL <= 0 || IL > 16 || 32 % IL != 0) return false;
+    if (N / NS < TP || 2 * TP * NS != N) return false;   // a radix-TP pass followed by the radix-2 one
+    if (FFTShape<N, TP>::T != TP) return false;
+    return FFTShape<N, TP>::G % (32 / IL) == 0;           // the transform's threads fill whole warp rows
+}
+
+// IL: 0, or the interleave of the caller's threads (see fft_pass_tail2), which fuses the last
+// two passes when the last one is radix 2 and its partners sit in one warp
+template <int N, int NS, int DIR, int SRC0, int DSTL, int TP, bool WS, int IL, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_rec(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
     constexpr int R = (N / NS >= TP) ? TP : N / NS;
     constexpr bool FIRST = (NS == 1);
     constexpr bool LAST = (NS * R == N);
     constexpr int SRC = FIRST ? SRC0 : SRC_SMEM;
     constexpr int DST = LAST ? DSTL : DST_SMEM;
-    fft_pass_io<N, NS, DIR, SRC, DST, TP, WS>(x, lane, active, tw, ld, st);
-    if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL, TP, WS>(x, lane, active, tw, ld, st);
+    constexpr bool TAIL2 = tail2_applies<N, NS, TP, IL>();
+    if constexpr (TAIL2) {
+        fft_pass_tail2<N, NS, DIR, SRC, DSTL, TP, WS, IL>(x, lane, active, tw, ld, st);
+    } else {
+        fft_pass_io<N, NS, DIR, SRC, DST, TP, WS>(x, lane, active, tw, ld, st);
+        if constexpr (!LAST) fft_rec<N, NS * R, DIR, SRC0, DSTL, TP, WS, IL>(x, lane, active, tw, ld, st);
+    }
 }
 
 template <class CT>
@@ -316,16 +398,16 @@ using NoIO = NoIOT<double2>;
 // synced by the caller) and delivering its output through st (DSTL = DST_FN) or into x
 // (DST_SMEM, synced block-wide on return).  Every thread of the block calls this (it may
 // contain __syncthreads).  WS as for fft_pass_io.
-template <int N, int DIR, int SRC0, int DSTL, int TP = 16, bool WS = false, class CT, class Ld, class St>
+template <int N, int DIR, int SRC0, int DSTL, int TP = 16, bool WS = false, int IL = 0, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_fused(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld ld, St st) {
-    fft_rec<N, 1, DIR, SRC0, DSTL, TP, WS>(x, lane, active, tw, ld, st);
+    fft_rec<N, 1, DIR, SRC0, DSTL, TP, WS, IL>(x, lane, active, tw, ld, st);
 }
 
 // In-place N-point transform of the padded array x (caller syncs before; ends with a barrier).
 template <int N, int DIR, int TP = 16, class CT>
 __device__ __forceinline__ void fft_block(CT* x, int lane, bool active, const CT* __restrict__ tw) {
     NoIOT<CT> io;
-    fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM, TP, false>(x, lane, active, tw, io, io);
+    fft_rec<N, 1, DIR, SRC_SMEM, DST_SMEM, TP, false, 0>(x, lane, active, tw, io, io);
 }
 
 }  // namespace qgn

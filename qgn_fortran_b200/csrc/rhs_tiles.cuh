@@ -326,7 +326,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
                 };
                 // SRC_FN_SMEM: every thread has read the staged column before the first pass
                 // overwrites the slot (block-wide barrier inside the pass)
-                fft_fused<NY, +1, SRC_FN_SMEM, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, lds, omap);
+                fft_fused<NY, +1, SRC_FN_SMEM, DST_SMEM_MAP, C::TP, false, C::TKX>(xs, lane, true, twy, lds, omap);
                 if (tid == 0) bar_inval(&ybar);           // every waiter has passed the barrier
                 staged = true;
             }
@@ -339,7 +339,7 @@ __device__ __forceinline__ void yinv_tile(const Geom g, int bx, int l, const CT*
                 if (!in_bounds(g, ci, g.csize())) return cmk<CT>(0.0, 0.0);
                 return deriv(src[ci], j);
             };
-            fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
+            fft_fused<NY, +1, SRC_FN, DST_SMEM_MAP, C::TP, false, C::TKX>(xs, lane, true, twy, ld, omap);
         }
         // pack rows (2p, 2p+1): e -> (pair p, column c); both arrays of a pair row per thread
         CT* dl = dst + (size_t)l * (NY / 2) * 2 * g.nkxp;
@@ -530,7 +530,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
             const bool ok = colok && in_bounds(g, i, (size_t)g.ny * 2 * g.nkxp);
             return unpack_pair(pd, i, kx0 + c, fld, ok, C::TKX);
         };
-        fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ldd, omap);
+        fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP, false, C::SLOTS>(xs, lane, true, twy, ldd, omap);
         const RT dc = (RT)lc->dragc;
         for (int e = tid; e < C::TKX * nky; e += C::THREADS) {
             const int cc = e / nky, m = e % nky;
@@ -553,7 +553,7 @@ __device__ __forceinline__ void yfwd_tile(const Geom g, int bx, int l, const Lay
         const bool ok = colok && in_bounds(g, i, 2 * g.hsize());
         return unpack_pair(pp, i, kx0 + c, fld, ok, C::TKX);
     };
-    fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP>(xs, lane, true, twy, ld, omap);
+    fft_fused<NY, -1, SRC_FN, DST_SMEM_MAP, C::TP, false, C::SLOTS>(xs, lane, true, twy, ld, omap);
 
     const RT ub = (RT)lc->uBar[l], bq = (RT)lc->betaq[l];
     const RT ek = (RT)lc->ekman;
