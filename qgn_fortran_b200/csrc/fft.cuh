@@ -294,30 +294,34 @@ __device__ __forceinline__ void fft_pass_io(CT* x, int lane, bool active, const 
     if constexpr (TO_SMEM) fft_sync<LAST, WS>();
 }
 
-// The last two passes of an N = 2 TP NS point transform (a radix-TP pass at sub-length NS, then
-// the final radix-2 pass), fused, with the exchange between them done by warp shuffles
-// instead of shared memory.  Radix-2 butterfly j' (< N/2) pairs element j' + NS r of the first
-// with element N/2 + j' + NS r: outputs r of the first pass's butterflies j and j + NS.  The
-// first pass assigns its butterflies to the transform's threads so that j and j + NS are 16
-// threads of the block apart in one warp: the transform's thread l has block thread
-// l IL + slot (IL threads of other transforms interleaved, IL * LPW = 32 with LPW of its
-// threads in each warp), and takes butterfly
-//   j(l) = H (l / LPW) + l % H + NS ((l % LPW) / H),  H = LPW / 2,
-// whose partner l ^ H is block thread ^ 16.  The lower thread of a pair keeps its outputs
-// r < TP/2 and the partner's r < TP/2, the upper one the outputs r >= TP/2 of both; each
-// then does TP/2 radix-2 butterflies.  One read of shared memory, one write and two barriers
-// in place of two of each and four.  Every thread of the warp executes the shuffles (a
-// transform's threads share `active`, and inactive ones exchange unused registers).
+// The last two passes of an N = RL TP NS point transform (a radix-TP pass at sub-length NS, then
+// the final radix-RL pass, RL = 2, 4 or 8), fused, with the exchange between them done by warp
+// shuffles instead of shared memory.  Final butterfly j' (< N/RL) takes the elements
+// j' + m N/RL, m < RL, which are outputs r of the first pass's butterflies j + m NS
+// (j' = j + NS r, j < NS).  The first pass assigns its butterflies to the transform's threads
+// so that these RL sit in one warp: the transform's thread l is block thread l IL + slot (IL
+// threads of other transforms interleaved, LPW = 32/IL of its threads per warp), and takes
+// butterfly
+//   j(l) = H (l / LPW) + l % H + NS q,  q = (l % LPW) / H,  H = LPW / RL,
+// so that partner q ^ m is block thread ^ (32/RL) m.  Thread q finishes the final butterflies of
+// its outputs r in [q TP/RL, (q+1) TP/RL): in round m = 1 .. RL-1 it sends partner p = q ^ m its
+// block of outputs p and receives the partner's block q into the registers of the block just
+// sent, after which register block m holds the inputs from partner m.  One read of shared
+// memory, one write and two barriers in place of two of each and four.  Every thread of the
+// warp executes the shuffles (a transform's threads share `active`; inactive ones exchange
+// unused registers).
 template <int N, int NS, int DIR, int SRC, int DST, int TP, bool WS, int IL, class CT, class Ld, class St>
 __device__ __forceinline__ void fft_pass_tail2(CT* x, int lane, bool active, const CT* __restrict__ tw, Ld& ld, St& st) {
     constexpr int R = TP;
-    constexpr int LPW = 32 / IL, H = LPW / 2;
+    constexpr int RL = N / (TP * NS);
+    constexpr int B = R / RL;                    // outputs per block
+    constexpr int LPW = 32 / IL, H = LPW / RL;
     constexpr int STRIDE = N / R;
-    static_assert(2 * R * NS == N && IL >= 1 && IL <= 16 && 32 % IL == 0, "fused radix-2 tail");
-    static_assert(FFTShape<N, TP>::T == R && FFTShape<N, TP>::G % LPW == 0, "whole warps per transform");
-    const int j = H * (lane / LPW) + lane % H + NS * ((lane % LPW) / H);
-    const bool upper = j >= NS;
-    const int jl = upper ? j - NS : j;
+    static_assert((RL == 2 || RL == 4 || RL == 8) && RL * R * NS == N && H >= 1, "fused radix-RL tail");
+    static_assert(FFTShape<N, TP>::T == R && FFTShape<N, TP>::G % LPW == 0, "whole warp rows per transform");
+    const int q = (lane % LPW) / H;
+    const int jl = H * (lane / LPW) + lane % H;
+    const int j = jl + NS * q;
     CT v[R];
     if (active) {
 #pragma unroll
@@ -331,39 +335,58 @@ __device__ __forceinline__ void fft_pass_tail2(CT* x, int lane, bool active, con
     if constexpr (TO_SMEM && SRC != SRC_FN) fft_sync<SRC == SRC_FN_SMEM, WS>();
     if (active) twiddled_dft<N, NS, R, DIR>(v, j & (NS - 1), tw);
 #pragma unroll
-    for (int r = 0; r < R / 2; ++r) {
-        // the upper thread sends its outputs r < R/2, the lower one its outputs r >= R/2
-        const CT send = upper ? v[r] : v[r + R / 2];
-        CT recv;
-        recv.x = __shfl_xor_sync(0xffffffffu, send.x, 16);
-        recv.y = __shfl_xor_sync(0xffffffffu, send.y, 16);
-        if (active) {
-            const int rr = upper ? r + R / 2 : r;
-            CT a = upper ? recv : v[r];
-            CT b = upper ? v[r + R / 2] : recv;
-            const int jp = jl + NS * rr;   // radix-2 butterfly: twiddle w^jp, outputs jp and jp + N/2
-            const CT t = __ldg(&tw[jp]);
-            fold2(a, b, DIR > 0 ? cconj(t) : t);
-            if constexpr (DST == DST_SMEM) {
-                x[fpad<TP>(jp)] = a;
-                x[fpad<TP>(jp + N / 2)] = b;
-            } else if constexpr (DST == DST_SMEM_MAP) {
-                x[st(jp)] = a;
-                x[st(jp + N / 2)] = b;
-            } else {
-                st(jp, a);
-                st(jp + N / 2, b);
+    for (int m = 1; m < RL; ++m) {
+        const int p = q ^ m;
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            CT send = v[i];
+#pragma unroll
+            for (int b = 1; b < RL; ++b)
+                if (b == p) send = v[b * B + i];
+            CT recv;
+            recv.x = __shfl_xor_sync(0xffffffffu, send.x, (32 / RL) * m);
+            recv.y = __shfl_xor_sync(0xffffffffu, send.y, (32 / RL) * m);
+#pragma unroll
+            for (int b = 0; b < RL; ++b)
+                if (b == p) v[b * B + i] = recv;
+        }
+    }
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < B; ++i) {
+            CT u[RL];
+#pragma unroll
+            for (int m = 0; m < RL; ++m) u[m] = v[m * B + i];
+            const int jp = jl + NS * (q * B + i);   // final butterfly: outputs jp + m N/RL
+            twiddled_dft<N, N / RL, RL, DIR>(u, jp, tw);
+#pragma unroll
+            for (int m = 0; m < RL; ++m) {
+                const int idx = jp + m * (N / RL);
+                if constexpr (DST == DST_SMEM) x[fpad<TP>(idx)] = u[m];
+                else if constexpr (DST == DST_SMEM_MAP) x[st(idx)] = u[m];
+                else st(idx, u[m]);
             }
         }
     }
     if constexpr (TO_SMEM) fft_sync<true, WS>();
 }
 
+// Largest final radix whose pass fft_pass_tail2 fuses (build-time knob, default 2).  Measured on
+// B200: with radix-4 tails too, the FP32 1024-point y transforms (16 x 16 x 4) ran slower --
+// y-inverse 38.4 -> 41.2 us, y-forward 43.6 -> 46.2 us, mixed 1024^2 x 8 step 1.021 -> 1.058
+// ms: FP32 values are cheap to exchange through shared memory, and the rounds' selects are not
+#ifndef QGN_TAIL_RADIX_MAX
+#define QGN_TAIL_RADIX_MAX 2
+#endif
+
 // whether fft_pass_tail2 takes the pass at sub-length NS and the last one
 template <int N, int NS, int TP, int IL>
 __host__ __device__ constexpr bool tail2_applies() {
     if (IL <= 0 || IL > 16 || 32 % IL != 0) return false;
-    if (N / NS < TP || 2 * TP * NS != N) return false;   // a radix-TP pass followed by the radix-2 one
+    if (N / NS < TP || N % (TP * NS) != 0) return false;
+    const int rl = N / (TP * NS);                         // a radix-TP pass, then the radix-rl one
+    if ((rl != 2 && rl != 4 && rl != 8) || rl > QGN_TAIL_RADIX_MAX) return false;
+    if ((32 / IL) % rl != 0) return false;                // the rl partners in one warp row
     if (FFTShape<N, TP>::T != TP) return false;
     return FFTShape<N, TP>::G % (32 / IL) == 0;           // the transform's threads fill whole warp rows
 }
