@@ -69,4 +69,7 @@ def test_argument_validation_without_device(lib):
     assert lib.qgn_step(None, None, None, None) == _lib.QGN_ERR_ARG
     assert lib.qgn_destroy(None) == 0
     assert lib.qgn_probe_fp64_fma(0, None, None) == _lib.QGN_ERR_ARG
+    r = C.c_int()
+    assert lib.qgn_ens_fft_radix(None, 0, C.byref(r)) == _lib.QGN_ERR_ARG
+    assert lib.qgn_ens_set_tiles(None, 0, 128, 16, 0) == _lib.QGN_ERR_ARG
     assert lib.qgn_last_error(None) == b"null context"
