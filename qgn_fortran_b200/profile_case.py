@@ -3,6 +3,7 @@
     python -m qgn_fortran_b200.profile_case --workload strat1024x8 --steps 1
     python -m qgn_fortran_b200.profile_case --workload strat1024x8 --nx 128 --nz 4 --steps 3 --closure
     python -m qgn_fortran_b200.profile_case --cnn-batch 8
+    python -m qgn_fortran_b200.profile_case --cnn-batch 32 --cnn-train 2
     python -m qgn_fortran_b200.profile_case --ensemble 8 --steps 2
 
 The first two build the named workload (optionally at another grid, optionally with a
@@ -10,7 +11,9 @@ closure network of zero weights attached, which always passes the budget check a
 the whole closure path), set the seeded IC on the GPU and advance ``--steps`` device-resident
 TimeSteps, then print the per-kernel-family launch counts and CUDA-event times of those steps.
 ``--cnn-batch`` runs two forwards of the 6-layer closure network (128^2, 4 layers of q and
-psi in, BF16, tcgen05).  ``--ensemble`` advances that many members of the batched-ensemble
+psi in, BF16, tcgen05); with ``--cnn-train`` it instead takes that many Adam steps on seeded
+data of that batch (forward, backward-data and weight gradients on tcgen05, the six layers'
+weight gradients last layer first).  ``--ensemble`` advances that many members of the batched-ensemble
 workload (mixed precision).  Device memory held: the working set only (about 0.7 GB for
 strat1024x8, well under 1 GB for the others).
 """
@@ -66,6 +69,18 @@ def run_cnn(a):
 
     from . import closure as cl
     net = cl.ClosureNet(nz=4, H=128, W=128, layers=6, max_batch=a.cnn_batch, seed=3)
+    if a.cnn_train:
+        gen = torch.Generator(device="cpu").manual_seed(3)
+        n = 2 * a.cnn_batch
+        xd = torch.randn((n, 128, 128, net.cin_p), generator=gen).to(torch.bfloat16).cuda()
+        yd = torch.randn((n, 128, 128, net.cout_p), generator=gen).cuda()
+        idx = torch.arange(a.cnn_batch, dtype=torch.int32).cuda()
+        torch.cuda.synchronize()
+        for _ in range(a.cnn_train):
+            net.train_step(xd, yd, idx, a.cnn_batch, 1e-4, want_loss=False)
+        net.check()
+        print(json.dumps({"cnn_batch": a.cnn_batch, "train_steps": a.cnn_train, "ok": True}))
+        return
     x = torch.zeros((a.cnn_batch, 128, 128, net.cin_p), dtype=torch.bfloat16, device="cuda")
     y = torch.zeros((a.cnn_batch, 128, 128, net.cout_p), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
@@ -96,6 +111,7 @@ def main():
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--closure", action="store_true")
     ap.add_argument("--cnn-batch", type=int, default=0)
+    ap.add_argument("--cnn-train", type=int, default=0)
     ap.add_argument("--ensemble", type=int, default=0)
     a = ap.parse_args()
     if a.cnn_batch:
